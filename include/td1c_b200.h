@@ -1,0 +1,112 @@
+/*
+ * td1c_b200.h -- C-ABI of the B200 (sm_100a) implementation of td1c's
+ * orbital-equation right-hand side.  Plain C types only.
+ *
+ * Drop-in entry points keep the reference's Fortran-to-C symbol names and
+ * argument meaning (include/wrapper.hpp in the td1c tree):
+ *   hprod_bind_      include/wrapper.hpp:110   (src/hprod/hprod_bind.F90)
+ *   hprod_init_      include/wrapper.hpp:185   (src/hprod/hprod_init.F90:2-103)
+ *   hprod_set_wfn0_  include/wrapper.hpp:400   (src/hprod/hprod_set_wfn0.F90:2-130)
+ *   hprod_htot_      include/wrapper.hpp:159   (src/hprod/hprod_htot.F90:2-42)
+ *   hprod_final_     include/wrapper.hpp:132   (src/hprod/hprod_final.F90)
+ * The geometry, tables and flags that the reference hands to Fortran through
+ * bas_rad_bind_, bas_sph_bind_, bas_bas_bind_, ormas_bind_ and control_bind_
+ * (include/wrapper.hpp:773-806; called from src/bas/clbas.cpp:59-146 and
+ * src/control/clcontrol.cpp:185-189) arrive through the td1c_gpu_bind_*
+ * calls below, restricted to the fields the RHS reads.  Operator tables the
+ * reference derives in bas_gen_* (tmat, pmat, d2ll, zfac, pzfac, d2fac) are
+ * derived by the library itself on the device.
+ *
+ * Complex arrays are interleaved (re, im) float64, Fortran column-major:
+ *   wfn, hwfn : orb(1:nrad-1, 0:lmax1, 1:nfun)
+ *   cic, hcic : cic(1:lcic), determinants ordered by beta string, then by the
+ *               alpha strings of matching M; string lists sorted by (M, mask)
+ *   lfield    : lfield(1:3, 1:3) column-major (gauge field, E, A)
+ * Errors: the void drop-in calls record a status readable with
+ * td1c_gpu_last_status() (0 = ok); the td1c_gpu_* calls return it directly.
+ */
+#ifndef TD1C_B200_H
+#define TD1C_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+#define TD1C_BOOL bool
+extern "C" {
+#else
+#define TD1C_BOOL _Bool
+#endif
+
+/* ---- binding of geometry, tables and flags --------------------------- */
+
+/* bas_rad_bind_ (src/bas/bas_bind.F90:2-74): FEDVR radial grid.  Arrays are
+ * indexed 0..nrad; band arrays are (2*ndvr+1) x (nrad+1), band index fastest. */
+int td1c_gpu_bind_rad(int nfe, int ndvr, int nrad, const double* xrad, const double* wrad,
+                      const double* radp, const double* radk, const double* radk0,
+                      double rmask, const double* mask);
+
+/* bas_sph_bind_ (src/bas/bas_bind.F90:76-120): Gauss-Legendre theta grid and
+ * normalised associated Legendre tables, reference layouts
+ * legf1(0:lmax1, 1:nlat, -mmax1:mmax1), legb1(1:nlat, 0:lmax1, -mmax1:mmax1),
+ * legf2(0:lmax2, 1:nlat, -mmax2:mmax2), legb2(1:nlat, 0:lmax2, -mmax2:mmax2). */
+int td1c_gpu_bind_sph(int lmax1, int lmax2, int mmax1, int mmax2, int nlat,
+                      const double* wlat, const double* cost,
+                      const double* legf1, const double* legb1,
+                      const double* legf2, const double* legb2);
+
+/* bas_bas_bind_ + ormas_bind_ (src/bas/bas_bind.F90:122-194,
+ * src/ormas/ormas_bind.F90:1-70): nuclear charge and orbital classes.
+ * otype: -1 frozen core (fc1), 0 dynamic core, 1 active; orbitals ordered
+ * frozen, dynamic core, active.  lval is the nominal l of each orbital. */
+int td1c_gpu_bind_bas(double znuc, int smul, int mtot, int nfun, const int* otype,
+                      const int* mval, const int* lval, int nela, int nelb);
+
+/* control_bind_ (src/control/control_bind.F90:2-61): icomp 1 real time,
+ * 0 imaginary time; igauge 0 length, 1 velocity. */
+int td1c_gpu_bind_control(int icomp, int igauge);
+
+/* ---- drop-in hprod entry points -------------------------------------- */
+void hprod_bind_(double* ene_fcore, double* ene_dcore, double* ene_core, double* ene_act,
+                 double* ene_tot, double* dip_exp, double* vel_exp, double* acc_exp,
+                 const TD1C_BOOL* projhigh, const double* cutoff);
+void hprod_init_(void);
+void hprod_set_wfn0_(const double* wfn, const double* cic, const char* v2xfc_type, int len);
+void hprod_htot_(const double* dtime, const double* lfield, const double* wfn, const double* cic,
+                 double* hwfn, double* hcic);
+void hprod_final_(void);
+
+/* ---- extensions ------------------------------------------------------- */
+int td1c_gpu_last_status(void);
+/* sizes: [nrad, nbas, nbas2, ngrid, nlat, lcic, nfcore, ndcore, nact, ncore,
+ *         nstr_alpha, nstr_beta, npair, ndvr, lmax1, lmax2] */
+int td1c_gpu_dims(int* dims16);
+/* CI tables (for building CI vectors in the library's determinant order):
+ * stra[nstr_a], strb[nstr_b] bit strings; detoff/afirst/acount[nstr_b]. */
+int td1c_gpu_ci_tables(unsigned* stra, unsigned* strb, int* detoff, int* afirst, int* acount);
+/* energies of the last htot: ene_fcore, ene_dcore, ene_core, ene_act, ene_tot */
+int td1c_gpu_energies(double* ene5);
+/* RHS on device-resident buffers (no host copies), on the library stream.
+ * lfield is a host array of 9 doubles. */
+int td1c_gpu_htot_dev(double dtime, const double* lfield, const void* d_wfn, const void* d_cic,
+                      void* d_hwfn, void* d_hcic);
+/* Copy a named device intermediate of the last htot to host memory
+ * (complex arrays as interleaved doubles); returns doubles copied or -1. */
+long td1c_gpu_debug_get(const char* name, double* out, long capacity);
+
+/* Device-resident RK4 propagation (clcrk::prop with the standard tableau,
+ * src/prop/clcrk.cpp:55-87,221-235, plus wfn_mask after every step).
+ * d_wfn / d_cic are device buffers updated in place.  The sin^2 pulse is
+ * evaluated on the host at every stage time (clfield1 velocity1/length1)
+ * and staged in device memory once per call; steps run as one CUDA graph
+ * per step when use_graph != 0. */
+int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep,
+                 double fint, double wlen, double numcyc, double cep, int use_graph);
+/* Synchronise the library stream. */
+int td1c_gpu_sync(void);
+/* Number of kernel launches issued by the last td1c_gpu_rk4 call. */
+long td1c_gpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

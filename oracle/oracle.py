@@ -1,0 +1,159 @@
+"""ctypes wrapper of the CPU oracle (liboracle built by oracle/Makefile).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference leg of bench.py.  The product package never imports
+this module.  See td1c_oracle.h for the restated reference routines and for
+why parity against the reference binary is unpinned.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libtd1c_oracle.so")
+_lib = None
+
+
+def build():
+    """Compile the oracle with its Makefile (system g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    lib.orc_create.restype = vp
+    lib.orc_create.argtypes = [ctypes.POINTER(OrcConfig)]
+    lib.orc_destroy.argtypes = [vp]
+    lib.orc_dims.argtypes = [vp, ip]
+    lib.orc_get.restype = ctypes.c_long
+    lib.orc_get.argtypes = [vp, ctypes.c_char_p, dp]
+    lib.orc_set_wfn0.argtypes = [vp, dp, dp]
+    lib.orc_htot.argtypes = [vp, ctypes.c_double, dp, dp, dp, dp, dp]
+    lib.orc_energies.argtypes = [vp, dp]
+    lib.orc_field.argtypes = [ctypes.POINTER(OrcPulse), ctypes.c_double, dp]
+    lib.orc_rk4.argtypes = [vp, ctypes.POINTER(OrcPulse), ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp]
+    lib.orc_dipole.restype = ctypes.c_double
+    lib.orc_dipole.argtypes = [vp, dp, dp]
+    lib.orc_num_threads.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+class OrcConfig(ctypes.Structure):
+    _fields_ = [
+        ("znuc", ctypes.c_double), ("rmin", ctypes.c_double), ("rmax", ctypes.c_double),
+        ("ndvr", ctypes.c_int), ("nfe", ctypes.c_int),
+        ("lmax1", ctypes.c_int), ("lmax2", ctypes.c_int), ("nlat", ctypes.c_int),
+        ("nfun", ctypes.c_int),
+        ("otype", ctypes.POINTER(ctypes.c_int)), ("mval", ctypes.POINTER(ctypes.c_int)),
+        ("lval", ctypes.POINTER(ctypes.c_int)),
+        ("nela", ctypes.c_int), ("nelb", ctypes.c_int), ("mtot", ctypes.c_int), ("smul", ctypes.c_int),
+        ("igauge", ctypes.c_int), ("icomp", ctypes.c_int),
+        ("rmask", ctypes.c_double), ("mask_cos_order", ctypes.c_double),
+    ]
+
+
+class OrcPulse(ctypes.Structure):
+    _fields_ = [("fint", ctypes.c_double), ("wlen", ctypes.c_double), ("numcyc", ctypes.c_double),
+                ("cep", ctypes.c_double), ("igauge", ctypes.c_int)]
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+DIM_NAMES = ["nrad", "nbas", "nbas2", "ngrid", "nlat", "lcic", "nfcore", "ndcore", "nact",
+             "ncore", "nstr_a", "nstr_b", "ndvr", "lmax1", "lmax2", "nfun"]
+
+
+class Oracle:
+    """One oracle instance for a workload dict (see td1c_b200.workloads)."""
+
+    def __init__(self, wl):
+        self.lib = _load()
+        self.wl = dict(wl)
+        orbs = wl["orbitals"]
+        self._ot = (ctypes.c_int * len(orbs))(*[o[3] for o in orbs])
+        self._mv = (ctypes.c_int * len(orbs))(*[o[2] for o in orbs])
+        self._lv = (ctypes.c_int * len(orbs))(*[o[1] for o in orbs])
+        cfg = OrcConfig(
+            znuc=wl["znuc"], rmin=wl["rmin"], rmax=wl["rmax"], ndvr=wl["ndvr"], nfe=wl["nfe"],
+            lmax1=wl["lmax1"], lmax2=wl["lmax2"], nlat=wl.get("nlat", 0) or 0, nfun=len(orbs),
+            otype=self._ot, mval=self._mv, lval=self._lv, nela=wl["nela"], nelb=wl["nelb"],
+            mtot=wl.get("mtot", 0), smul=wl.get("smul", 1), igauge=wl["igauge"], icomp=wl.get("icomp", 1),
+            rmask=wl["rmask"], mask_cos_order=wl["mask_cos_order"])
+        self.h = self.lib.orc_create(ctypes.byref(cfg))
+        d = (ctypes.c_int * 16)()
+        self.lib.orc_dims(self.h, d)
+        self.dims = dict(zip(DIM_NAMES, list(d)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def get(self, name, complex_=None):
+        n = self.lib.orc_get(self.h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        self.lib.orc_get(self.h, name.encode(), _dp(out))
+        if complex_:
+            out = out.view(np.complex128)
+        return out
+
+    def set_wfn0(self, wfn, cic):
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
+        cic = np.ascontiguousarray(cic, dtype=np.complex128)
+        self.lib.orc_set_wfn0(self.h, _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)))
+
+    def htot(self, dtime, lfield, wfn, cic):
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
+        cic = np.ascontiguousarray(cic, dtype=np.complex128)
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        hw = np.zeros_like(wfn)
+        hc = np.zeros_like(cic)
+        self.lib.orc_htot(self.h, float(dtime), _dp(lf), _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)),
+                          _dp(hw.view(np.float64)), _dp(hc.view(np.float64)))
+        return hw, hc
+
+    def energies(self):
+        e = np.zeros(5)
+        self.lib.orc_energies(self.h, _dp(e))
+        return dict(zip(["ene_fcore", "ene_dcore", "ene_core", "ene_act", "ene_tot"], e.tolist()))
+
+    def pulse(self):
+        wl = self.wl
+        return OrcPulse(fint=wl["fint"], wlen=wl["wlen"], numcyc=wl["numcyc"], cep=wl.get("cep", 0.0),
+                        igauge=wl["igauge"])
+
+    def field(self, t):
+        lf = np.zeros(9)
+        p = self.pulse()
+        self.lib.orc_field(ctypes.byref(p), float(t), _dp(lf))
+        return lf
+
+    def rk4(self, wfn, cic, t0, dt, nstep):
+        wfn = np.array(wfn, dtype=np.complex128, copy=True)
+        cic = np.array(cic, dtype=np.complex128, copy=True)
+        dip = np.zeros(nstep)
+        p = self.pulse()
+        self.lib.orc_rk4(self.h, ctypes.byref(p), float(t0), float(dt), int(nstep), _dp(wfn.view(np.float64)),
+                         _dp(cic.view(np.float64)), _dp(dip))
+        return wfn, cic, dip
+
+    def dipole(self, wfn, cic):
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
+        cic = np.ascontiguousarray(cic, dtype=np.complex128)
+        return self.lib.orc_dipole(self.h, _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)))
+
+    def num_threads(self):
+        return self.lib.orc_num_threads()

@@ -1,0 +1,1364 @@
+// td1c_oracle.cpp -- CPU oracle: C++17/OpenMP restatement of td1c's
+// orbital-equation right-hand side (hprod_htot) and its set-up.
+//
+// TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+// cpu_baseline leg of bench.py as the checker and the timed CPU baseline.  The
+// product (td1c_b200) never links or loads it.  Parity against the reference
+// binary is unpinned (the reference cannot be built here and has no golden
+// outputs); the restatement is pinned by analytic known-answer tests instead.
+//
+// Each routine cites the reference file:line it restates (paths relative to
+// the td1c source tree).  Only the branches used by the orbital-equation hot
+// path are restated: ecs_flag = 0, exact3j = false, dft_type = 0, no PSP/SAE,
+// fedvr_normalized = true, jfc_implicit = xfc_implicit = true, iprojfc = 2,
+// ioorot = 0 / isplit = 0 (full-H RK), nsub = 1 (CAS), thradfc < 0
+// (nradfc = nrad - 1), frozen cores of type -1 only.
+//
+// CI vector layout (ormas_madapt.F90 restated): alpha and beta strings are
+// bit masks over the active orbitals, each list sorted by (M, mask value).
+// Determinant (Ia, Ib) is allowed when M(Ia) + M(Ib) = mtot; the vector is
+// ordered by beta string, and within a beta string by the allowed alpha
+// strings in list order.  Creation operators are ordered alpha block first,
+// each block by increasing orbital index.
+#include "td1c_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using cd = std::complex<double>;
+using ld = long double;
+const double PI = 3.14159265358979323846264338327950288;
+const cd IU(0.0, 1.0);
+const double THRWFN = 1.0e-15;   // mod_const.F90:32
+const double THROCC1 = 1.0e-15;  // clcontrol.cpp throcc1 default
+const double THROCC2 = 1.0e-15;  // clcontrol.cpp throcc2 default
+
+// ---------------------------------------------------------------------------
+// Legendre helpers
+// ---------------------------------------------------------------------------
+// P_n(x) and P_n'(x) by the three-term recurrence (cldvr.cpp:159-185).
+static void legendre_pd(int n, ld x, ld& p, ld& dp) {
+  if (n == 0) { p = 1; dp = 0; return; }
+  ld p0 = 1, p1 = x;
+  for (int k = 2; k <= n; ++k) {
+    ld p2 = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+    p0 = p1; p1 = p2;
+  }
+  p = p1;
+  // P_n'(x) = n (x P_n - P_{n-1}) / (x^2 - 1)
+  dp = (std::fabs((double)(x * x - 1)) > 0) ? n * (x * p1 - p0) / (x * x - 1) : 0;
+}
+
+// Gauss-Lobatto nodes on [-1,1] (cldvr.cpp:82-139 finds the interior nodes as
+// eigenvalues of a Jacobi matrix with dsyev; here Newton on P_n'(x) = 0 gives
+// the same nodes to rounding) and weights (cldvr.cpp:140-158).
+static void gauss_lobatto(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n + 1, 0.0); w.assign(n + 1, 0.0);
+  x[0] = -1.0; x[n] = 1.0;
+  for (int k = 1; k < n; ++k) {
+    ld z = -std::cos(PI * (ld)k / (ld)n);
+    for (int it = 0; it < 100; ++it) {
+      ld p, dp; legendre_pd(n, z, p, dp);
+      ld d2p = (2 * z * dp - (ld)n * (n + 1) * p) / (1 - z * z);
+      ld dz = dp / d2p;
+      z -= dz;
+      if (std::fabs((double)dz) < 1e-19) break;
+    }
+    x[k] = (double)z;
+  }
+  const double scale = 2.0 / ((double)n * (n + 1));
+  w[0] = scale; w[n] = scale;
+  for (int k = 1; k < n; ++k) {
+    ld p, dp; legendre_pd(n, std::fabs((ld)x[k]), p, dp);
+    w[k] = (double)(scale / (p * p));
+  }
+}
+
+// Gauss-Legendre nodes (ascending cos theta) and weights: SHGLQ's quadrature
+// (sph_gen.F90:37).
+static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0); w.assign(n, 0.0);
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    ld z = std::cos(PI * (i + 0.75L) / (n + 0.5L));
+    ld p = 0, dp = 1;
+    for (int it = 0; it < 100; ++it) {
+      legendre_pd(n, z, p, dp);
+      ld dz = p / dp;
+      z -= dz;
+      if (std::fabs((double)dz) < 1e-19) break;
+    }
+    legendre_pd(n, z, p, dp);
+    ld wt = 2 / ((1 - z * z) * dp * dp);
+    x[n - 1 - i] = (double)z; x[i] = (double)(-z);
+    w[n - 1 - i] = (double)wt; w[i] = (double)wt;
+  }
+}
+
+// Normalised associated Legendre functions with the Condon-Shortley phase,
+// int_{-1}^{1} Th_lm(x)^2 dx = 1: SHTOOLS orthonormalised, complex
+// normalisation, csphase = -1, times sqrt(2 pi) (sph_gen.F90:37,62-86).
+// out[l] = Th_{l,m}(x) for l = m..lmax (0 below m).
+static void assoc_legendre(int lmax, int m, ld x, std::vector<ld>& out) {
+  out.assign(lmax + 1, 0);
+  if (m > lmax) return;
+  ld s = std::sqrt(std::max((ld)0, 1 - x * x));
+  ld pmm = std::sqrt((ld)0.5);
+  for (int k = 1; k <= m; ++k) pmm = -std::sqrt((2 * k + 1) / (ld)(2 * k)) * s * pmm;
+  out[m] = pmm;
+  if (m + 1 > lmax) return;
+  ld p1 = std::sqrt((ld)(2 * m + 3)) * x * pmm;
+  out[m + 1] = p1;
+  ld pm2 = pmm, pm1 = p1;
+  for (int l = m + 2; l <= lmax; ++l) {
+    ld a = std::sqrt((4 * (ld)l * l - 1) / ((ld)l * l - (ld)m * m));
+    ld b = std::sqrt((((ld)(l - 1) * (l - 1)) - (ld)m * m) / (4 * (ld)(l - 1) * (l - 1) - 1));
+    ld p = a * (x * pm1 - b * pm2);
+    out[l] = p;
+    pm2 = pm1; pm1 = p;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Banded Cholesky (LAPACK dpbtrf/dpbtrs 'L', restated from the published
+// algorithm).  Storage ab[(i-j) + (kd+1)*j] = A(i,j), j <= i <= j+kd.
+// ---------------------------------------------------------------------------
+static int band_cholesky(int n, int kd, double* ab) {
+  const int ld1 = kd + 1;
+  for (int j = 0; j < n; ++j) {
+    double d = ab[ld1 * j];
+    for (int k = std::max(0, j - kd); k < j; ++k) { double v = ab[(j - k) + ld1 * k]; d -= v * v; }
+    if (!(d > 0)) return j + 1;
+    d = std::sqrt(d);
+    ab[ld1 * j] = d;
+    for (int i = j + 1; i <= std::min(n - 1, j + kd); ++i) {
+      double s = ab[(i - j) + ld1 * j];
+      for (int k = std::max(0, i - kd); k < j; ++k) s -= ab[(i - k) + ld1 * k] * ab[(j - k) + ld1 * k];
+      ab[(i - j) + ld1 * j] = s / d;
+    }
+  }
+  return 0;
+}
+static void band_solve(int n, int kd, const double* ab, double* b) {
+  const int ld1 = kd + 1;
+  for (int j = 0; j < n; ++j) {
+    double s = b[j];
+    for (int k = std::max(0, j - kd); k < j; ++k) s -= ab[(j - k) + ld1 * k] * b[k];
+    b[j] = s / ab[ld1 * j];
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    double s = b[j];
+    for (int i = std::min(n - 1, j + kd); i >= j + 1; --i) s -= ab[(i - j) + ld1 * j] * b[i];
+    b[j] = s / ab[ld1 * j];
+  }
+}
+
+// Regularised inverse of a Hermitian matrix: U diag(d/(d^2+thr)) U^H
+// (hprod_invden.F90:62-107; zheev replaced by a cyclic complex Jacobi).
+static void herm_reg_inverse(int n, double thr, const cd* a, cd* inva) {
+  std::vector<cd> A(a, a + n * n), V(n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + n * i] = 1.0;
+  auto at = [&](int i, int j) -> cd& { return A[i + n * j]; };
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0, diag = 0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        if (i != j) off += std::norm(at(i, j)); else diag += std::norm(at(i, j));
+      }
+    if (off <= 1e-32 * std::max(diag, 1e-300)) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double b = std::abs(at(p, q));
+        if (b < 1e-300) continue;
+        cd e = at(p, q) / b;  // e^{i phi}
+        double app = at(p, p).real(), aqq = at(q, q).real();
+        double tau = (aqq - app) / (2 * b);
+        double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1 + tau * tau));
+        double c = 1 / std::sqrt(1 + t * t), s = t * c;
+        cd em = std::conj(e);
+        for (int k = 0; k < n; ++k) {  // columns: A <- A U
+          cd akp = at(k, p), akq = at(k, q);
+          at(k, p) = c * akp - s * em * akq;
+          at(k, q) = s * akp + c * em * akq;
+          cd vkp = V[k + n * p], vkq = V[k + n * q];
+          V[k + n * p] = c * vkp - s * em * vkq;
+          V[k + n * q] = s * vkp + c * em * vkq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows: A <- U^H A
+          cd apk = at(p, k), aqk = at(q, k);
+          at(p, k) = c * apk - s * e * aqk;
+          at(q, k) = s * apk + c * e * aqk;
+        }
+      }
+  }
+  for (int i = 0; i < n * n; ++i) inva[i] = 0.0;
+  for (int k = 0; k < n; ++k) {
+    double d = at(k, k).real();
+    double invd = thr > 0 ? d / (d * d + thr) : 1.0 / d;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) inva[i + n * j] += V[i + n * k] * invd * std::conj(V[j + n * k]);
+  }
+}
+
+static int popcount(unsigned v) { return __builtin_popcount(v); }
+
+// ---------------------------------------------------------------------------
+// Oracle state
+// ---------------------------------------------------------------------------
+struct Oracle {
+  // configuration
+  orc_config cfg{};
+  std::vector<int> otype, mval, lval;
+  int nfun = 0, nfcore = 0, ndcore = 0, nact = 0, ncore = 0;
+  int nela = 0, nelb = 0, nelact_a = 0, nelact_b = 0, neltot = 0;
+  int mmax1 = 0, mmax2 = 0;
+  // radial grid (clfedvr.cpp)
+  int nfe = 0, nd = 0, nrad = 0, Nr = 0;
+  std::vector<double> xrad, wrad, mask, radk, radk0, radp;  // radk: (2nd+1)*(nrad+1)
+  // angular grid (clsph.cpp / sph_gen.F90)
+  int lmax1 = 0, lmax2 = 0, L1 = 0, L2 = 0, nlat = 0;
+  std::vector<double> cost, wlat, legf1, legb1, legf2, legb2;
+  // operator tables (bas_gen_*.F90)
+  std::vector<double> tmat;   // (2nd+1, Nr, L1) real (ecs_flag = 0)
+  std::vector<double> pmat;   // (2nd+1, Nr)
+  std::vector<double> d2ll;   // (nd+1, Nr, L2) Cholesky factor
+  std::vector<double> alph;   // alph_lm(l, m) at [(m+mmax1)*L1 + l]
+  std::vector<double> d2rpl0, d2rpl1, d2invr, d2fac2, d2fac1;  // (Nr, L2) and (L2)
+  int nbas = 0, nbas2 = 0, ngrid = 0;
+  // CI (ormas_*)
+  std::vector<unsigned> stra, strb;     // strings sorted by (M, mask)
+  std::vector<int> Ma, Mb;
+  std::vector<int> idx_a, idx_b;        // mask -> string index (-1 if none)
+  std::vector<int> detoff;              // per beta string: offset of its block, or -1
+  std::vector<int> afirst, acount;      // per beta string: first allowed alpha string, count
+  int lcic = 1;
+  bool spin_sym = false;
+  // state
+  std::vector<cd> orb0;  // stored wfn for frozen core (hprod_set_wfn0)
+  std::vector<cd> v2jfc;
+  double ene_fcore = 0, ene_dcore = 0, ene_core = 0, ene_act = 0, ene_tot = 0;
+  // scratch (mod_hprod.F90)
+  std::vector<cd> orb, orbg, h0orb, h1orb, gorb, gorbg, v2orb, v2orbg, torbg;
+  std::vector<cd> rho2, v2sph, v2ang, rho2g;
+  std::vector<cd> den1, den2, rden, rrden, int1e, int2e, xmat, fmat, bmat, dcic;
+
+  // ---- index helpers -------------------------------------------------------
+  size_t io(int irad, int l, int f) const { return ((size_t)f * L1 + l) * Nr + irad; }        // orb(irad,l,f), irad 0-based
+  size_t ig(int irad, int t, int f) const { return ((size_t)f * nlat + t) * Nr + irad; }     // orbg(irad,ilat,f)
+  size_t isp(int irad, int l, int j, int i) const { return (((size_t)i * nfun + j) * L2 + l) * Nr + irad; }  // rho2(irad,l,j,i)
+  size_t ian(int irad, int t, int j, int i) const { return (((size_t)i * nfun + j) * nlat + t) * Nr + irad; } // v2ang(irad,ilat,j,i)
+  double lf1(int l, int t, int m) const { return legf1[((size_t)(m + mmax1) * nlat + t) * L1 + l]; }
+  double lb1(int t, int l, int m) const { return legb1[((size_t)(m + mmax1) * L1 + l) * nlat + t]; }
+  double lf2(int l, int t, int m) const { return legf2[((size_t)(m + mmax2) * nlat + t) * L2 + l]; }
+  double lb2(int t, int l, int m) const { return legb2[((size_t)(m + mmax2) * L2 + l) * nlat + t]; }
+  double& RK(std::vector<double>& a, int jb, int irad) { return a[(size_t)(2 * nd + 1) * irad + jb]; }  // radk(jb+1, irad)
+  cd& D1(std::vector<cd>& a, int i, int j) { return a[i + nact * j]; }
+  cd& D2(std::vector<cd>& a, int i, int j, int k, int l) { return a[i + nact * (j + nact * (k + nact * l))]; }
+
+  // =========================================================================
+  // Set-up
+  // =========================================================================
+  void setup(const orc_config* c) {
+    cfg = *c;
+    nfun = c->nfun;
+    otype.assign(c->otype, c->otype + nfun);
+    mval.assign(c->mval, c->mval + nfun);
+    lval.assign(c->lval, c->lval + nfun);
+    for (int i = 0; i < nfun; ++i) {
+      if (otype[i] == -1) nfcore++;
+      else if (otype[i] == 0) ndcore++;
+      else if (otype[i] == 1) nact++;
+      else { fprintf(stderr, "oracle: unsupported orbital type %d\n", otype[i]); abort(); }
+      if (i > 0 && otype[i] < otype[i - 1]) { fprintf(stderr, "oracle: orbitals must be ordered fc, dc, act\n"); abort(); }
+    }
+    ncore = nfcore + ndcore;
+    nela = c->nela; nelb = c->nelb; neltot = nela + nelb;
+    nelact_a = nela - ncore; nelact_b = nelb - ncore;
+    for (int i = 0; i < nfun; ++i) mmax1 = std::max(mmax1, std::abs(mval[i]));
+    mmax2 = 2 * mmax1;  // clsph.cpp:101
+    gen_radial();
+    gen_angular();
+    nbas = Nr * L1; nbas2 = Nr * L2; ngrid = Nr * nlat;  // clbas.cpp:87-89
+    gen_tables();
+    gen_ci();
+    size_t so = (size_t)nbas * nfun, sg = (size_t)ngrid * nfun;
+    orb.assign(so, 0.0); h0orb.assign(so, 0.0); h1orb.assign(so, 0.0); gorb.assign(so, 0.0); v2orb.assign(so, 0.0);
+    orbg.assign(sg, 0.0); gorbg.assign(sg, 0.0); v2orbg.assign(sg, 0.0); torbg.assign(sg, 0.0);
+    rho2.assign((size_t)nbas2 * nfun * nfun, 0.0); v2sph.assign((size_t)nbas2 * nfun * nfun, 0.0);
+    v2ang.assign((size_t)ngrid * nfun * nfun, 0.0); rho2g.assign((size_t)ngrid * nfun * nfun, 0.0);
+    int na = std::max(nact, 1);
+    den1.assign(na * na, 0.0); rden.assign(na * na, 0.0); rrden.assign(na * na, 0.0); int1e.assign(na * na, 0.0);
+    den2.assign((size_t)na * na * na * na, 0.0); int2e.assign((size_t)na * na * na * na, 0.0);
+    xmat.assign(nfun * nfun, 0.0); fmat.assign(nfun * nfun, 0.0); bmat.assign(nfun * nfun, 0.0);
+    dcic.assign(lcic, 0.0);
+    orb0.assign(so, 0.0);
+    v2jfc.assign(Nr, 0.0);
+  }
+
+  // clfedvr.cpp:197-338 (read_x, gen_map, gen_grid), 361-398 (gen_mask),
+  // 676-793 (gen_radk, gen_radp); cldvr.cpp:57-222 (Lobatto DVR).
+  void gen_radial() {
+    nfe = cfg.nfe; nd = cfg.ndvr; nrad = nd * nfe; Nr = nrad - 1;
+    std::vector<double> x01, w01; gauss_lobatto(nd, x01, w01);
+    const double dfe = (cfg.rmax - cfg.rmin) / nfe;
+    std::vector<std::vector<double>> xe(nfe), we(nfe), dsh(nfe);
+    for (int i = 0; i < nfe; ++i) {
+      double x0 = cfg.rmin + dfe * i, x1 = x0 + dfe;
+      double len = 0.5 * (x1 - x0), mid = 0.5 * (x1 + x0);
+      xe[i].resize(nd + 1); we[i].resize(nd + 1);
+      for (int k = 0; k <= nd; ++k) { xe[i][k] = x01[k] * len + mid; we[i][k] = w01[k] * len; }
+      // dshape[(n+1)*m + k] = f_m'(x_k) (cldvr.cpp:186-215)
+      dsh[i].assign((nd + 1) * (nd + 1), 0.0);
+      const auto& xp = xe[i];
+      for (int m = 0; m <= nd; ++m)
+        for (int k = 0; k <= nd; ++k) {
+          if (m == k) continue;
+          double d = 1.0 / (xp[m] - xp[k]);
+          for (int l = 0; l <= nd; ++l)
+            if (l != m && l != k) d *= (xp[k] - xp[l]) / (xp[m] - xp[l]);
+          dsh[i][(nd + 1) * m + k] = d;
+        }
+      dsh[i][0] = -0.5 / we[i][0];
+      dsh[i][(nd + 1) * (nd + 1) - 1] = 0.5 / we[i][nd];
+    }
+    xrad.assign(nrad + 1, 0.0); wrad.assign(nrad + 1, 0.0);
+    for (int iB = 0; iB <= nrad; ++iB) {
+      int i = std::min(iB / nd, nfe - 1), m = iB - nd * i;
+      xrad[iB] = xe[i][m]; wrad[iB] = we[i][m];
+    }
+    for (int i = 1; i < nfe; ++i) wrad[nd * i] += we[i - 1][nd];  // bridge weights
+    // mask (clfedvr.cpp:361-398)
+    mask.assign(nrad + 1, 0.0);
+    double order = cfg.mask_cos_order > 0 ? 1.0 / cfg.mask_cos_order : std::fabs(cfg.mask_cos_order);
+    const double rul = cfg.rmax;
+    for (int iB = 1; iB < nrad; ++iB) {
+      double ax = std::fabs(xrad[iB]);
+      mask[iB] = ax <= cfg.rmask ? 1.0 : std::pow(std::cos(0.5 * PI * (ax - cfg.rmask) / (rul - cfg.rmask)), order);
+    }
+    // radk / radk0 / radp (band (2nd+1) x (nrad+1))
+    const int bw = 2 * nd + 1;
+    radk.assign((size_t)bw * (nrad + 1), 0.0);
+    radk0.assign((size_t)bw * (nrad + 1), 0.0);
+    radp.assign((size_t)bw * (nrad + 1), 0.0);
+    for (int i = 0; i < nfe; ++i) {
+      const int iB0 = nd * i;
+      for (int m = 0; m <= nd; ++m)
+        for (int k = 0; k <= nd; ++k) {
+          int mB = iB0 + m, kB = iB0 + k;
+          size_t kmB = (size_t)bw * mB + nd + kB - mB;
+          if ((i == 0 && (m == 0 || k == 0)) || (i == nfe - 1 && (m == nd || k == nd))) continue;
+          double t = 0, t0 = 0;
+          for (int l = 0; l <= nd; ++l) {
+            double v = we[i][l] * dsh[i][(nd + 1) * m + l] * dsh[i][(nd + 1) * k + l];
+            t += v;
+            if (!(i == 0 && l == 0)) t0 += v;
+          }
+          double nrm = std::sqrt(wrad[mB] * wrad[kB]);
+          radk[kmB] += 0.5 * t / nrm;
+          radk0[kmB] += 0.5 * t0 / nrm;
+          radp[kmB] += we[i][m] * dsh[i][(nd + 1) * k + m] / nrm;
+        }
+    }
+  }
+
+  // clsph.cpp:97-134, sph_gen.F90:2-115
+  void gen_angular() {
+    lmax1 = cfg.lmax1; lmax2 = cfg.lmax2; L1 = lmax1 + 1; L2 = lmax2 + 1;
+    nlat = cfg.nlat > 0 ? cfg.nlat : lmax2 + 1;
+    gauss_legendre(nlat, cost, wlat);
+    legf1.assign((size_t)nlat * L1 * (2 * mmax1 + 1), 0.0);
+    legb1.assign(legf1.size(), 0.0);
+    legf2.assign((size_t)nlat * L2 * (2 * mmax2 + 1), 0.0);
+    legb2.assign(legf2.size(), 0.0);
+    std::vector<ld> th;
+    for (int m = -mmax2; m <= mmax2; ++m)
+      for (int t = 0; t < nlat; ++t) {
+        assoc_legendre(lmax2, std::abs(m), (ld)cost[t], th);
+        for (int l = std::abs(m); l <= lmax2; ++l) {
+          legf2[((size_t)(m + mmax2) * nlat + t) * L2 + l] = (double)th[l];
+          legb2[((size_t)(m + mmax2) * L2 + l) * nlat + t] = (double)(th[l] * (ld)wlat[t]);
+        }
+        if (std::abs(m) <= mmax1)
+          for (int l = std::abs(m); l <= lmax1; ++l) {
+            legf1[((size_t)(m + mmax1) * nlat + t) * L1 + l] = (double)th[l];
+            legb1[((size_t)(m + mmax1) * L1 + l) * nlat + t] = (double)(th[l] * (ld)wlat[t]);
+          }
+      }
+  }
+
+  // bas_gen_alph.F90:2-26, bas_gen_tmat.F90:2-75 (ecs_flag 0),
+  // bas_gen_pmat.F90:2-25, bas_gen_d2ll.F90:2-140, bas_gen_d2fac.F90:2-60
+  void gen_tables() {
+    const int bw = 2 * nd + 1;
+    alph.assign((size_t)L1 * (2 * mmax1 + 1), 0.0);
+    for (int m = -mmax1; m <= mmax1; ++m)
+      for (int l = std::abs(m); l <= lmax1; ++l)
+        alph[(m + mmax1) * L1 + l] = std::sqrt(((l + 1.0) * (l + 1.0) - (double)m * m) / ((2.0 * l + 1) * (2.0 * l + 3)));
+    tmat.assign((size_t)bw * Nr * L1, 0.0);
+    for (int l = 0; l <= lmax1; ++l) {
+      double l2 = (double)l * (l + 1);
+      for (int ir = 1; ir <= Nr; ++ir) {
+        double oor = 1.0 / xrad[ir];
+        tmat[((size_t)l * Nr + ir - 1) * bw + nd] = oor * (-cfg.znuc + l2 * oor * 0.5);
+      }
+      std::vector<double>& rk = (l == 0) ? radk : radk0;
+      for (int ir = 1; ir <= Nr; ++ir) {
+        int jll = std::max(1, ir - nd), jul = std::min(Nr, ir + nd);
+        for (int jr = jll; jr <= jul; ++jr) {
+          int jb = nd + jr - ir;
+          tmat[((size_t)l * Nr + ir - 1) * bw + jb] += rk[(size_t)bw * ir + jb];
+        }
+      }
+    }
+    pmat.assign((size_t)bw * Nr, 0.0);
+    for (int ir = 1; ir <= Nr; ++ir) {
+      int jll = std::max(1, ir - nd), jul = std::min(Nr, ir + nd);
+      for (int jr = jll; jr <= jul; ++jr) {
+        int jb = nd + jr - ir;
+        pmat[(size_t)(ir - 1) * bw + jb] = radp[(size_t)bw * ir + jb];
+      }
+    }
+    const int ld1 = nd + 1;
+    d2ll.assign((size_t)ld1 * Nr * L2, 0.0);
+    for (int l = 0; l <= lmax2; ++l) {
+      double* ab = &d2ll[(size_t)l * ld1 * Nr];
+      double l2 = (double)l * (l + 1);
+      for (int ir = 1; ir <= Nr; ++ir) {
+        double ak = 1.0 / xrad[ir];
+        ab[(size_t)ld1 * (ir - 1)] = ak * ak * l2;
+      }
+      for (int ir = 1; ir <= Nr; ++ir) {
+        int jul = std::min(Nr, ir + nd);
+        for (int jr = ir; jr <= jul; ++jr) {
+          int jb1 = jr - ir + nd, jb2 = jr - ir;
+          ab[(size_t)ld1 * (ir - 1) + jb2] += 2.0 * radk[(size_t)bw * ir + jb1];
+        }
+      }
+      int info = band_cholesky(Nr, nd, ab);
+      if (info != 0) { fprintf(stderr, "oracle: d2ll Cholesky failed l=%d info=%d\n", l, info); abort(); }
+    }
+    const double r2pi = 0.5 / PI;
+    d2rpl0.assign((size_t)Nr * L2, 0.0); d2rpl1.assign(d2rpl0.size(), 0.0);
+    d2invr.assign(d2rpl0.size(), 0.0); d2fac2.assign(d2rpl0.size(), 0.0);
+    d2fac1.assign(L2, 0.0);
+    for (int l = 0; l <= lmax2; ++l) {
+      for (int ir = 1; ir <= Nr; ++ir) {
+        double x = xrad[ir], sw = std::sqrt(wrad[ir]);
+        size_t k = (size_t)l * Nr + ir - 1;
+        double xl = 1.0; for (int e = 0; e < l; ++e) xl *= x;
+        d2rpl0[k] = xl * r2pi;
+        d2rpl1[k] = xl * x * sw;
+        d2invr[k] = (2 * l + 1) / (x * sw) * r2pi;
+        d2fac2[k] = 4.0 * PI / (2 * l + 1) / (x * sw);
+      }
+      double xr = xrad[Nr + 1], p = 1.0;
+      for (int e = 0; e < 2 * l + 1; ++e) p *= xr;
+      d2fac1[l] = 1.0 / p;  // hprod_mkv2mf.F90:140-142
+    }
+  }
+
+  // ORMAS CAS string set-up (ormas_init.F90:2-63, ormas_madapt.F90)
+  void gen_ci() {
+    if (nact == 0) { lcic = 1; return; }
+    auto build = [&](int nel, std::vector<unsigned>& s, std::vector<int>& M, std::vector<int>& idx) {
+      std::vector<std::pair<int, unsigned>> tmp;
+      for (unsigned b = 0; b < (1u << nact); ++b) {
+        if (popcount(b) != nel) continue;
+        int mm = 0; for (int a = 0; a < nact; ++a) if (b >> a & 1u) mm += mval[ncore + a];
+        tmp.push_back({mm, b});
+      }
+      std::sort(tmp.begin(), tmp.end());
+      s.clear(); M.clear(); idx.assign(1u << nact, -1);
+      for (size_t k = 0; k < tmp.size(); ++k) { s.push_back(tmp[k].second); M.push_back(tmp[k].first); idx[tmp[k].second] = (int)k; }
+    };
+    build(nelact_a, stra, Ma, idx_a);
+    build(nelact_b, strb, Mb, idx_b);
+    detoff.assign(strb.size(), -1); afirst.assign(strb.size(), 0); acount.assign(strb.size(), 0);
+    int off = 0;
+    for (size_t ib = 0; ib < strb.size(); ++ib) {
+      int need = cfg.mtot - Mb[ib];
+      int f = -1, n = 0;
+      for (size_t ia = 0; ia < stra.size(); ++ia) if (Ma[ia] == need) { if (f < 0) f = (int)ia; n++; }
+      if (n > 0) { detoff[ib] = off; afirst[ib] = f; acount[ib] = n; off += n; }
+    }
+    lcic = off;
+    spin_sym = (cfg.smul == 1 && nelact_a == nelact_b);
+  }
+  // index of determinant (alpha string ia, beta string ib), or -1
+  int det_index(int ia, int ib) const {
+    if (ia < 0 || ib < 0 || detoff[ib] < 0) return -1;
+    int p = ia - afirst[ib];
+    if (p < 0 || p >= acount[ib]) return -1;
+    return detoff[ib] + p;
+  }
+  // a^+_p a_q acting on string s: returns new string or ~0u if zero; sign in sg
+  static unsigned excite(unsigned s, int p, int q, int& sg) {
+    if (!(s >> q & 1u)) return ~0u;
+    unsigned t = s & ~(1u << q);
+    if (t >> p & 1u) return ~0u;
+    int lo = std::min(p, q), hi = std::max(p, q);
+    unsigned between = (hi - lo > 1) ? (t & (((1u << hi) - 1u) & ~((1u << (lo + 1)) - 1u))) : 0u;
+    sg = (popcount(between) & 1) ? -1 : 1;
+    return t | (1u << p);
+  }
+
+  // =========================================================================
+  // RHS pieces
+  // =========================================================================
+  // bas_sph2ang1_dyn (bas_sph2ang1.F90:88-156): orbg = sum_l orb * legf1
+  void sph2ang1(const std::vector<cd>& o, std::vector<cd>& og, int f) {
+    const int m = mval[f];
+    for (int t = 0; t < nlat; ++t) {
+      cd* dst = &og[ig(0, t, f)];
+      for (int ir = 0; ir < Nr; ++ir) dst[ir] = 0.0;
+      for (int l = std::abs(m); l <= lmax1; ++l) {
+        double w = lf1(l, t, m);
+        const cd* src = &o[io(0, l, f)];
+        for (int ir = 0; ir < Nr; ++ir) dst[ir] += src[ir] * w;
+      }
+    }
+  }
+  // bas_ang2sph1_dyn (bas_ang2sph1.F90:88-158): orb = sum_theta orbg * legb1
+  void ang2sph1(const std::vector<cd>& og, std::vector<cd>& o, int f) {
+    const int m = mval[f];
+    for (int l = 0; l <= lmax1; ++l) {
+      cd* dst = &o[io(0, l, f)];
+      for (int ir = 0; ir < Nr; ++ir) dst[ir] = 0.0;
+      if (l < std::abs(m)) continue;
+      for (int t = 0; t < nlat; ++t) {
+        double w = lb1(t, l, m);
+        const cd* src = &og[ig(0, t, f)];
+        for (int ir = 0; ir < Nr; ++ir) dst[ir] += src[ir] * w;
+      }
+    }
+  }
+
+  // hprod_orbin.F90:2-105
+  void orbin(const double* lfield, const cd* wfn) {
+    for (int f = nfcore; f < nfun; ++f)
+      std::copy(wfn + (size_t)f * nbas, wfn + (size_t)(f + 1) * nbas, orb.begin() + (size_t)f * nbas);
+#pragma omp parallel for schedule(static)
+    for (int f = nfcore; f < nfun; ++f) sph2ang1(orb, orbg, f);
+    if (nfcore == 0) return;
+    if (cfg.igauge == 0) {
+      std::copy(orb0.begin(), orb0.begin() + (size_t)nfcore * nbas, orb.begin());
+      for (int f = 0; f < nfcore; ++f) sph2ang1(orb, orbg, f);
+    } else {
+      for (int f = 0; f < nfcore; ++f) sph2ang1(orb0, orbg, f);
+      const double A = lfield[8];
+      for (int f = 0; f < nfcore; ++f)
+        for (int t = 0; t < nlat; ++t)
+          for (int ir = 0; ir < Nr; ++ir) {
+            cd fac = std::exp(-IU * (A * xrad[ir + 1] * cost[t]));
+            orbg[ig(ir, t, f)] *= fac;
+          }
+      for (int f = 0; f < nfcore; ++f) ang2sph1(orbg, orb, f);
+    }
+  }
+
+  // hprod_tprod.F90:125-235: h(irad,l) = sum_j tmat(jb,irad,l) wfn(j,l)
+  void tprod(const std::vector<cd>& w, std::vector<cd>& h, int f0, int f1) {
+    const int bw = 2 * nd + 1;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int f = f0; f < f1; ++f)
+      for (int l = 0; l <= lmax1; ++l) {
+        if (l < std::abs(mval[f])) continue;
+        const double* tm = &tmat[(size_t)l * Nr * bw];
+        for (int ir = 1; ir <= Nr; ++ir) {
+          int jll = std::max(1, ir - nd), jul = std::min(Nr, ir + nd);
+          cd s = 0.0;
+          for (int jr = jll; jr <= jul; ++jr) s += w[io(jr - 1, l, f)] * tm[(size_t)(ir - 1) * bw + nd + jr - ir];
+          h[io(ir - 1, l, f)] = s;
+        }
+      }
+  }
+  // hprod_zprod.F90:108-135 (length gauge r*alpha_lm coupling)
+  void zprod(cd zfac, const std::vector<cd>& w, std::vector<cd>& h, int f0, int f1) {
+    for (int f = f0; f < f1; ++f) {
+      int m = mval[f];
+      for (int l = std::abs(m); l <= lmax1 - 1; ++l) {
+        double a = alph[(m + mmax1) * L1 + l];
+        for (int ir = 0; ir < Nr; ++ir) {
+          cd tmp = zfac * (xrad[ir + 1] * a);
+          h[io(ir, l, f)] += w[io(ir, l + 1, f)] * tmp;
+          h[io(ir, l + 1, f)] += w[io(ir, l, f)] * tmp;
+        }
+      }
+    }
+  }
+  // hprod_pzprod.F90:114-213 (velocity gauge)
+  void pzprod(cd zfac, const std::vector<cd>& w, std::vector<cd>& h, int f0, int f1) {
+    const int bw = 2 * nd + 1;
+    std::vector<cd> dw((size_t)Nr * L1);
+    for (int f = f0; f < f1; ++f) {
+      int m = mval[f];
+      std::fill(dw.begin(), dw.end(), cd(0.0));
+      for (int l = std::abs(m); l <= lmax1; ++l)
+        for (int ir = 1; ir <= Nr; ++ir) {
+          int jll = std::max(1, ir - nd), jul = std::min(Nr, ir + nd);
+          cd s = 0.0;
+          for (int jr = jll; jr <= jul; ++jr) s += w[io(jr - 1, l, f)] * pmat[(size_t)(ir - 1) * bw + nd + jr - ir];
+          dw[(size_t)l * Nr + ir - 1] += s;
+        }
+      for (int l = std::abs(m); l <= lmax1 - 1; ++l) {
+        double a = alph[(m + mmax1) * L1 + l];
+        cd t1 = zfac * (-IU * a);
+        for (int ir = 0; ir < Nr; ++ir) {
+          cd t2 = zfac * (-IU * a * (l + 1.0) / xrad[ir + 1]);
+          h[io(ir, l, f)] += dw[(size_t)(l + 1) * Nr + ir] * t1 + w[io(ir, l + 1, f)] * t2;
+          h[io(ir, l + 1, f)] += dw[(size_t)l * Nr + ir] * t1 - w[io(ir, l, f)] * t2;
+        }
+      }
+    }
+  }
+
+  // pair list helpers: 'dyn' pairs (j >= i, both dynamic) and 'fc1dyn'
+  // (i frozen core, j dynamic); hprod_mkrho2.F90:115-197
+  void pairs(const char* type, std::vector<std::pair<int, int>>& out) const {
+    out.clear();
+    std::string t(type);
+    if (t == "dyn") { for (int i = nfcore; i < nfun; ++i) for (int j = i; j < nfun; ++j) out.push_back({j, i}); }
+    else if (t == "fc1dyn") { for (int i = 0; i < nfcore; ++i) for (int j = nfcore; j < nfun; ++j) out.push_back({j, i}); }
+    else if (t == "fcfc") { for (int i = 0; i < nfcore; ++i) for (int j = i; j < nfcore; ++j) out.push_back({j, i}); }
+  }
+  // hprod_mkrho2p + bas_ang2sph2 (bas_ang2sph2.F90:330-482, 590-634)
+  void mkrho2(const char* type) {
+    std::vector<std::pair<int, int>> P; pairs(type, P);
+#pragma omp parallel for schedule(dynamic)
+    for (size_t k = 0; k < P.size(); ++k) {
+      int j = P[k].first, i = P[k].second;
+      for (int t = 0; t < nlat; ++t)
+        for (int ir = 0; ir < Nr; ++ir) rho2g[ian(ir, t, j, i)] = std::conj(orbg[ig(ir, t, j)]) * orbg[ig(ir, t, i)];
+      int mji = mval[i] - mval[j];
+      for (int l = 0; l <= lmax2; ++l) {
+        cd* dst = &rho2[isp(0, l, j, i)];
+        for (int ir = 0; ir < Nr; ++ir) dst[ir] = 0.0;
+        if (l < std::abs(mji)) continue;
+        for (int t = 0; t < nlat; ++t) {
+          double w = lb2(t, l, mji);
+          const cd* src = &rho2g[ian(0, t, j, i)];
+          for (int ir = 0; ir < Nr; ++ir) dst[ir] += src[ir] * w;
+        }
+      }
+    }
+  }
+  // hprod_mkv2mf_poissonp (hprod_mkv2mf.F90:118-182)
+  void poisson(const char* type) {
+    std::vector<std::pair<int, int>> P; pairs(type, P);
+    const int dim = Nr, ld1 = nd + 1;
+#pragma omp parallel
+    {
+      std::vector<double> rr(dim), ri(dim);
+#pragma omp for collapse(2) schedule(dynamic)
+      for (size_t k = 0; k < P.size(); ++k)
+        for (int l = 0; l <= lmax2; ++l) {
+          int j = P[k].first, i = P[k].second;
+          int m = mval[j] - mval[i];
+          cd* v = &v2sph[isp(0, l, j, i)];
+          if (l < std::abs(m)) { for (int ir = 0; ir < dim; ++ir) v[ir] = 0.0; continue; }
+          const cd* r = &rho2[isp(0, l, j, i)];
+          const double* rpl0 = &d2rpl0[(size_t)l * Nr];
+          const double* invr = &d2invr[(size_t)l * Nr];
+          double tr = 0, ti = 0;
+          for (int ir = 0; ir < dim; ++ir) {
+            rr[ir] = r[ir].real(); ri[ir] = r[ir].imag();
+            tr += rr[ir] * rpl0[ir]; ti += ri[ir] * rpl0[ir];
+            rr[ir] *= invr[ir]; ri[ir] *= invr[ir];
+          }
+          tr *= d2fac1[l]; ti *= d2fac1[l];
+          const double* ab = &d2ll[(size_t)l * ld1 * Nr];
+          band_solve(dim, nd, ab, rr.data());
+          band_solve(dim, nd, ab, ri.data());
+          const double* rpl1 = &d2rpl1[(size_t)l * Nr];
+          const double* fac2 = &d2fac2[(size_t)l * Nr];
+          for (int ir = 0; ir < dim; ++ir)
+            v[ir] = cd((rr[ir] + tr * rpl1[ir]) * fac2[ir], (ri[ir] + ti * rpl1[ir]) * fac2[ir]);
+        }
+    }
+  }
+  // bas_sph2ang2_dyn/fc1dyn (bas_sph2ang2.F90:334-463, 569-613) and
+  // hprod_mkv2mf_herm (hprod_mkv2mf.F90:257-345)
+  void sph2ang2_herm(const char* type) {
+    std::vector<std::pair<int, int>> P; pairs(type, P);
+#pragma omp parallel for schedule(dynamic)
+    for (size_t k = 0; k < P.size(); ++k) {
+      int j = P[k].first, i = P[k].second;
+      int mji = mval[i] - mval[j];
+      for (int t = 0; t < nlat; ++t) {
+        cd* dst = &v2ang[ian(0, t, j, i)];
+        for (int ir = 0; ir < Nr; ++ir) dst[ir] = 0.0;
+        for (int l = std::abs(mji); l <= lmax2; ++l) {
+          double w = lf2(l, t, mji);
+          const cd* src = &v2sph[isp(0, l, j, i)];
+          for (int ir = 0; ir < Nr; ++ir) dst[ir] += src[ir] * w;
+        }
+      }
+    }
+    for (auto& pr : P) {
+      int j = pr.first, i = pr.second;
+      if (j <= i) continue;
+      for (int l = 0; l <= lmax2; ++l)
+        for (int ir = 0; ir < Nr; ++ir) v2sph[isp(ir, l, i, j)] = std::conj(v2sph[isp(ir, l, j, i)]);
+      for (int t = 0; t < nlat; ++t)
+        for (int ir = 0; ir < Nr; ++ir) v2ang[ian(ir, t, i, j)] = std::conj(v2ang[ian(ir, t, j, i)]);
+    }
+  }
+
+  // hprod_mfprod2.F90:2-34 with its callees (dofc = false)
+  void mfprod2() {
+    const size_t NG = ngrid;
+    auto OG = [&](int f) { return &orbg[(size_t)f * NG]; };
+    auto GG = [&](int f) { return &gorbg[(size_t)f * NG]; };
+    auto VG = [&](int f) { return &v2orbg[(size_t)f * NG]; };
+    auto W = [&](int j, int i) { return &v2ang[ian(0, 0, j, i)]; };
+    // fcx1 (hprod_mfprod2.F90:158-200): nfcore2 = 0, all frozen cores are fc1
+    for (int i = nfcore; i < nfun; ++i)
+      for (int j = 0; j < nfcore; ++j) {
+        cd* g = GG(i); const cd* v = W(j, i); const cd* o = OG(j);
+#pragma omp parallel for
+        for (size_t q = 0; q < NG; ++q) g[q] -= v[q] * o[q];
+      }
+    if (ndcore > 0) {
+      // dcj (242-306)
+      std::vector<cd> d2v(NG, 0.0);
+      for (int j = nfcore; j < ncore; ++j) { const cd* v = W(j, j); for (size_t q = 0; q < NG; ++q) d2v[q] += v[q] * 2.0; }
+      for (int i = nfcore; i < nfun; ++i) { cd* g = GG(i); const cd* o = OG(i); for (size_t q = 0; q < NG; ++q) g[q] += d2v[q] * o[q]; }
+      // dcx (308-366)
+      for (int i = nfcore; i < nfun; ++i)
+        for (int j = nfcore; j < ncore; ++j) {
+          cd* g = GG(i); const cd* v = W(j, i); const cd* o = OG(j);
+          for (size_t q = 0; q < NG; ++q) g[q] -= v[q] * o[q];
+        }
+    }
+    if (ncore > 0 && nact > 0) {
+      // actj (368-437): into v2orbg of dynamic-core orbitals
+      std::vector<cd> d2v(NG, 0.0);
+      for (int ja = 0; ja < nact; ++ja)
+        for (int ka = 0; ka < nact; ++ka) {
+          cd dens = D1(den1, ka, ja); const cd* v = W(ncore + ja, ncore + ka);
+          for (size_t q = 0; q < NG; ++q) d2v[q] += v[q] * dens;
+        }
+      for (int i = nfcore; i < ncore; ++i) { cd* g = VG(i); const cd* o = OG(i); for (size_t q = 0; q < NG; ++q) g[q] += d2v[q] * o[q]; }
+      // actx (439-514)
+      std::vector<cd> wd1(NG);
+      for (int ja = 0; ja < nact; ++ja) {
+        int jf = ncore + ja;
+        std::fill(wd1.begin(), wd1.end(), cd(0.0));
+        for (int ka = 0; ka < nact; ++ka) {
+          int kf = ncore + ka;
+          if (mval[jf] != mval[kf]) continue;
+          cd dens = -D1(den1, ka, ja) * 0.5; const cd* o = OG(kf);
+          for (size_t q = 0; q < NG; ++q) wd1[q] += o[q] * dens;
+        }
+        for (int i = nfcore; i < ncore; ++i) { cd* g = VG(i); const cd* v = W(jf, i); for (size_t q = 0; q < NG; ++q) g[q] += wd1[q] * v[q]; }
+      }
+    }
+    // act2 (619-694): the 2-RDM contraction
+    if (nact > 0 && nelact_a + nelact_b >= 2) {
+      std::fill(torbg.begin(), torbg.end(), cd(0.0));
+      for (int ia = 0; ia < nact; ++ia)
+        for (int ja = 0; ja <= ia; ++ja) {
+          int ifn = ncore + ia, jfn = ncore + ja;
+          std::vector<cd> d2v(NG, 0.0);
+          for (int ka = 0; ka < nact; ++ka)
+            for (int la = 0; la < nact; ++la) {
+              int kfn = ncore + ka, lfn = ncore + la;
+              if (mval[ifn] + mval[kfn] != mval[jfn] + mval[lfn]) continue;
+              cd dens = D2(den2, ja, ia, la, ka);
+              if (std::abs(dens) <= THRWFN) continue;
+              const cd* v = W(kfn, lfn);
+#pragma omp parallel for
+              for (size_t q = 0; q < NG; ++q) d2v[q] += dens * v[q];
+            }
+          cd* ti = &torbg[(size_t)ifn * NG]; const cd* oj = OG(jfn);
+          for (size_t q = 0; q < NG; ++q) ti[q] += oj[q] * d2v[q];
+          if (ia > ja) {
+            cd* tj = &torbg[(size_t)jfn * NG]; const cd* oi = OG(ifn);
+            for (size_t q = 0; q < NG; ++q) tj[q] += oi[q] * std::conj(d2v[q]);
+          }
+        }
+      for (int ia = 0; ia < nact; ++ia)
+        for (int ka = 0; ka < nact; ++ka) {
+          int ifn = ncore + ia, kfn = ncore + ka;
+          if (mval[ifn] != mval[kfn]) continue;
+          cd tmp = D1(rden, ia, ka);
+          cd* g = VG(kfn); const cd* t = &torbg[(size_t)ifn * NG];
+          for (size_t q = 0; q < NG; ++q) g[q] += tmp * t[q];
+        }
+    }
+  }
+
+  // ---- CI: RDMs and sigma (ormas_mkden1_ras.F90, ormas_mkden2_ras.F90,
+  //      ormas_hcic_ras.F90), restated from their definitions -------------
+  // den1(x, y) = <a^+_y a_x> summed over spin
+  void mkden1(const cd* c) {
+    std::fill(den1.begin(), den1.end(), cd(0.0));
+    if (nact == 0) return;
+    for (size_t ib = 0; ib < strb.size(); ++ib) {
+      if (detoff[ib] < 0) continue;
+      for (int p = 0; p < acount[ib]; ++p) {
+        int ia = afirst[ib] + p, I = detoff[ib] + p;
+        cd cI = c[I];
+        for (int y = 0; y < nact; ++y)
+          for (int x = 0; x < nact; ++x) {
+            if (!spin_sym) {
+              int sg; unsigned t = excite(stra[ia], y, x, sg);
+              if (t != ~0u) { int J = det_index(idx_a[t], (int)ib); if (J >= 0) D1(den1, x, y) += std::conj(c[J]) * (double)sg * cI; }
+            }
+            int sg; unsigned t = excite(strb[ib], y, x, sg);
+            if (t != ~0u) { int J = det_index(ia, idx_b[t]); if (J >= 0) D1(den1, x, y) += std::conj(c[J]) * (double)sg * cI * (spin_sym ? 2.0 : 1.0); }
+          }
+      }
+    }
+  }
+  // den2(p,q,r,s) = <a^+_q a^+_s a_r a_p> = <E_qp E_sr> - delta_ps <E_qr>
+  void mkden2(const cd* c) {
+    std::fill(den2.begin(), den2.end(), cd(0.0));
+    if (nact == 0 || nelact_a + nelact_b < 2) return;
+    const int n = nact;
+    // G(p,q,r,s) = <Psi| E_qp E_sr |Psi> = sum conj(c_J) <J|E_qp|K><K|E_sr|I> c_I
+    for (size_t ib = 0; ib < strb.size(); ++ib) {
+      if (detoff[ib] < 0) continue;
+      for (int pp = 0; pp < acount[ib]; ++pp) {
+        int ia = afirst[ib] + pp, I = detoff[ib] + pp;
+        cd cI = c[I];
+        for (int s = 0; s < n; ++s)
+          for (int r = 0; r < n; ++r)
+            for (int sp1 = 0; sp1 < 2; ++sp1) {  // spin of E_sr: 0 alpha, 1 beta
+              int sg1; unsigned ka, kb;
+              if (sp1 == 0) { ka = excite(stra[ia], s, r, sg1); kb = strb[ib]; if (ka == ~0u) continue; }
+              else { kb = excite(strb[ib], s, r, sg1); ka = stra[ia]; if (kb == ~0u) continue; }
+              for (int q = 0; q < n; ++q)
+                for (int p = 0; p < n; ++p)
+                  for (int sp2 = 0; sp2 < 2; ++sp2) {  // spin of E_qp
+                    // spin-symmetric shortcut (ormas_mkden2_ras.F90:77,161,292):
+                    // keep only (E_qp beta, E_sr beta) and (E_qp beta, E_sr alpha), doubled
+                    if (spin_sym && sp2 == 0) continue;
+                    int sg2; unsigned ja, jb;
+                    if (sp2 == 0) { ja = excite(ka, q, p, sg2); jb = kb; if (ja == ~0u) continue; }
+                    else { jb = excite(kb, q, p, sg2); ja = ka; if (jb == ~0u) continue; }
+                    int J = det_index(idx_a[ja], idx_b[jb]);
+                    if (J < 0) continue;
+                    double f = (double)(sg1 * sg2) * (spin_sym ? 2.0 : 1.0);
+                    D2(den2, p, q, r, s) += std::conj(c[J]) * f * cI;
+                  }
+            }
+      }
+    }
+    for (int p = 0; p < n; ++p)
+      for (int q = 0; q < n; ++q)
+        for (int r = 0; r < n; ++r) D2(den2, p, q, r, p) -= D1(den1, r, q);
+  }
+  // sigma = H c with H = sum h_pq E_pq + 1/2 sum (pq|rs)(E_pq E_rs - d_qr E_ps)
+  void hcic_sigma(const cd* c, cd* sig) {
+    const int n = nact;
+    for (int I = 0; I < lcic; ++I) sig[I] = 0.0;
+    if (nact == 0) return;
+    std::vector<cd> k1(n * n);
+    for (int p = 0; p < n; ++p)
+      for (int q = 0; q < n; ++q) {
+        cd s = D1(int1e, p, q);
+        for (int r = 0; r < n; ++r) s -= 0.5 * D2(int2e, p, r, r, q);
+        k1[p + n * q] = s;
+      }
+#pragma omp parallel
+    {
+      std::vector<cd> loc(lcic, 0.0);
+#pragma omp for schedule(dynamic)
+      for (int ib = 0; ib < (int)strb.size(); ++ib) {
+        if (detoff[ib] < 0) continue;
+        for (int pp = 0; pp < acount[ib]; ++pp) {
+          int ia = afirst[ib] + pp, I = detoff[ib] + pp;
+          cd cI = c[I];
+          if (cI == cd(0.0)) continue;
+          for (int s = 0; s < n; ++s)
+            for (int r = 0; r < n; ++r)
+              for (int sp1 = 0; sp1 < 2; ++sp1) {
+                int sg1; unsigned ka, kb;
+                if (sp1 == 0) { ka = excite(stra[ia], r, s, sg1); kb = strb[ib]; if (ka == ~0u) continue; }
+                else { kb = excite(strb[ib], r, s, sg1); ka = stra[ia]; if (kb == ~0u) continue; }
+                // E_rs |I> = sg1 |K>
+                int K = det_index(idx_a[ka], idx_b[kb]);
+                if (K >= 0) loc[K] += k1[r + n * s] * (double)sg1 * cI;
+                for (int q = 0; q < n; ++q)
+                  for (int p = 0; p < n; ++p) {
+                    cd g = D2(int2e, p, q, r, s);
+                    if (g == cd(0.0)) continue;
+                    for (int sp2 = 0; sp2 < 2; ++sp2) {
+                      int sg2; unsigned ja, jb;
+                      if (sp2 == 0) { ja = excite(ka, p, q, sg2); jb = kb; if (ja == ~0u) continue; }
+                      else { jb = excite(kb, p, q, sg2); ja = ka; if (jb == ~0u) continue; }
+                      int J = det_index(idx_a[ja], idx_b[jb]);
+                      if (J < 0) continue;
+                      loc[J] += 0.5 * g * (double)(sg1 * sg2) * cI;
+                    }
+                  }
+              }
+        }
+      }
+#pragma omp critical
+      for (int I = 0; I < lcic; ++I) sig[I] += loc[I];
+    }
+  }
+
+  // hprod_invden.F90:2-60
+  void invden() {
+    if (nact == 0) return;
+    herm_reg_inverse(nact, THROCC1, den1.data(), rden.data());
+    std::fill(rrden.begin(), rrden.end(), cd(0.0));
+    if (ncore > 0 && nact * 2 != nelact_a + nelact_b) {
+      std::vector<cd> t(nact * nact);
+      for (int i = 0; i < nact * nact; ++i) t[i] = -den1[i];
+      for (int i = 0; i < nact; ++i) t[i + nact * i] += 2.0;
+      herm_reg_inverse(nact, THROCC2, t.data(), rrden.data());
+    }
+  }
+
+  cd dot_orb(const std::vector<cd>& a, int fa, const std::vector<cd>& b, int fb) const {  // sum conj(a)*b
+    cd s = 0.0;
+    const cd* pa = &a[(size_t)fa * nbas]; const cd* pb = &b[(size_t)fb * nbas];
+    for (int k = 0; k < nbas; ++k) s += std::conj(pa[k]) * pb[k];
+    return s;
+  }
+  // <phi_j | (h0+h1+g+v2) phi_i>
+  cd fock_elem(int j, int i) const {
+    cd s = 0.0;
+    const size_t oj = (size_t)j * nbas, oi = (size_t)i * nbas;
+    for (int k = 0; k < nbas; ++k)
+      s += std::conj(orb[oj + k]) * (v2orb[oi + k] + gorb[oi + k] + h1orb[oi + k] + h0orb[oi + k]);
+    return s;
+  }
+
+  // =========================================================================
+  // hprod_htot / hprod_htotx (hprod_htot.F90:2-208)
+  // =========================================================================
+  void htot(double dtime, const double* lfield, const cd* wfn, const cd* cic, cd* hwfn, cd* hcic) {
+    const cd zfield = lfield[2], efield = lfield[5];
+    // hprod_htot_init (hprod_htot_init.F90:2-130)
+    for (auto* v : {&orb, &h0orb, &h1orb, &gorb, &v2orb}) std::fill(v->begin(), v->end(), cd(0.0));
+    for (auto* v : {&orbg, &gorbg, &v2orbg, &torbg}) std::fill(v->begin(), v->end(), cd(0.0));
+    for (auto* v : {&den1, &den2, &rden, &rrden, &int1e, &int2e, &xmat, &fmat, &bmat}) std::fill(v->begin(), v->end(), cd(0.0));
+    std::fill(dcic.begin(), dcic.end(), cd(0.0));
+    for (int i = 0; i < nfun; ++i)
+      for (int j = std::max(nfcore, i); j < nfun; ++j)
+        for (int l = 0; l <= lmax2; ++l)
+          for (int ir = 0; ir < Nr; ++ir) {
+            rho2[isp(ir, l, j, i)] = 0.0; rho2[isp(ir, l, i, j)] = 0.0;
+            v2sph[isp(ir, l, j, i)] = 0.0; v2sph[isp(ir, l, i, j)] = 0.0;
+          }
+    orbin(lfield, wfn);
+    // RDMs
+    mkden1(cic);
+    mkden2(cic);
+    invden();
+    // atomic hamiltonian
+    tprod(orb, h0orb, nfcore, nfun);
+    tprod(orb, h0orb, 0, nfcore);
+    // laser hamiltonian
+    if (cfg.igauge == 0) { zprod(zfield, orb, h1orb, nfcore, nfun); zprod(zfield, orb, h1orb, 0, nfcore); }
+    else { pzprod(zfield, orb, h1orb, nfcore, nfun); pzprod(zfield, orb, h1orb, 0, nfcore); }
+    if (nfcore > 0 && cfg.igauge == 1) zprod(efield, orb, h1orb, 0, nfcore);
+    // mean field
+    if (neltot >= 2) {
+      mkrho2("dyn"); mkrho2("fc1dyn");
+      poisson("dyn"); sph2ang2_herm("dyn");
+      poisson("fc1dyn"); sph2ang2_herm("fc1dyn");
+      mfprod2();
+#pragma omp parallel for
+      for (int f = nfcore; f < nfun; ++f) { ang2sph1(gorbg, gorb, f); ang2sph1(v2orbg, v2orb, f); }
+    }
+    // integrals: hprod_mkint1_sph.F90:2-103, hprod_mkint2_sph.F90:2-100
+    for (int ia = 0; ia < nact; ++ia)
+      for (int ja = 0; ja <= ia; ++ja) {
+        int ifn = ncore + ia, jfn = ncore + ja;
+        cd t = 0.0;
+        if (mval[ifn] == mval[jfn]) {
+          const size_t oj = (size_t)jfn * nbas, oi = (size_t)ifn * nbas;
+          for (int k = 0; k < nbas; ++k) t += std::conj(orb[oj + k]) * (gorb[oi + k] + h1orb[oi + k] + h0orb[oi + k]);
+        }
+        D1(int1e, ja, ia) = t;
+      }
+    for (int ia = 0; ia < nact; ++ia)
+      for (int ja = ia + 1; ja < nact; ++ja) D1(int1e, ja, ia) = std::conj(D1(int1e, ia, ja));
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int ia = 0; ia < nact; ++ia)
+      for (int ka = 0; ka < nact; ++ka)
+        for (int ja = 0; ja <= ia; ++ja)
+          for (int la = 0; la < nact; ++la) {
+            int ifn = ncore + ia, jfn = ncore + ja, kfn = ncore + ka, lfn = ncore + la;
+            if (mval[ifn] + mval[kfn] != mval[jfn] + mval[lfn]) continue;
+            const cd* r = &rho2[isp(0, 0, ifn, jfn)];
+            const cd* v = &v2sph[isp(0, 0, kfn, lfn)];
+            cd s = 0.0;
+            for (int q = 0; q < nbas2; ++q) s += r[q] * v[q];
+            D2(int2e, ia, ja, ka, la) = s;
+          }
+    for (int ia = 0; ia < nact; ++ia)
+      for (int ja = ia + 1; ja < nact; ++ja)
+        for (int ka = 0; ka < nact; ++ka)
+          for (int la = 0; la < nact; ++la) D2(int2e, ia, ja, ka, la) = std::conj(D2(int2e, ja, ia, la, ka));
+    // energies (hprod_htot.F90:172-179; hprod_ene_dcore.F90; hprod_ene_act.F90)
+    ene_dcore = 0;
+    for (int f = nfcore; f < ncore; ++f) {
+      cd t = 0.0;
+      const size_t o = (size_t)f * nbas;
+      for (int k = 0; k < nbas; ++k) {
+        cd h01 = h1orb[o + k] + h0orb[o + k];
+        t += std::conj(orb[o + k]) * (gorb[o + k] + h01 + h01);
+      }
+      ene_dcore += t.real();
+    }
+    ene_act = 0;
+    if (nact > 0) {
+      cd t1 = 0.0, t2 = 0.0;
+      for (int ia = 0; ia < nact; ++ia)
+        for (int ja = 0; ja < nact; ++ja) {
+          t1 += D1(int1e, ia, ja) * D1(den1, ja, ia);
+          for (int ka = 0; ka < nact; ++ka)
+            for (int la = 0; la < nact; ++la) t2 += D2(int2e, ia, ja, ka, la) * D2(den2, ja, ia, la, ka);
+        }
+      ene_act = t1.real() + 0.5 * t2.real();
+    }
+    ene_core = ene_fcore + ene_dcore;
+    ene_tot = ene_core + ene_act;
+    // X matrix (hprod_htot_mkxmat.F90)
+    const cd tfac = cfg.icomp == 0 ? cd(dtime) : IU * dtime;
+    auto X = [&](int j, int i) -> cd& { return xmat[j + nfun * i]; };
+    auto F = [&](int j, int i) -> cd& { return fmat[j + nfun * i]; };
+    auto B = [&](int j, int i) -> cd& { return bmat[j + nfun * i]; };
+    // _fc (2-77)
+    for (int i = nfcore; i < nfun; ++i)
+      for (int j = 0; j < nfcore; ++j) {
+        cd t = 0.0;
+        if (mval[j] == mval[i]) {
+          const size_t oj = (size_t)j * nbas, oi = (size_t)i * nbas;
+          for (int k = 0; k < nbas; ++k) t += std::conj(h0orb[oj + k] + h1orb[oj + k]) * orb[oi + k];
+          for (int k = 0; k < nbas; ++k) t += std::conj(orb[oj + k]) * (gorb[oi + k] + v2orb[oi + k]);
+        }
+        X(j, i) = t * tfac;
+      }
+    // _cc (79-166)
+    for (int i = nfcore; i < ncore; ++i)
+      for (int j = nfcore; j < ncore; ++j) X(j, i) = (mval[j] == mval[i] ? fock_elem(j, i) : cd(0.0)) * tfac;
+    // _ca / _ca0 (549-834)
+    if (nact * 2 == nelact_a + nelact_b) {
+      if (ncore != nfcore && nact > 0)
+        for (int i = nfcore; i < ncore; ++i)
+          for (int j = ncore; j < nfun; ++j) {
+            cd ac = 0.0, ca = 0.0;
+            if (mval[j] == mval[i]) { ac = fock_elem(j, i); ca = fock_elem(i, j); }
+            X(j, i) = ac * tfac; X(i, j) = ca * tfac;
+          }
+    } else if (ncore > 0 && nact > 0) {
+      for (int i = nfcore; i < ncore; ++i)
+        for (int j = ncore; j < nfun; ++j) {
+          cd ac = 0.0, ca = 0.0;
+          if (mval[j] == mval[i]) { ac = fock_elem(j, i); ca = fock_elem(i, j); }
+          F(j, i) = ac; F(i, j) = ca;
+        }
+      for (int i = nfcore; i < ncore; ++i)
+        for (int j = ncore; j < nfun; ++j) { X(j, i) = F(j, i) * tfac; X(i, j) = F(i, j) * tfac; }
+      for (int i = nfcore; i < ncore; ++i)
+        for (int ja = 0; ja < nact; ++ja) {
+          int jf = ncore + ja;
+          F(jf, i) = F(jf, i) + F(jf, i);
+          cd t = 0.0;
+          for (int ka = 0; ka < nact; ++ka) t += D1(den1, ja, ka) * std::conj(F(i, ncore + ka));
+          F(jf, i) -= t;
+        }
+      for (int i = nfcore; i < ncore; ++i)
+        for (int ja = 0; ja < nact; ++ja) {
+          int jf = ncore + ja;
+          cd t = 0.0;
+          for (int ka = 0; ka < nact; ++ka) t += D1(rrden, ja, ka) * F(ncore + ka, i);
+          B(jf, i) = -tfac * t;
+          B(i, jf) = -std::conj(B(jf, i));
+        }
+      for (int i = nfcore; i < ncore; ++i)
+        for (int j = ncore; j < nfun; ++j) { X(j, i) += B(j, i); X(i, j) += B(i, j); }
+    }
+    // _aa1 (265-378), nsub = 1
+    for (int ia = 0; ia < nact; ++ia)
+      for (int ja = 0; ja < nact; ++ja) {
+        int ifn = ncore + ia, jfn = ncore + ja;
+        if (mval[ifn] != mval[jfn]) continue;
+        cd t = fock_elem(jfn, ifn);
+        F(jfn, ifn) = t;
+        X(jfn, ifn) = t * tfac;
+      }
+    // _aa2 (380-547) -> ormas_xact2 -> ormas_hcic (nsub = 1: CI part only)
+    if (nact > 0) {
+      hcic_sigma(cic, dcic.data());
+      for (int I = 0; I < lcic; ++I) dcic[I] -= ene_act * cic[I];  // ormas_phase
+      const cd fac = cfg.icomp == 1 ? -IU * dtime : cd(-dtime);
+      for (int I = 0; I < lcic; ++I) dcic[I] *= fac;
+    }
+    for (int I = 0; I < lcic; ++I) hcic[I] = dcic[I];
+    // hprod_htot_dtorb (hprod_htot_dtorb.F90:2-111)
+    for (size_t k = 0; k < (size_t)nbas * nfun; ++k) hwfn[k] = 0.0;
+    const cd tf2 = cfg.icomp == 0 ? cd(-dtime) : -IU * dtime;
+#pragma omp parallel for
+    for (int i = nfcore; i < nfun; ++i) {
+      const size_t oi = (size_t)i * nbas;
+      for (int k = 0; k < nbas; ++k) hwfn[oi + k] = (v2orb[oi + k] + gorb[oi + k] + h1orb[oi + k] + h0orb[oi + k]) * tf2;
+      for (int j = 0; j < nfun; ++j) {
+        if (mval[i] != mval[j]) continue;
+        cd x = X(j, i);
+        const size_t oj = (size_t)j * nbas;
+        for (int k = 0; k < nbas; ++k) hwfn[oi + k] += orb[oj + k] * x;
+      }
+    }
+  }
+
+  // hprod_set_wfn0 / hprod_v2fc (hprod_set_wfn0.F90:2-130, 132-219, 790-865)
+  void set_wfn0(const cd* wfn, const cd* cic) {
+    (void)cic;
+    std::copy(wfn, wfn + (size_t)nbas * nfun, orb0.begin());
+    std::fill(v2jfc.begin(), v2jfc.end(), cd(0.0));
+    ene_fcore = 0;
+    if (nfcore == 0 || neltot < 2) return;
+    double lf0[9] = {0};
+    std::fill(orbg.begin(), orbg.end(), cd(0.0));
+    orbin(lf0, wfn);
+    // hprod_mkrhofc (221-251) and hprod_mkv2jfc (289-335)
+    std::vector<double> rr(Nr), ri(Nr);
+    double tr = 0, ti = 0;
+    for (int ir = 0; ir < Nr; ++ir) {
+      cd rho = 0.0;
+      for (int f = 0; f < nfcore; ++f)
+        if (mval[f] == 0) { cd o = orb[io(ir, lval[f], f)]; rho += std::conj(o) * o * (2.0 * lval[f] + 1.0); }
+      rr[ir] = rho.real(); ri[ir] = rho.imag();
+      tr += rr[ir] * d2rpl0[ir]; ti += ri[ir] * d2rpl0[ir];
+      rr[ir] *= d2invr[ir]; ri[ir] *= d2invr[ir];
+    }
+    const double fac1 = 1.0 / xrad[Nr + 1];
+    tr *= fac1; ti *= fac1;
+    band_solve(Nr, nd, &d2ll[0], rr.data());
+    band_solve(Nr, nd, &d2ll[0], ri.data());
+    for (int ir = 0; ir < Nr; ++ir)
+      v2jfc[ir] = cd((rr[ir] + tr * d2rpl1[ir]) * d2fac2[ir], (ri[ir] + ti * d2rpl1[ir]) * d2fac2[ir]);
+    // frozen-core pair potentials (fcfc)
+    mkrho2("fcfc"); poisson("fcfc"); sph2ang2_herm("fcfc");
+    // hprod_v2fc_enefc (790-865)
+    for (int f = 0; f < nfcore; ++f) for (int k = 0; k < nbas; ++k) h0orb[(size_t)f * nbas + k] = 0.0;
+    tprod(orb, h0orb, 0, nfcore);
+    cd t = 0.0;
+    for (int f = 0; f < nfcore; ++f) t += dot_orb(orb, f, h0orb, f);
+    double enefc = t.real() * 2.0;
+    for (int f = 0; f < nfcore; ++f)
+      for (int q = 0; q < ngrid; ++q) gorbg[(size_t)f * ngrid + q] = 0.0;
+    for (int i = 0; i < nfcore; ++i)
+      for (int tt = 0; tt < nlat; ++tt)
+        for (int ir = 0; ir < Nr; ++ir) gorbg[ig(ir, tt, i)] += v2jfc[ir] * orbg[ig(ir, tt, i)];  // fcj, dofc
+    for (int i = 0; i < nfcore; ++i)
+      for (int j = 0; j < nfcore; ++j)  // fcx1, dofc
+        for (int q = 0; q < ngrid; ++q) gorbg[(size_t)i * ngrid + q] -= v2ang[ian(0, 0, j, i) + q] * orbg[(size_t)j * ngrid + q];
+    for (int f = 0; f < nfcore; ++f) ang2sph1(gorbg, gorb, f);
+    t = 0.0;
+    for (int f = 0; f < nfcore; ++f) t += dot_orb(orb, f, gorb, f);
+    enefc += t.real();
+    ene_fcore = enefc;
+    // hprod_addfc_tmat (hprod_addfc_tmat.F90:2-33)
+    const int bw = 2 * nd + 1;
+    for (int l = 0; l <= lmax1; ++l)
+      for (int ir = 0; ir < Nr; ++ir) tmat[((size_t)l * Nr + ir) * bw + nd] += v2jfc[ir].real();
+  }
+
+  // length-form dipole <z> = sum_ij <phi_i|z|phi_j> den1_full(j,i)
+  double dipole(const cd* wfn, const cd* cic) {
+    std::vector<cd> zo((size_t)nbas * nfun, 0.0), w(wfn, wfn + (size_t)nbas * nfun);
+    zprod(1.0, w, zo, 0, nfun);
+    mkden1(cic);
+    cd s = 0.0;
+    for (int f = 0; f < ncore; ++f) s += 2.0 * dot_orb(w, f, zo, f);
+    for (int ia = 0; ia < nact; ++ia)
+      for (int ja = 0; ja < nact; ++ja) {
+        int ifn = ncore + ia, jfn = ncore + ja;
+        if (mval[ifn] != mval[jfn]) continue;
+        s += dot_orb(w, ifn, zo, jfn) * D1(den1, ja, ia);
+      }
+    return s.real();
+  }
+};
+
+// clfield1.cpp:15-115 (sin2 envelope), 472-500 (A explicit), 573-620 (E by
+// 6-point numerical derivative of the explicit A in velocity1);
+// length1: E explicit, A implicit is not needed by the RHS (lfield(3,3)
+// is only read in the velocity gauge).
+static double field_a(const orc_pulse* p, double t) {
+  double famp = std::sqrt(p->fint / 3.50944506E+16);
+  double freq = 1239.84190 / (p->wlen * 27.2113845);
+  double period = 2 * PI / freq, tau = p->numcyc * period * 0.5;
+  double tleft = 0, tright = 2 * tau;
+  if (!(t > tleft && t < tright)) return 0.0;
+  double env = std::sin(PI * t / (p->numcyc * period)); env *= env;
+  return env * famp / freq * std::sin(freq * t + p->cep / 180.0 * PI);
+}
+static double field_e(const orc_pulse* p, double t) {
+  double famp = std::sqrt(p->fint / 3.50944506E+16);
+  double freq = 1239.84190 / (p->wlen * 27.2113845);
+  double period = 2 * PI / freq, tau = p->numcyc * period * 0.5;
+  if (!(t > 0 && t < 2 * tau)) return 0.0;
+  double env = std::sin(PI * t / (p->numcyc * period)); env *= env;
+  return env * famp * std::sin(freq * t + p->cep / 180.0 * PI);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_create(const orc_config* cfg) {
+  Oracle* o = new Oracle();
+  o->setup(cfg);
+  return o;
+}
+void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
+void orc_dims(void* h, int* d) {
+  Oracle* o = static_cast<Oracle*>(h);
+  int v[16] = {o->nrad, o->nbas, o->nbas2, o->ngrid, o->nlat, o->lcic, o->nfcore, o->ndcore, o->nact,
+               o->ncore, (int)o->stra.size(), (int)o->strb.size(), o->nd, o->lmax1, o->lmax2, o->nfun};
+  std::memcpy(d, v, sizeof(v));
+}
+static long put_d(const std::vector<double>& v, double* out) {
+  if (out) std::memcpy(out, v.data(), v.size() * sizeof(double));
+  return (long)v.size();
+}
+static long put_c(const std::vector<cd>& v, double* out) {
+  if (out) std::memcpy(out, v.data(), v.size() * sizeof(cd));
+  return (long)v.size() * 2;
+}
+long orc_get(void* h, const char* name, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::string n(name);
+  if (n == "xrad") return put_d(o->xrad, out);
+  if (n == "wrad") return put_d(o->wrad, out);
+  if (n == "mask") return put_d(o->mask, out);
+  if (n == "radk") return put_d(o->radk, out);
+  if (n == "radk0") return put_d(o->radk0, out);
+  if (n == "radp") return put_d(o->radp, out);
+  if (n == "cost") return put_d(o->cost, out);
+  if (n == "wlat") return put_d(o->wlat, out);
+  if (n == "legf1") return put_d(o->legf1, out);
+  if (n == "legb1") return put_d(o->legb1, out);
+  if (n == "legf2") return put_d(o->legf2, out);
+  if (n == "legb2") return put_d(o->legb2, out);
+  if (n == "tmat") return put_d(o->tmat, out);
+  if (n == "pmat") return put_d(o->pmat, out);
+  if (n == "d2ll") return put_d(o->d2ll, out);
+  if (n == "alph") return put_d(o->alph, out);
+  if (n == "d2rpl0") return put_d(o->d2rpl0, out);
+  if (n == "d2rpl1") return put_d(o->d2rpl1, out);
+  if (n == "d2invr") return put_d(o->d2invr, out);
+  if (n == "d2fac2") return put_d(o->d2fac2, out);
+  if (n == "d2fac1") return put_d(o->d2fac1, out);
+  if (n == "orb") return put_c(o->orb, out);
+  if (n == "orbg") return put_c(o->orbg, out);
+  if (n == "h0orb") return put_c(o->h0orb, out);
+  if (n == "h1orb") return put_c(o->h1orb, out);
+  if (n == "gorb") return put_c(o->gorb, out);
+  if (n == "v2orb") return put_c(o->v2orb, out);
+  if (n == "gorbg") return put_c(o->gorbg, out);
+  if (n == "v2orbg") return put_c(o->v2orbg, out);
+  if (n == "rho2") return put_c(o->rho2, out);
+  if (n == "v2sph") return put_c(o->v2sph, out);
+  if (n == "v2ang") return put_c(o->v2ang, out);
+  if (n == "den1") return put_c(o->den1, out);
+  if (n == "den2") return put_c(o->den2, out);
+  if (n == "rden") return put_c(o->rden, out);
+  if (n == "rrden") return put_c(o->rrden, out);
+  if (n == "int1e") return put_c(o->int1e, out);
+  if (n == "int2e") return put_c(o->int2e, out);
+  if (n == "xmat") return put_c(o->xmat, out);
+  if (n == "v2jfc") return put_c(o->v2jfc, out);
+  if (n == "stra") { if (out) for (size_t k = 0; k < o->stra.size(); ++k) out[k] = o->stra[k]; return (long)o->stra.size(); }
+  if (n == "strb") { if (out) for (size_t k = 0; k < o->strb.size(); ++k) out[k] = o->strb[k]; return (long)o->strb.size(); }
+  if (n == "detoff") { if (out) for (size_t k = 0; k < o->detoff.size(); ++k) out[k] = o->detoff[k]; return (long)o->detoff.size(); }
+  return -1;
+}
+void orc_set_wfn0(void* h, const double* wfn, const double* cic) {
+  static_cast<Oracle*>(h)->set_wfn0(reinterpret_cast<const cd*>(wfn), reinterpret_cast<const cd*>(cic));
+}
+void orc_htot(void* h, double dtime, const double* lfield, const double* wfn, const double* cic,
+              double* hwfn, double* hcic) {
+  static_cast<Oracle*>(h)->htot(dtime, lfield, reinterpret_cast<const cd*>(wfn), reinterpret_cast<const cd*>(cic),
+                                reinterpret_cast<cd*>(hwfn), reinterpret_cast<cd*>(hcic));
+}
+void orc_energies(void* h, double* e) {
+  Oracle* o = static_cast<Oracle*>(h);
+  e[0] = o->ene_fcore; e[1] = o->ene_dcore; e[2] = o->ene_core; e[3] = o->ene_act; e[4] = o->ene_tot;
+}
+void orc_field(const orc_pulse* p, double t, double* lf) {
+  for (int i = 0; i < 9; ++i) lf[i] = 0.0;
+  double A = field_a(p, t);
+  if (p->igauge == 1) {
+    // velocity1: gauge field = A explicit; E = -dA/dt by the 6-point rule
+    const double dstep = 2 * PI / (1239.84190 / (800.0 * 27.2113845)) / 100000.0;
+    double e = 0;
+    e += field_a(p, t + 3 * dstep) / 60.0;
+    e -= field_a(p, t + 2 * dstep) / 20.0 * 3.0;
+    e += field_a(p, t + dstep) / 4.0 * 3.0;
+    e -= field_a(p, t - dstep) / 4.0 * 3.0;
+    e += field_a(p, t - 2 * dstep) / 20.0 * 3.0;
+    e -= field_a(p, t - 3 * dstep) / 60.0;
+    lf[2] = A; lf[5] = -e / dstep; lf[8] = A;
+  } else {
+    double E = field_e(p, t);
+    lf[2] = E; lf[5] = E; lf[8] = A;
+  }
+}
+void orc_rk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, double* wfn, double* cic, double* dip) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t no = (size_t)o->nbas * o->nfun, nc = o->lcic, n = no + nc;
+  std::vector<cd> y0(n), ty(n), k[4];
+  for (auto& v : k) v.assign(n, 0.0);
+  cd* Y = reinterpret_cast<cd*>(wfn);
+  cd* C = reinterpret_cast<cd*>(cic);
+  const double nodes[4] = {0, 0.5, 0.5, 1}, wg[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+  const double a[4][3] = {{0, 0, 0}, {0.5, 0, 0}, {0, 0.5, 0}, {0, 0, 1}};
+  double t = t0;
+  for (int s = 0; s < nstep; ++s) {
+    for (size_t q = 0; q < no; ++q) y0[q] = Y[q];
+    for (size_t q = 0; q < nc; ++q) y0[no + q] = C[q];
+    for (int is = 0; is < 4; ++is) {  // clcrk.cpp:55-87, set_coeff_04 221-235
+      for (size_t q = 0; q < n; ++q) {
+        cd v = y0[q];
+        for (int js = 0; js < is; ++js) v += dt * a[is][js] * k[js][q];
+        ty[q] = v;
+      }
+      double lf[9]; orc_field(p, t + dt * nodes[is], lf);
+      o->htot(1.0, lf, ty.data(), ty.data() + no, k[is].data(), k[is].data() + no);
+      for (size_t q = 0; q < no; ++q) Y[q] += dt * wg[is] * k[is][q];
+      for (size_t q = 0; q < nc; ++q) C[q] += dt * wg[is] * k[is][no + q];
+    }
+    // wfn_mask (wfn_mask.F90:2-35)
+    int min_ir = 1;
+    for (int ir = 1; ir <= o->Nr; ++ir) if (o->xrad[ir] > o->cfg.rmask) { min_ir = ir; break; }
+    for (int f = o->nfcore; f < o->nfun; ++f)
+      for (int l = std::abs(o->mval[f]); l <= o->lmax1; ++l)
+        for (int ir = min_ir; ir <= o->Nr; ++ir) Y[o->io(ir - 1, l, f)] *= o->mask[ir];
+    t += dt;
+    if (dip) dip[s] = o->dipole(Y, C);
+  }
+}
+double orc_dipole(void* h, const double* wfn, const double* cic) {
+  return static_cast<Oracle*>(h)->dipole(reinterpret_cast<const cd*>(wfn), reinterpret_cast<const cd*>(cic));
+}
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+}  // extern "C"

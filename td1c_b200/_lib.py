@@ -1,0 +1,81 @@
+"""Build and load libtd1c_b200.so (the sm_100a CUDA library with the C-ABI).
+
+The library is built in-tree by nvcc for sm_100a.  Loading never falls back
+to anything else: if the shared library is missing or fails to load, the
+error propagates.
+"""
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB_DIR = os.path.join(HERE, "_lib")
+LIB_PATH = os.path.join(LIB_DIR, "libtd1c_b200.so")
+SOURCES = ["hprod.cu", "legendre_gemm.cu", "onebody.cu", "poisson.cu", "mfprod.cu", "reductions.cu", "ci.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+_lib = None
+
+
+def build(verbose=False):
+    """Compile every CUDA source into td1c_b200/_lib/libtd1c_b200.so."""
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = [NVCC] + NVCC_FLAGS + ["-o", LIB_PATH] + [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+def _newer_sources():
+    if not os.path.exists(LIB_PATH):
+        return True
+    t = os.path.getmtime(LIB_PATH)
+    for f in os.listdir(CSRC):
+        if os.path.getmtime(os.path.join(CSRC, f)) > t:
+            return True
+    return False
+
+
+def load():
+    """Load the CUDA library (building it first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = ctypes.CDLL(LIB_PATH)
+    c_int, c_double, c_long, vp = ctypes.c_int, ctypes.c_double, ctypes.c_long, ctypes.c_void_p
+    dp, ip, up = ctypes.POINTER(c_double), ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_uint)
+    lib.td1c_gpu_bind_rad.argtypes = [c_int, c_int, c_int, dp, dp, dp, dp, dp, c_double, dp]
+    lib.td1c_gpu_bind_sph.argtypes = [c_int, c_int, c_int, c_int, c_int, dp, dp, dp, dp, dp, dp]
+    lib.td1c_gpu_bind_bas.argtypes = [c_double, c_int, c_int, c_int, ip, ip, ip, c_int, c_int]
+    lib.td1c_gpu_bind_control.argtypes = [c_int, c_int]
+    lib.hprod_bind_.argtypes = [dp, dp, dp, dp, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_bool), dp]
+    lib.hprod_init_.argtypes = []
+    lib.hprod_set_wfn0_.argtypes = [dp, dp, ctypes.c_char_p, c_int]
+    lib.hprod_htot_.argtypes = [dp, dp, dp, dp, dp, dp]
+    lib.hprod_final_.argtypes = []
+    lib.td1c_gpu_last_status.restype = c_int
+    lib.td1c_gpu_dims.argtypes = [ip]
+    lib.td1c_gpu_ci_tables.argtypes = [up, up, ip, ip, ip]
+    lib.td1c_gpu_energies.argtypes = [dp]
+    lib.td1c_gpu_htot_dev.argtypes = [c_double, dp, vp, vp, vp, vp]
+    lib.td1c_gpu_debug_get.restype = c_long
+    lib.td1c_gpu_debug_get.argtypes = [ctypes.c_char_p, dp, c_long]
+    lib.td1c_gpu_rk4.argtypes = [vp, vp, c_double, c_double, c_int, c_double, c_double, c_double, c_double, c_int]
+    lib.td1c_gpu_sync.restype = c_int
+    lib.td1c_gpu_launch_count.restype = c_long
+    _lib = lib
+    return lib
+
+
+EXPORTED = [
+    "td1c_gpu_bind_rad", "td1c_gpu_bind_sph", "td1c_gpu_bind_bas", "td1c_gpu_bind_control",
+    "hprod_bind_", "hprod_init_", "hprod_set_wfn0_", "hprod_htot_", "hprod_final_",
+    "td1c_gpu_last_status", "td1c_gpu_dims", "td1c_gpu_ci_tables", "td1c_gpu_energies",
+    "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
+]

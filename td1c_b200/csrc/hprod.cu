@@ -1,0 +1,1354 @@
+// hprod.cu -- orchestration of the B200 orbital-equation RHS and the C-ABI.
+//
+// hprod_htot (src/hprod/hprod_htot.F90:2-208) as a fixed sequence of device
+// kernels on one stream, all data resident in HBM:
+//   orbin        sph2ang1 GEMM (+ frozen-core gauge phase)   hprod_orbin.F90
+//   CI           D = E_pq c, 1-/2-RDM, regularised 1/D        ormas_mkden1/2, hprod_invden.F90
+//   one-body     tprod + zprod/pzprod stencil                 hprod_tprod/zprod/pzprod.F90
+//   pair density fused into the theta->l GEMM                 hprod_mkrho2.F90, bas_ang2sph2.F90
+//   Poisson      banded Cholesky solves per (pair, l)         hprod_mkv2mf.F90
+//   l->theta     GEMM (Hermitian half read with conj)         bas_sph2ang2.F90
+//   mfprod       core J/K, active J/K, 2-RDM contraction      hprod_mfprod2.F90
+//   theta->l     GEMM for g and v2 orbitals                   bas_ang2sph1.F90
+//   integrals    orbital matrix elements, int2e block GEMM    hprod_mkint1/2_sph.F90
+//   small        int1e, energies, X matrix                    hprod_ene_*.F90, hprod_htot_mkxmat.F90
+//   sigma        CI sigma vector                              ormas_xact2/ormas_hcic
+//   dtorb        hwfn = -i dt (h0+h1+g+v2) phi + sum_j phi_j X_ji  hprod_htot_dtorb.F90
+// Set-up (the bas_gen_* tables, the band Cholesky factors, the CI string
+// tables, pair and batch lists) happens once in hprod_init_.  There is no
+// host fallback: every RHS value is produced by the kernels in this library.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "reductions.cuh"
+#include "../../include/td1c_b200.h"
+
+using namespace td1c;
+
+namespace {
+
+const double PI = 3.14159265358979323846264338327950288;
+
+std::vector<void*> g_allocs;  // every device allocation of the context, freed by hprod_final_
+
+template <class T>
+T* dalloc(size_t n) {
+  T* p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+    fprintf(stderr, "td1c_b200: cudaMalloc of %zu bytes failed\n", n * sizeof(T));
+    return nullptr;
+  }
+  cudaMemset(p, 0, n * sizeof(T));
+  g_allocs.push_back(p);
+  return p;
+}
+template <class T>
+T* dupload(const std::vector<T>& v) {
+  T* p = dalloc<T>(v.size());
+  if (p && !v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return p;
+}
+
+struct Ctx {
+  // ---- bound inputs
+  bool have_rad = false, have_sph = false, have_bas = false, initialized = false;
+  int nfe = 0, nd = 0, nrad = 0, Nr = 0;
+  double rmask = 0;
+  std::vector<double> h_xrad, h_wrad, h_radp, h_radk, h_radk0, h_mask;
+  int lmax1 = 0, lmax2 = 0, mmax1 = 0, mmax2 = 0, nlat = 0, L1 = 0, L2 = 0;
+  std::vector<double> h_wlat, h_cost, h_legf1, h_legb1, h_legf2, h_legb2;
+  double znuc = 0; int smul = 1, mtot = 0, nfun = 0, nela = 0, nelb = 0;
+  std::vector<int> otype, mval, lval;
+  int icomp = 1, igauge = 0;
+  int nfcore = 0, ndcore = 0, nact = 0, ncore = 0, nelact = 0, neltot = 0;
+  // ---- hprod_bind_ outputs
+  double *p_ene_fcore = nullptr, *p_ene_dcore = nullptr, *p_ene_core = nullptr, *p_ene_act = nullptr, *p_ene_tot = nullptr;
+  // ---- device tables
+  double *xrad = nullptr, *mask = nullptr, *radk = nullptr, *radk0 = nullptr, *radp = nullptr, *cost = nullptr;
+  double *legf1 = nullptr, *legb1 = nullptr, *legf2 = nullptr, *legb2 = nullptr, *alph = nullptr;
+  double *tdiag = nullptr, *d2ll = nullptr, *d2rinv = nullptr, *rpl0 = nullptr, *rpl1 = nullptr, *invr = nullptr, *fac2 = nullptr, *fac1 = nullptr;
+  int* d_mval = nullptr;
+  // ---- pairs
+  int npair = 0, npair_all = 0, nfcfc = 0;
+  std::vector<int> pa, pb;  // stored pair p = (a, b)
+  int *pair_m = nullptr, *pair_of = nullptr, *pair_cj = nullptr;
+  // ---- state
+  size_t nbas = 0, nbas2 = 0, ngrid = 0;
+  cplx *orb = nullptr, *orb0 = nullptr, *orbg0 = nullptr, *orbg = nullptr, *h0orb = nullptr, *h1orb = nullptr;
+  cplx *gorb = nullptr, *v2orb = nullptr, *gorbg = nullptr, *v2orbg = nullptr, *rho2 = nullptr, *v2sph = nullptr, *W = nullptr;
+  cplx *wfn_io = nullptr, *cic_io = nullptr, *hwfn_io = nullptr, *hcic_io = nullptr;
+  double* lfield = nullptr;  // device [9]
+  double* v2jfc = nullptr;   // device [Nr] (real)
+  // ---- CI
+  int lcic = 1, nstr_a = 0, nstr_b = 0, smin = 0, nsec = 0, maxsec = 0, spin_sym = 0;
+  std::vector<unsigned> h_stra, h_strb;
+  std::vector<int> h_detoff, h_afirst, h_acount;
+  CiTables cit{};
+  cplx *Da = nullptr, *Db = nullptr, *T = nullptr, *den1 = nullptr, *den2 = nullptr, *rden = nullptr, *rrden = nullptr;
+  cplx *int1e = nullptr, *int2e = nullptr, *cic = nullptr;
+  // ---- reductions
+  OrbdotsArgs od{};
+  std::vector<int4> h_ent;
+  int* ent_index = nullptr;  // [5][nfun][nfun] -> entry id or -1 (A, B, C, E, GV)
+  Int2eArgs i2{};
+  int i2_nsplit = 64;
+  Act2Entry* act2_list = nullptr; int nact2 = 0;
+  // ---- small matrices
+  cplx *xmat = nullptr;
+  double* ene = nullptr;  // device [5]
+  double h_ene[5] = {0, 0, 0, 0, 0};
+  double ene_fcore = 0;
+  // ---- GEMM batches
+  LegGemmBatch *b_orbg = nullptr, *b_orbfc = nullptr, *b_rho = nullptr, *b_rho_fcfc = nullptr, *b_W = nullptr,
+               *b_W_fcfc = nullptr, *b_gorb = nullptr, *b_orbg0 = nullptr, *b_gorbfc = nullptr;
+  int n_orbg = 0, n_orbfc = 0, n_gorb = 0;
+  // ---- RK4
+  cplx *y0 = nullptr, *yacc = nullptr, *ytmp = nullptr, *kbuf = nullptr;
+  double* field_tab = nullptr; int field_cap = 0;
+  cudaGraphExec_t graph_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  long launches = 0;
+  // ---- misc
+  cudaStream_t st = nullptr;
+  int status = 0;
+  int* d_status = nullptr;  // device status word (ST_* bits)
+  double* d_scalar = nullptr;
+};
+
+Ctx* g = nullptr;
+Ctx& ctx() {
+  if (!g) g = new Ctx();
+  return *g;
+}
+
+// ===========================================================================
+// set-up kernels
+// ===========================================================================
+// band Cholesky (dpbtrf 'L') of A_l = l(l+1)/r^2 + 2 radk (bas_gen_d2ll.F90:2-140),
+// one thread per l; factor stored as ab[(i-j) + (nd+1) j] for each l.
+__global__ void d2ll_factor_kernel(int Nr, int nd, int L2, const double* __restrict__ xrad,
+                                   const double* __restrict__ radk, double* __restrict__ d2ll,
+                                   double* __restrict__ rinv, int* status) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L2) return;
+  const int ld1 = nd + 1, bw = 2 * nd + 1;
+  double* ab = d2ll + (size_t)l * ld1 * Nr;
+  const double l2 = (double)l * (l + 1);
+  for (int ir = 1; ir <= Nr; ++ir) {
+    double ak = 1.0 / xrad[ir];
+    ab[(size_t)ld1 * (ir - 1)] = ak * ak * l2;
+    for (int k = 1; k <= nd; ++k) ab[(size_t)ld1 * (ir - 1) + k] = 0.0;
+  }
+  for (int ir = 1; ir <= Nr; ++ir) {
+    int jul = min(Nr, ir + nd);
+    for (int jr = ir; jr <= jul; ++jr) ab[(size_t)ld1 * (ir - 1) + (jr - ir)] += 2.0 * radk[(size_t)bw * ir + (jr - ir + nd)];
+  }
+  for (int j = 0; j < Nr; ++j) {
+    double d = ab[ld1 * j];
+    for (int k = max(0, j - nd); k < j; ++k) { double v = ab[(j - k) + ld1 * k]; d -= v * v; }
+    if (!(d > 0)) { atomicOr(status, ST_CHOLESKY); return; }
+    d = sqrt(d);
+    ab[ld1 * j] = d;
+    for (int i = j + 1; i <= min(Nr - 1, j + nd); ++i) {
+      double s = ab[(i - j) + ld1 * j];
+      for (int k = max(0, i - nd); k < j; ++k) s -= ab[(i - k) + ld1 * k] * ab[(j - k) + ld1 * k];
+      ab[(i - j) + ld1 * j] = s / d;
+    }
+  }
+  for (int j = 0; j < Nr; ++j) rinv[(size_t)l * Nr + j] = 1.0 / ab[ld1 * j];
+}
+
+// tmat diagonal (bas_gen_tmat.F90:30-75) plus the frozen-core Hartree
+// potential (hprod_addfc_tmat.F90:2-33)
+__global__ void tdiag_kernel(int Nr, int L1, int nd, double znuc, const double* __restrict__ xrad,
+                             const double* __restrict__ radk, const double* __restrict__ radk0,
+                             const double* __restrict__ v2jfc, double* __restrict__ tdiag) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= Nr * L1) return;
+  int l = t / Nr, r = t % Nr, ir = r + 1;
+  const int bw = 2 * nd + 1;
+  double oor = 1.0 / xrad[ir];
+  double zor = oor * (-znuc + (double)(l * (l + 1)) * oor * 0.5);
+  double rk = (l == 0 ? radk : radk0)[(size_t)bw * ir + nd];
+  double v = zor + rk;
+  if (v2jfc) v += v2jfc[r];
+  tdiag[t] = v;
+}
+
+// frozen-core Hartree potential v2jfc: l = 0 Poisson of the frozen-core
+// density (hprod_set_wfn0.F90:221-335); one thread, set-up only
+__global__ void v2jfc_kernel(int Nr, int nd, int L1, int nfcore, const int* __restrict__ mval, const int* __restrict__ lvalv,
+                             const cplx* __restrict__ orb, const double* __restrict__ d2ll, const double* __restrict__ rinv,
+                             const double* __restrict__ rpl0, const double* __restrict__ rpl1, const double* __restrict__ invr,
+                             const double* __restrict__ fac2, double rmax, double* __restrict__ v) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const int ld1 = nd + 1;
+  double t = 0.0;
+  for (int r = 0; r < Nr; ++r) {
+    double rho = 0.0;
+    for (int f = 0; f < nfcore; ++f)
+      if (mval[f] == 0) { cplx o = orb[((size_t)f * L1 + lvalv[f]) * Nr + r]; rho += cabs2(o) * (2.0 * lvalv[f] + 1.0); }
+    t += rho * rpl0[r];
+    v[r] = rho * invr[r];
+  }
+  t *= 1.0 / rmax;
+  for (int j = 0; j < Nr; ++j) {
+    double s = v[j];
+    for (int k = max(0, j - nd); k < j; ++k) s -= d2ll[(j - k) + ld1 * k] * v[k];
+    v[j] = s * rinv[j];
+  }
+  for (int j = Nr - 1; j >= 0; --j) {
+    double s = v[j];
+    for (int i = min(Nr - 1, j + nd); i >= j + 1; --i) s -= d2ll[(i - j) + ld1 * j] * v[i];
+    v[j] = s * rinv[j];
+  }
+  for (int r = 0; r < Nr; ++r) v[r] = (v[r] + t * rpl1[r]) * fac2[r];
+}
+
+// frozen-core mean field on the frozen core for the frozen-core energy
+// (hprod_v2fc_enefc: fcj and fcx1 with dofc, hprod_set_wfn0.F90:823-833)
+__global__ void fc_g_kernel(int Nr, int nlat, int nfcore, int nfun, const cplx* __restrict__ orbg, const cplx* __restrict__ W,
+                            const int* __restrict__ pair_of, const int* __restrict__ pair_cj, const double* __restrict__ v2jfc,
+                            cplx* __restrict__ gorbg) {
+  const size_t ng = (size_t)Nr * nlat;
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ng * nfcore) return;
+  const int i = (int)(t / ng);
+  const size_t q = t % ng;
+  const int r = (int)(q % Nr);
+  cplx v = cscale(orbg[(size_t)i * ng + q], v2jfc[r]);
+  for (int j = 0; j < nfcore; ++j) {
+    int p = pair_of[j * nfun + i], cj = pair_cj[j * nfun + i];
+    cplx w = W[(size_t)p * ng + q];
+    if (cj) w = cconj(w);
+    v = csub(v, cmul(w, orbg[(size_t)j * ng + q]));
+  }
+  gorbg[(size_t)i * ng + q] = v;
+}
+
+// out = Re sum conj(a) b over n complex values (one block, fixed order)
+__global__ void __launch_bounds__(256) dot_re_kernel(const cplx* __restrict__ a, const cplx* __restrict__ b, size_t n, double* out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) s += a[k].x * b[k].x + a[k].y * b[k].y;
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// ===========================================================================
+// per-RHS small kernels
+// ===========================================================================
+// frozen core in the velocity gauge: orbg_fc = sph2ang1(orb0_fc) exp(-i A r cos th)
+// (hprod_orbin.F90:68-105)
+__global__ void fc_phase_kernel(int Nr, int nlat, int nfcore, const double* __restrict__ xrad, const double* __restrict__ cost,
+                                const double* __restrict__ lfield, const cplx* __restrict__ orbg0, cplx* __restrict__ orbg) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t n = (size_t)Nr * nlat * nfcore;
+  if (t >= n) return;
+  int r = t % Nr, th = (t / Nr) % nlat;
+  double ph = lfield[8] * xrad[r + 1] * cost[th];
+  double s, c;
+  sincos(ph, &s, &c);
+  orbg[t] = cmul(orbg0[t], mkc(c, -s));
+}
+
+// Hermitian regularised inverse U diag(d/(d^2+thr)) U^H by a one-warp cyclic
+// complex Jacobi (hprod_invden.F90:62-107; zheev replaced).  Matrix n <= 16.
+__device__ void herm_reg_inverse_warp(int n, double thr, const cplx* a, cplx* inv, cplx* A, cplx* V, int* status) {
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < n * n; e += 32) { A[e] = a[e]; V[e] = mkc((e % n) == (e / n) ? 1.0 : 0.0, 0.0); }
+  __syncwarp();
+  bool conv = false;
+  for (int sweep = 0; sweep < 60 && !conv; ++sweep) {
+    double off = 0, dg = 0;
+    for (int e = lane; e < n * n; e += 32) { if ((e % n) != (e / n)) off += cabs2(A[e]); else dg += cabs2(A[e]); }
+    for (int o = 16; o > 0; o >>= 1) { off += __shfl_xor_sync(0xffffffff, off, o); dg += __shfl_xor_sync(0xffffffff, dg, o); }
+    if (off <= 1e-32 * fmax(dg, 1e-300)) { conv = true; break; }
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        cplx apq = A[p + n * q];
+        double b = sqrt(cabs2(apq));
+        if (b < 1e-300) continue;
+        cplx e = cscale(apq, 1.0 / b);
+        double app = A[p + n * p].x, aqq = A[q + n * q].x;
+        double tau = (aqq - app) / (2 * b);
+        double tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+        double c = 1 / sqrt(1 + tt * tt), s = tt * c;
+        cplx em = cconj(e);
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+          cplx akp = A[k + n * p], akq = A[k + n * q];
+          A[k + n * p] = csub(cscale(akp, c), cscale(cmul(em, akq), s));
+          A[k + n * q] = cadd(cscale(akp, s), cscale(cmul(em, akq), c));
+          cplx vkp = V[k + n * p], vkq = V[k + n * q];
+          V[k + n * p] = csub(cscale(vkp, c), cscale(cmul(em, vkq), s));
+          V[k + n * q] = cadd(cscale(vkp, s), cscale(cmul(em, vkq), c));
+        }
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+          cplx apk = A[p + n * k], aqk = A[q + n * k];
+          A[p + n * k] = csub(cscale(apk, c), cscale(cmul(e, aqk), s));
+          A[q + n * k] = cadd(cscale(apk, s), cscale(cmul(e, aqk), c));
+        }
+        __syncwarp();
+      }
+  }
+  if (!conv && lane == 0) atomicOr(status, ST_JACOBI);
+  __syncwarp();
+  for (int e = lane; e < n * n; e += 32) {
+    int i = e % n, j = e / n;
+    cplx s = mkc(0, 0);
+    for (int k = 0; k < n; ++k) {
+      double d = A[k + n * k].x;
+      double invd = thr > 0 ? d / (d * d + thr) : 1.0 / d;
+      s = cadd(s, cscale(cmulc(V[j + n * k], V[i + n * k]), invd));
+    }
+    inv[e] = s;
+  }
+}
+
+__global__ void invden_kernel(int nact, int need_rr, const cplx* __restrict__ den1, cplx* rden, cplx* rrden, int* status) {
+  __shared__ cplx sA[2][16 * 16], sV[2][16 * 16], sT[16 * 16];  // nact <= 16
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w == 0) {
+    herm_reg_inverse_warp(nact, 1.0e-15, den1, rden, sA[0], sV[0], status);
+  } else if (w == 1) {
+    if (need_rr) {
+      for (int e = lane; e < nact * nact; e += 32) {
+        cplx v = cscale(den1[e], -1.0);
+        if ((e % nact) == (e / nact)) v.x += 2.0;
+        sT[e] = v;
+      }
+      __syncwarp();
+      herm_reg_inverse_warp(nact, 1.0e-15, sT, rrden, sA[1], sV[1], status);
+    } else {
+      for (int e = lane; e < nact * nact; e += 32) rrden[e] = mkc(0, 0);
+    }
+  }
+}
+
+struct SmallArgs {
+  int nfun, nfcore, ndcore, nact, ncore, nelact, icomp;
+  double dtime, ene_fcore;
+  const int* mval;
+  const int* ent_index;  // [5][nfun][nfun]
+  const cplx* res;       // orbdots results
+  const cplx* den1; const cplx* den2; const cplx* rrden;
+  cplx* int1e; const cplx* int2e;
+  cplx* xmat;
+  double* ene;           // [5]
+};
+
+__device__ __forceinline__ cplx resv(const SmallArgs& a, int kind, int j, int i) {
+  int e = a.ent_index[(kind * a.nfun + j) * a.nfun + i];
+  return e >= 0 ? a.res[e] : mkc(0, 0);
+}
+
+// int1e, energies and the X matrix (hprod_mkint1_sph.F90, hprod_ene_act.F90,
+// hprod_ene_dcore.F90, hprod_htot_mkxmat.F90 _fc/_cc/_ca/_ca0/_aa1)
+__global__ void __launch_bounds__(256) smallmat_kernel(SmallArgs a) {
+  __shared__ double red[256];
+  __shared__ cplx F[16 * 16];
+  const int n = a.nact, nf = a.nfun, nc = a.ncore, nfc = a.nfcore;
+  const int tid = threadIdx.x;
+  // int1e(ja, ia) = A(j, i) for ja <= ia, conj fill
+  for (int e = tid; e < n * n; e += blockDim.x) {
+    int ja = e % n, ia = e / n;
+    int j = nc + ja, i = nc + ia;
+    cplx v = mkc(0, 0);
+    if (a.mval[j] == a.mval[i]) v = (ja <= ia) ? resv(a, 0, j, i) : cconj(resv(a, 0, i, j));
+    a.int1e[e] = v;
+  }
+  // Fock elements F(j,i) = A + B for dynamic j, i of equal m
+  for (int e = tid; e < nf * nf; e += blockDim.x) {
+    int j = e % nf, i = e / nf;
+    F[e] = (j >= nfc && i >= nfc && a.mval[j] == a.mval[i]) ? cadd(resv(a, 0, j, i), resv(a, 1, j, i)) : mkc(0, 0);
+  }
+  __syncthreads();
+  // ene_act = Re sum int1e(i,j) den1(j,i) + 1/2 Re sum int2e(i,j,k,l) den2(j,i,l,k)
+  double part = 0.0;
+  const int n2 = n * n, n4 = n2 * n2;
+  for (int e = tid; e < n4; e += blockDim.x) {
+    int i = e % n, j = (e / n) % n, k = (e / n2) % n, l = e / (n2 * n);
+    cplx p = cmul(a.int2e[e], a.den2[j + n * (i + n * (l + n * k))]);
+    part += 0.5 * p.x;
+  }
+  for (int e = tid; e < n2; e += blockDim.x) {
+    int i = e % n, j = e / n;
+    cplx p = cmul(a.int1e[i + n * j], a.den1[j + n * i]);
+    part += p.x;
+  }
+  red[tid] = part;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) { if (tid < s) red[tid] += red[tid + s]; __syncthreads(); }
+  const double ene_act = red[0];
+  __syncthreads();
+  // ene_dcore = Re sum_{dc} <phi|g + 2(h0+h1)|phi> = Re [A(i,i) + E(i)]
+  double ed = 0.0;
+  for (int i = nfc; i < nc; ++i) ed += resv(a, 0, i, i).x + resv(a, 3, i, i).x;
+  if (tid == 0) {
+    a.ene[0] = a.ene_fcore; a.ene[1] = ed; a.ene[2] = a.ene_fcore + ed; a.ene[3] = ene_act;
+    a.ene[4] = a.ene_fcore + ed + ene_act;
+  }
+  // X matrix
+  const cplx tfac = a.icomp == 0 ? mkc(a.dtime, 0) : mkc(0, a.dtime);
+  for (int e = tid; e < nf * nf; e += blockDim.x) a.xmat[e] = mkc(0, 0);
+  __syncthreads();
+  // _fc: X(j,i) = tfac (<(h0+h1) phi_j|phi_i> + <phi_j|(g+v2) phi_i>), j frozen, i dynamic
+  for (int e = tid; e < nfc * (nf - nfc); e += blockDim.x) {
+    int j = e % nfc, i = nfc + e / nfc;
+    cplx v = mkc(0, 0);
+    if (a.mval[j] == a.mval[i]) v = cadd(resv(a, 2, j, i), resv(a, 4, j, i));
+    a.xmat[j + nf * i] = cmul(v, tfac);
+  }
+  // _cc
+  for (int e = tid; e < (nc - nfc) * (nc - nfc); e += blockDim.x) {
+    int j = nfc + e % (nc - nfc), i = nfc + e / (nc - nfc);
+    a.xmat[j + nf * i] = cmul(F[j + nf * i], tfac);
+  }
+  // _aa1 (nsub = 1)
+  for (int e = tid; e < n * n; e += blockDim.x) {
+    int j = nc + e % n, i = nc + e / n;
+    if (a.mval[j] == a.mval[i]) a.xmat[j + nf * i] = cmul(F[j + nf * i], tfac);
+  }
+  // _ca0 / _ca
+  if (n > 0 && nc > nfc) {
+    if (n * 2 == a.nelact) {
+      for (int e = tid; e < (nc - nfc) * n; e += blockDim.x) {
+        int i = nfc + e % (nc - nfc), j = nc + e / (nc - nfc);
+        a.xmat[j + nf * i] = cmul(F[j + nf * i], tfac);
+        a.xmat[i + nf * j] = cmul(F[i + nf * j], tfac);
+      }
+    } else if (tid == 0) {
+      // fmat(j,i) = 2 F(j,i) - sum_k den1(ja,ka) conj(F(i,k)); bmat = -tfac rrden fmat
+      for (int i = nfc; i < nc; ++i) {
+        cplx Fm[16];
+        for (int ja = 0; ja < n; ++ja) {
+          int jf = nc + ja;
+          cplx t = mkc(0, 0);
+          for (int ka = 0; ka < n; ++ka) t = cadd(t, cmul(a.den1[ja + n * ka], cconj(F[i + nf * (nc + ka)])));
+          Fm[ja] = csub(cadd(F[jf + nf * i], F[jf + nf * i]), t);
+        }
+        for (int ja = 0; ja < n; ++ja) {
+          int jf = nc + ja;
+          cplx t = mkc(0, 0);
+          for (int ka = 0; ka < n; ++ka) t = cadd(t, cmul(a.rrden[ja + n * ka], Fm[ka]));
+          cplx bm = cscale(cmul(tfac, t), -1.0);
+          a.xmat[jf + nf * i] = cadd(cmul(F[jf + nf * i], tfac), bm);
+          a.xmat[i + nf * jf] = cadd(cmul(F[i + nf * jf], tfac), cscale(cconj(bm), -1.0));
+        }
+      }
+    }
+  }
+}
+
+// hwfn_i = tf2 (v2 + g + h1 + h0)_i + sum_{j, m_j = m_i} orb_j X(j,i)
+// (hprod_htot_dtorb.F90:54-104); frozen-core rows are zero.
+__global__ void dtorb_kernel(int Nr, int L1, int nfun, int nfcore, int icomp, double dtime, const int* __restrict__ mval,
+                             const cplx* __restrict__ orb, const cplx* __restrict__ h0, const cplx* __restrict__ h1,
+                             const cplx* __restrict__ gg, const cplx* __restrict__ v2, const cplx* __restrict__ xmat,
+                             cplx* __restrict__ hwfn) {
+  const size_t nb = (size_t)Nr * L1;
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb * nfun) return;
+  const int i = (int)(t / nb);
+  const size_t k = t % nb;
+  if (i < nfcore) { hwfn[t] = mkc(0, 0); return; }
+  const cplx tf2 = icomp == 0 ? mkc(-dtime, 0) : mkc(0, -dtime);
+  cplx h = cadd(cadd(cadd(v2[t], gg[t]), h1[t]), h0[t]);
+  cplx o = cmul(h, tf2);
+  const int mi = mval[i];
+  for (int j = 0; j < nfun; ++j) {
+    if (mval[j] != mi) continue;
+    o = cadd(o, cmul(orb[(size_t)j * nb + k], xmat[j + nfun * i]));
+  }
+  hwfn[t] = o;
+}
+
+// ===========================================================================
+// host set-up helpers
+// ===========================================================================
+int build_tables(Ctx& c) {
+  const int bw = 2 * c.nd + 1;
+  c.xrad = dupload(c.h_xrad);
+  c.mask = dupload(c.h_mask);
+  c.radk = dupload(c.h_radk);
+  c.radk0 = dupload(c.h_radk0);
+  c.radp = dupload(c.h_radp);
+  c.cost = dupload(c.h_cost);
+  c.legf1 = dupload(c.h_legf1); c.legb1 = dupload(c.h_legb1);
+  c.legf2 = dupload(c.h_legf2); c.legb2 = dupload(c.h_legb2);
+  (void)bw;
+  // alph_lm (bas_gen_alph.F90:2-26)
+  std::vector<double> alph((size_t)c.L1 * (2 * c.mmax1 + 1), 0.0);
+  for (int m = -c.mmax1; m <= c.mmax1; ++m)
+    for (int l = std::abs(m); l <= c.lmax1; ++l)
+      alph[(size_t)(m + c.mmax1) * c.L1 + l] = std::sqrt(((l + 1.0) * (l + 1.0) - (double)m * m) / ((2.0 * l + 1) * (2.0 * l + 3)));
+  c.alph = dupload(alph);
+  // Poisson factors (bas_gen_d2fac.F90:2-60, hprod_mkv2mf.F90:140-142)
+  const int Nr = c.Nr;
+  std::vector<double> rpl0((size_t)Nr * c.L2), rpl1(rpl0.size()), invr(rpl0.size()), fac2(rpl0.size()), fac1(c.L2);
+  const double r2pi = 0.5 / PI;
+  for (int l = 0; l <= c.lmax2; ++l) {
+    for (int ir = 1; ir <= Nr; ++ir) {
+      double x = c.h_xrad[ir], sw = std::sqrt(c.h_wrad[ir]);
+      size_t k = (size_t)l * Nr + ir - 1;
+      double xl = 1.0;
+      for (int e = 0; e < l; ++e) xl *= x;
+      rpl0[k] = xl * r2pi;
+      rpl1[k] = xl * x * sw;
+      invr[k] = (2 * l + 1) / (x * sw) * r2pi;
+      fac2[k] = 4.0 * PI / (2 * l + 1) / (x * sw);
+    }
+    double xr = c.h_xrad[Nr + 1], p = 1.0;
+    for (int e = 0; e < 2 * l + 1; ++e) p *= xr;
+    fac1[l] = 1.0 / p;
+  }
+  c.rpl0 = dupload(rpl0); c.rpl1 = dupload(rpl1); c.invr = dupload(invr); c.fac2 = dupload(fac2); c.fac1 = dupload(fac1);
+  // Cholesky factors on the device
+  c.d2ll = dalloc<double>((size_t)(c.nd + 1) * Nr * c.L2);
+  c.d2rinv = dalloc<double>((size_t)Nr * c.L2);
+  int* dstat = dalloc<int>(1);
+  d2ll_factor_kernel<<<(c.L2 + 31) / 32, 32>>>(Nr, c.nd, c.L2, c.xrad, c.radk, c.d2ll, c.d2rinv, dstat);
+  int hst = 0;
+  cudaMemcpy(&hst, dstat, sizeof(int), cudaMemcpyDeviceToHost);
+  if (hst) { fprintf(stderr, "td1c_b200: Poisson band factorisation failed\n"); return ST_CHOLESKY; }
+  c.tdiag = dalloc<double>((size_t)Nr * c.L1);
+  c.v2jfc = dalloc<double>(Nr);
+  tdiag_kernel<<<(Nr * c.L1 + 255) / 256, 256>>>(Nr, c.L1, c.nd, c.znuc, c.xrad, c.radk, c.radk0, nullptr, c.tdiag);
+  c.d_mval = dupload(c.mval);
+  return (int)cudaGetLastError();
+}
+
+int build_pairs(Ctx& c) {
+  // 'dyn' pairs (a >= b, both dynamic), then 'fc1dyn' (a dynamic, b frozen),
+  // then 'fcfc' (set-up only)
+  c.pa.clear(); c.pb.clear();
+  for (int b = c.nfcore; b < c.nfun; ++b)
+    for (int a = b; a < c.nfun; ++a) { c.pa.push_back(a); c.pb.push_back(b); }
+  for (int b = 0; b < c.nfcore; ++b)
+    for (int a = c.nfcore; a < c.nfun; ++a) { c.pa.push_back(a); c.pb.push_back(b); }
+  c.npair = (int)c.pa.size();
+  for (int b = 0; b < c.nfcore; ++b)
+    for (int a = b; a < c.nfcore; ++a) { c.pa.push_back(a); c.pb.push_back(b); }
+  c.npair_all = (int)c.pa.size();
+  c.nfcfc = c.npair_all - c.npair;
+  std::vector<int> pm(c.npair_all), po(c.nfun * c.nfun, -1), pc(c.nfun * c.nfun, 0);
+  for (int p = 0; p < c.npair_all; ++p) {
+    int a = c.pa[p], b = c.pb[p];
+    pm[p] = c.mval[b] - c.mval[a];
+    po[a * c.nfun + b] = p; pc[a * c.nfun + b] = 0;
+    if (a != b) { po[b * c.nfun + a] = p; pc[b * c.nfun + a] = 1; }
+  }
+  c.pair_m = dupload(pm); c.pair_of = dupload(po); c.pair_cj = dupload(pc);
+  return 0;
+}
+
+int build_state(Ctx& c) {
+  c.nbas = (size_t)c.Nr * c.L1; c.nbas2 = (size_t)c.Nr * c.L2; c.ngrid = (size_t)c.Nr * c.nlat;
+  const size_t so = c.nbas * c.nfun, sg = c.ngrid * c.nfun;
+  c.orb = dalloc<cplx>(so); c.orb0 = dalloc<cplx>(so); c.h0orb = dalloc<cplx>(so); c.h1orb = dalloc<cplx>(so);
+  c.gorb = dalloc<cplx>(so); c.v2orb = dalloc<cplx>(so);
+  c.orbg0 = dalloc<cplx>(c.ngrid * std::max(1, c.nfcore));
+  c.orbg = dalloc<cplx>(sg); c.gorbg = dalloc<cplx>(sg); c.v2orbg = dalloc<cplx>(sg);
+  c.rho2 = dalloc<cplx>(c.nbas2 * c.npair_all); c.v2sph = dalloc<cplx>(c.nbas2 * c.npair_all);
+  c.W = dalloc<cplx>(c.ngrid * c.npair_all);
+  c.wfn_io = dalloc<cplx>(so); c.hwfn_io = dalloc<cplx>(so);
+  c.lfield = dalloc<double>(9);
+  c.xmat = dalloc<cplx>((size_t)c.nfun * c.nfun);
+  c.ene = dalloc<double>(5);
+  c.d_status = dalloc<int>(1);
+  c.d_scalar = dalloc<double>(4);
+  if (!c.orb || !c.W || !c.rho2 || !c.v2sph) return ST_CUDA;
+  return 0;
+}
+
+void batch_upload(LegGemmBatch*& dst, const std::vector<LegGemmBatch>& v) { dst = v.empty() ? nullptr : dupload(v); }
+
+int build_batches(Ctx& c) {
+  const int N = 2 * c.Nr;
+  auto lf1 = [&](int m) { return c.legf1 + (size_t)(m + c.mmax1) * c.nlat * c.L1; };
+  auto lb1 = [&](int m) { return c.legb1 + (size_t)(m + c.mmax1) * c.L1 * c.nlat; };
+  auto lf2 = [&](int m) { return c.legf2 + (size_t)(m + c.mmax2) * c.nlat * c.L2; };
+  auto lb2 = [&](int m) { return c.legb2 + (size_t)(m + c.mmax2) * c.L2 * c.nlat; };
+  std::vector<LegGemmBatch> v;
+  // sph2ang1 of dynamic orbitals: orbg[f] = legf1[m] (nlat x L1) * orb[f] (L1 x 2Nr)
+  for (int f = c.nfcore; f < c.nfun; ++f)
+    v.push_back({lf1(c.mval[f]), (const double*)(c.orb + f * c.nbas), nullptr, (double*)(c.orbg + f * c.ngrid), N, N});
+  c.n_orbg = (int)v.size(); batch_upload(c.b_orbg, v); v.clear();
+  // sph2ang1 of the stored frozen core (set-up): orbg0[f] = legf1 * orb0[f]
+  for (int f = 0; f < c.nfcore; ++f)
+    v.push_back({lf1(c.mval[f]), (const double*)(c.orb0 + f * c.nbas), nullptr, (double*)(c.orbg0 + f * c.ngrid), N, N});
+  batch_upload(c.b_orbg0, v); v.clear();
+  // ang2sph1 of the gauge-transformed frozen core: orb[f] = legb1 (L1 x nlat) * orbg[f]
+  for (int f = 0; f < c.nfcore; ++f)
+    v.push_back({lb1(c.mval[f]), (const double*)(c.orbg + f * c.ngrid), nullptr, (double*)(c.orb + f * c.nbas), N, N});
+  c.n_orbfc = (int)v.size(); batch_upload(c.b_orbfc, v); v.clear();
+  // pair density -> rho2 (M = L2, K = nlat)
+  for (int p = 0; p < c.npair; ++p) {
+    int a = c.pa[p], b = c.pb[p];
+    v.push_back({lb2(c.mval[b] - c.mval[a]), (const double*)(c.orbg + a * c.ngrid), (const double*)(c.orbg + b * c.ngrid),
+                 (double*)(c.rho2 + (size_t)p * c.nbas2), N, N});
+  }
+  batch_upload(c.b_rho, v); v.clear();
+  for (int p = c.npair; p < c.npair_all; ++p) {
+    int a = c.pa[p], b = c.pb[p];
+    v.push_back({lb2(c.mval[b] - c.mval[a]), (const double*)(c.orbg + a * c.ngrid), (const double*)(c.orbg + b * c.ngrid),
+                 (double*)(c.rho2 + (size_t)p * c.nbas2), N, N});
+  }
+  batch_upload(c.b_rho_fcfc, v); v.clear();
+  // W = legf2 (nlat x L2) * v2sph
+  for (int p = 0; p < c.npair_all; ++p) {
+    int a = c.pa[p], b = c.pb[p];
+    v.push_back({lf2(c.mval[b] - c.mval[a]), (const double*)(c.v2sph + (size_t)p * c.nbas2), nullptr,
+                 (double*)(c.W + (size_t)p * c.ngrid), N, N});
+  }
+  {
+    std::vector<LegGemmBatch> v1(v.begin(), v.begin() + c.npair), v2(v.begin() + c.npair, v.end());
+    batch_upload(c.b_W, v1); batch_upload(c.b_W_fcfc, v2);
+  }
+  v.clear();
+  // ang2sph1 of g and v2 for dynamic orbitals (M = L1, K = nlat)
+  for (int f = c.nfcore; f < c.nfun; ++f)
+    v.push_back({lb1(c.mval[f]), (const double*)(c.gorbg + f * c.ngrid), nullptr, (double*)(c.gorb + f * c.nbas), N, N});
+  for (int f = c.nfcore; f < c.nfun; ++f)
+    v.push_back({lb1(c.mval[f]), (const double*)(c.v2orbg + f * c.ngrid), nullptr, (double*)(c.v2orb + f * c.nbas), N, N});
+  c.n_gorb = (int)v.size(); batch_upload(c.b_gorb, v); v.clear();
+  for (int f = 0; f < c.nfcore; ++f)
+    v.push_back({lb1(c.mval[f]), (const double*)(c.gorbg + f * c.ngrid), nullptr, (double*)(c.gorb + f * c.nbas), N, N});
+  batch_upload(c.b_gorbfc, v);
+  return 0;
+}
+
+int build_reductions(Ctx& c) {
+  // orbdots entries: kind 0 (A) and 1 (B) for dynamic j, i of equal m (and the
+  // frozen j for kind 2 (C) and 4 (<phi_j|(g+v2) phi_i>)); kind 3 (E) for dynamic cores
+  std::vector<int> idx(5 * c.nfun * c.nfun, -1);
+  c.h_ent.clear();
+  auto add = [&](int kind, int j, int i) {
+    idx[(kind * c.nfun + j) * c.nfun + i] = (int)c.h_ent.size();
+    c.h_ent.push_back(make_int4(kind, j, i, 0));
+  };
+  for (int i = c.nfcore; i < c.nfun; ++i)
+    for (int j = c.nfcore; j < c.nfun; ++j)
+      if (c.mval[j] == c.mval[i]) { add(0, j, i); add(1, j, i); }
+  for (int i = c.nfcore; i < c.nfun; ++i)
+    for (int j = 0; j < c.nfcore; ++j)
+      if (c.mval[j] == c.mval[i]) { add(2, j, i); add(4, j, i); }
+  for (int i = c.nfcore; i < c.ncore; ++i) add(3, i, i);
+  c.ent_index = dupload(idx);
+  c.od.nbas = (int)c.nbas; c.od.nfun = c.nfun; c.od.nent = (int)c.h_ent.size();
+  c.od.orb = c.orb; c.od.h0orb = c.h0orb; c.od.h1orb = c.h1orb; c.od.gorb = c.gorb; c.od.v2orb = c.v2orb;
+  c.od.ent = dupload(c.h_ent);
+  const int nchunk = (int)((c.nbas + 127) / 128);
+  c.od.partial = dalloc<cplx>((size_t)nchunk * std::max(1, c.od.nent));
+  c.od.result = dalloc<cplx>(std::max(1, c.od.nent));
+  // int2e blocks by delta = m_i - m_j
+  const int n = c.nact, nc = c.ncore;
+  std::vector<Int2eBlock> blocks;
+  std::vector<int> rows;
+  std::vector<int2> cols;
+  std::vector<int4> dst;
+  if (n > 0) {
+    int dmax = 0;
+    for (int a = 0; a < n; ++a) for (int b = 0; b < n; ++b) dmax = std::max(dmax, std::abs(c.mval[nc + a] - c.mval[nc + b]));
+    for (int d = -dmax; d <= dmax; ++d) {
+      std::vector<int> r_ij; std::vector<std::pair<int, int>> rr;
+      for (int ia = 0; ia < n; ++ia)
+        for (int ja = 0; ja <= ia; ++ja)
+          if (c.mval[nc + ia] - c.mval[nc + ja] == d) rr.push_back({ia, ja});
+      std::vector<std::pair<int, int>> cc;
+      for (int ka = 0; ka < n; ++ka)
+        for (int la = 0; la < n; ++la)
+          if (c.mval[nc + la] - c.mval[nc + ka] == d) cc.push_back({ka, la});
+      if (rr.empty() || cc.empty()) continue;
+      // split into chunks: rows <= 32, cols <= 96, rows * ceil(cols/3) <= 256
+      const int cchunk = std::min((int)cc.size(), 96);
+      const int rchunk = std::max(1, std::min(32, 256 / ((cchunk + 2) / 3)));
+      for (size_t r0 = 0; r0 < rr.size(); r0 += rchunk)
+        for (size_t c0 = 0; c0 < cc.size(); c0 += cchunk) {
+          int nr = (int)std::min((size_t)rchunk, rr.size() - r0), ncl = (int)std::min((size_t)cchunk, cc.size() - c0);
+          Int2eBlock bk{};
+          bk.row0 = (int)rows.size(); bk.nrow = nr; bk.col0 = (int)cols.size(); bk.ncol = ncl; bk.ent0 = (int)dst.size();
+          for (int x = 0; x < nr; ++x) {
+            int ia = rr[r0 + x].first, ja = rr[r0 + x].second;
+            rows.push_back(c.pair_of ? 0 : 0);
+            // stored pair of (i, j): a = i >= b = j
+            int p = -1;
+            for (int q = 0; q < c.npair; ++q) if (c.pa[q] == nc + ia && c.pb[q] == nc + ja) p = q;
+            rows.back() = p;
+          }
+          for (int y = 0; y < ncl; ++y) {
+            int ka = cc[c0 + y].first, la = cc[c0 + y].second;
+            int kf = nc + ka, lf = nc + la, p = -1, cj = 0;
+            for (int q = 0; q < c.npair; ++q) {
+              if (c.pa[q] == kf && c.pb[q] == lf) { p = q; cj = 0; }
+              if (c.pa[q] == lf && c.pb[q] == kf) { p = q; cj = 1; }
+            }
+            cols.push_back(make_int2(p, cj));
+          }
+          for (int x = 0; x < nr; ++x)
+            for (int y = 0; y < ncl; ++y)
+              dst.push_back(make_int4(rr[r0 + x].first, rr[r0 + x].second, cc[c0 + y].first, cc[c0 + y].second));
+          blocks.push_back(bk);
+        }
+    }
+  }
+  c.i2.nact = n; c.i2.nblocks = (int)blocks.size(); c.i2.nblkent = (int)dst.size(); c.i2.K = c.nbas2;
+  c.i2.blocks = dupload(blocks); c.i2.row_pair = dupload(rows); c.i2.col_pair = dupload(cols); c.i2.ent_dst = dupload(dst);
+  c.i2.rho2 = c.rho2; c.i2.v2sph = c.v2sph;
+  c.i2.partial = dalloc<cplx>((size_t)c.i2_nsplit * std::max(1, c.i2.nblkent));
+  c.int2e = dalloc<cplx>((size_t)std::max(1, n * n * n * n));
+  c.i2.int2e = c.int2e;
+  // act2 entry list (m-allowed (ij, kl), ordered by ij as in hprod_mfprod2_act2)
+  std::vector<Act2Entry> al;
+  int ij = 0;
+  for (int ia = 0; ia < n; ++ia)
+    for (int ja = 0; ja <= ia; ++ja, ++ij)
+      for (int ka = 0; ka < n; ++ka)
+        for (int la = 0; la < n; ++la) {
+          int ifn = nc + ia, jfn = nc + ja, kfn = nc + ka, lfn = nc + la;
+          if (c.mval[ifn] + c.mval[kfn] != c.mval[jfn] + c.mval[lfn]) continue;
+          Act2Entry e{};
+          e.ij = ij;
+          int p = -1, cj = 0;
+          for (int q = 0; q < c.npair; ++q) {
+            if (c.pa[q] == kfn && c.pb[q] == lfn) { p = q; cj = 0; }
+            if (c.pa[q] == lfn && c.pb[q] == kfn) { p = q; cj = 1; }
+          }
+          e.pair = p; e.conj = cj;
+          e.d2idx = ja + n * (ia + n * (la + n * ka));
+          al.push_back(e);
+        }
+  c.nact2 = (int)al.size();
+  c.act2_list = dupload(al);
+  return 0;
+}
+
+int build_ci(Ctx& c) {
+  const int n = c.nact;
+  c.den1 = dalloc<cplx>(std::max(1, n * n)); c.rden = dalloc<cplx>(std::max(1, n * n)); c.rrden = dalloc<cplx>(std::max(1, n * n));
+  c.int1e = dalloc<cplx>(std::max(1, n * n)); c.den2 = dalloc<cplx>((size_t)std::max(1, n * n * n * n));
+  if (n == 0) {
+    c.lcic = 1;
+    c.cic = dalloc<cplx>(1); c.cic_io = dalloc<cplx>(1); c.hcic_io = dalloc<cplx>(1);
+    return 0;
+  }
+  if (n > 16) return ST_CONFIG;
+  const int na = c.nela - c.ncore, nb = c.nelb - c.ncore;
+  std::vector<int> orbm(n);
+  for (int a = 0; a < n; ++a) orbm[a] = c.mval[c.ncore + a];
+  auto build = [&](int nel, std::vector<unsigned>& s, std::vector<int>& M, std::vector<int>& idx) {
+    std::vector<std::pair<int, unsigned>> tmp;
+    for (unsigned b = 0; b < (1u << n); ++b) {
+      if (__builtin_popcount(b) != nel) continue;
+      int mm = 0;
+      for (int a = 0; a < n; ++a) if ((b >> a) & 1u) mm += orbm[a];
+      tmp.push_back({mm, b});
+    }
+    std::sort(tmp.begin(), tmp.end());
+    s.clear(); M.clear(); idx.assign(1u << n, -1);
+    for (size_t k = 0; k < tmp.size(); ++k) { s.push_back(tmp[k].second); M.push_back(tmp[k].first); idx[tmp[k].second] = (int)k; }
+  };
+  std::vector<int> Ma, Mb, ia_idx, ib_idx;
+  build(na, c.h_stra, Ma, ia_idx);
+  build(nb, c.h_strb, Mb, ib_idx);
+  c.nstr_a = (int)c.h_stra.size(); c.nstr_b = (int)c.h_strb.size();
+  int mmaxa = 0;
+  for (int a = 0; a < n; ++a) mmaxa = std::max(mmaxa, std::abs(orbm[a]));
+  c.smin = c.mtot - 2 * mmaxa; c.nsec = 4 * mmaxa + 1;
+  std::vector<int> soff((size_t)c.nsec * c.nstr_b, -1), sfirst((size_t)c.nsec * c.nstr_b, 0), scnt((size_t)c.nsec * c.nstr_b, 0);
+  std::vector<int> ssize(c.nsec, 0), sbase(c.nsec, 0), sdetA, sdetB;
+  for (int sec = 0; sec < c.nsec; ++sec) {
+    int S = c.smin + sec, off = 0;
+    sbase[sec] = (int)sdetA.size();
+    for (int ib = 0; ib < c.nstr_b; ++ib) {
+      int need = S - Mb[ib], f = -1, cnt = 0;
+      for (int ia = 0; ia < c.nstr_a; ++ia) if (Ma[ia] == need) { if (f < 0) f = ia; cnt++; }
+      if (cnt > 0) {
+        soff[(size_t)sec * c.nstr_b + ib] = off; sfirst[(size_t)sec * c.nstr_b + ib] = f; scnt[(size_t)sec * c.nstr_b + ib] = cnt;
+        for (int k = 0; k < cnt; ++k) { sdetA.push_back(f + k); sdetB.push_back(ib); }
+        off += cnt;
+      }
+    }
+    ssize[sec] = off;
+    c.maxsec = std::max(c.maxsec, off);
+  }
+  const int sec0 = c.mtot - c.smin;
+  c.lcic = ssize[sec0];
+  c.h_detoff.assign(c.nstr_b, -1); c.h_afirst.assign(c.nstr_b, 0); c.h_acount.assign(c.nstr_b, 0);
+  std::vector<int> deta, detb;
+  for (int ib = 0; ib < c.nstr_b; ++ib) {
+    c.h_detoff[ib] = soff[(size_t)sec0 * c.nstr_b + ib];
+    c.h_afirst[ib] = sfirst[(size_t)sec0 * c.nstr_b + ib];
+    c.h_acount[ib] = scnt[(size_t)sec0 * c.nstr_b + ib];
+  }
+  for (int K = 0; K < c.lcic; ++K) { deta.push_back(sdetA[sbase[sec0] + K]); detb.push_back(sdetB[sbase[sec0] + K]); }
+  // D vector offsets (pq = p + n q in sector mtot + m_p - m_q)
+  std::vector<long> doff(n * n, 0);
+  long tot = 0;
+  for (int q = 0; q < n; ++q)
+    for (int p = 0; p < n; ++p) {
+      int sec = c.mtot + orbm[p] - orbm[q] - c.smin;
+      doff[p + n * q] = tot;
+      tot += ssize[sec];
+    }
+  // pq groups by delta = m_p - m_q (group index delta - (smin - mtot))
+  std::vector<int> dgrp, dgoff(c.nsec + 1, 0);
+  for (int gI = 0; gI < c.nsec; ++gI) {
+    int delta = gI + (c.smin - c.mtot);
+    dgoff[gI] = (int)dgrp.size();
+    for (int q = 0; q < n; ++q)
+      for (int p = 0; p < n; ++p)
+        if (orbm[p] - orbm[q] == delta) dgrp.push_back(p + n * q);
+  }
+  dgoff[c.nsec] = (int)dgrp.size();
+  // den2 quadruples with m_p - m_q = m_s - m_r
+  std::vector<int4> quads;
+  for (int s = 0; s < n; ++s)
+    for (int r = 0; r < n; ++r)
+      for (int q = 0; q < n; ++q)
+        for (int p = 0; p < n; ++p)
+          if (orbm[p] - orbm[q] == orbm[s] - orbm[r]) quads.push_back(make_int4(p, q, r, s));
+  c.spin_sym = (c.smul == 1 && na == nb) ? 1 : 0;
+  CiTables& t = c.cit;
+  t.nact = n; t.nstr_a = c.nstr_a; t.nstr_b = c.nstr_b; t.mtot = c.mtot; t.spin_sym = c.spin_sym;
+  t.smin = c.smin; t.nsec = c.nsec;
+  t.stra = dupload(c.h_stra); t.strb = dupload(c.h_strb);
+  t.idx_a = dupload(ia_idx); t.idx_b = dupload(ib_idx); t.Ma = dupload(Ma); t.Mb = dupload(Mb);
+  t.sec_off = dupload(soff); t.sec_first = dupload(sfirst); t.sec_cnt = dupload(scnt); t.sec_size = dupload(ssize);
+  t.dvec_off = dupload(doff); t.det_a = dupload(deta); t.det_b = dupload(detb); t.orb_m = dupload(orbm);
+  t.lcic = c.lcic; t.sec_detA = dupload(sdetA); t.sec_detB = dupload(sdetB); t.sec_base = dupload(sbase);
+  t.dgrp = dupload(dgrp); t.dgrp_off = dupload(dgoff); t.quads = dupload(quads); t.nquad = (int)quads.size();
+  c.Da = dalloc<cplx>(tot); c.Db = dalloc<cplx>(tot); c.T = dalloc<cplx>(tot);
+  c.cic = dalloc<cplx>(c.lcic); c.cic_io = dalloc<cplx>(c.lcic); c.hcic_io = dalloc<cplx>(c.lcic);
+  return 0;
+}
+
+// ===========================================================================
+// the RHS
+// ===========================================================================
+int gemm(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
+  c.launches++;
+  return launch_legendre_gemm(b, nb, M, K, 2 * c.Nr, pair, c.st);
+}
+
+// d_lf: device lfield[9]; wfn/cic device inputs; hwfn/hcic device outputs
+int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cplx* hwfn, cplx* hcic, double dtime) {
+  cudaStream_t st = c.st;
+  const size_t so = c.nbas * c.nfun, sg = c.ngrid * c.nfun;
+  int rc = 0;
+  // scratch initialisation (hprod_htot_init.F90)
+  cudaMemsetAsync(c.gorbg, 0, sg * sizeof(cplx), st);
+  cudaMemsetAsync(c.v2orbg, 0, sg * sizeof(cplx), st);
+  cudaMemsetAsync(c.gorb, 0, so * sizeof(cplx), st);
+  cudaMemsetAsync(c.v2orb, 0, so * sizeof(cplx), st);
+  // orbitals (hprod_orbin.F90)
+  cudaMemcpyAsync(c.orb + c.nfcore * c.nbas, wfn + c.nfcore * c.nbas, (so - c.nfcore * c.nbas) * sizeof(cplx),
+                  cudaMemcpyDeviceToDevice, st);
+  if (c.n_orbg) rc |= gemm(c, c.b_orbg, c.n_orbg, c.nlat, c.L1, false);
+  if (c.nfcore > 0) {
+    if (c.igauge == 0) {
+      cudaMemcpyAsync(c.orb, c.orb0, c.nfcore * c.nbas * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(c.orbg, c.orbg0, c.nfcore * c.ngrid * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+    } else {
+      size_t nfc = c.ngrid * c.nfcore;
+      fc_phase_kernel<<<(unsigned)((nfc + 255) / 256), 256, 0, st>>>(c.Nr, c.nlat, c.nfcore, c.xrad, c.cost, d_lf, c.orbg0, c.orbg);
+      c.launches++;
+      rc |= gemm(c, c.b_orbfc, c.n_orbfc, c.L1, c.nlat, false);
+    }
+  }
+  // RDMs (ormas_mkden1/2, hprod_invden)
+  CiArgs ca{};
+  ca.t = c.cit; ca.cic = cic_in; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
+  ca.sigma = hcic; ca.int1e = c.int1e; ca.int2e = c.int2e; ca.ene_act = c.ene + 3; ca.dtime = dtime; ca.icomp = c.icomp;
+  if (c.nact > 0) {
+    rc |= launch_ci_dvec(ca, c.maxsec, st);
+    rc |= launch_ci_rdm(ca, st);
+    int need_rr = (c.ncore > 0 && c.nact * 2 != c.nelact) ? 1 : 0;
+    invden_kernel<<<1, 64, 0, st>>>(c.nact, need_rr, c.den1, c.rden, c.rrden, c.d_status);
+    c.launches += 6;
+  }
+  // one-body
+  OneBodyArgs ob{};
+  ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = c.igauge;
+  ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
+  ob.mval = c.d_mval; ob.orb = c.orb; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = d_lf;
+  rc |= launch_onebody(ob, st);
+  c.launches++;
+  // mean field
+  if (c.neltot >= 2 && c.npair > 0) {
+    rc |= gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true);
+    PoissonArgs pa{};
+    pa.Nr = c.Nr; pa.L2 = c.L2; pa.nd = c.nd; pa.npair = c.npair; pa.d2ll = c.d2ll; pa.d2rinv = c.d2rinv;
+    pa.rpl0 = c.rpl0; pa.rpl1 = c.rpl1; pa.invr = c.invr; pa.fac2 = c.fac2; pa.fac1 = c.fac1; pa.pair_m = c.pair_m;
+    pa.rho2 = c.rho2; pa.v2sph = c.v2sph;
+    rc |= launch_poisson(pa, sizeof(double) * (size_t)c.Nr * (c.nd + 1), st);
+    c.launches++;
+    rc |= gemm(c, c.b_W, c.npair, c.nlat, c.L2, false);
+    MfprodArgs mf{};
+    mf.ngrid = (int)c.ngrid; mf.nfun = c.nfun; mf.npair = c.npair; mf.W = c.W; mf.orbg = c.orbg; mf.gorbg = c.gorbg;
+    mf.v2orbg = c.v2orbg; mf.act2_list = c.act2_list; mf.nact2 = c.nact2; mf.nact = c.nact; mf.ncore = c.ncore;
+    mf.nfcore = c.nfcore; mf.den1 = c.den1; mf.den2 = c.den2; mf.rden = c.rden; mf.mval = c.d_mval;
+    mf.pair_of = c.pair_of; mf.pair_cj = c.pair_cj; mf.nelact = c.nelact;
+    rc |= launch_mfprod(mf, st);
+    c.launches += 2;
+    rc |= gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false);
+  }
+  // integrals
+  rc |= launch_orbdots(c.od, st);
+  c.launches += 2;
+  if (c.nact > 0) { rc |= launch_int2e(c.i2, c.i2_nsplit, st); c.launches += 3; }
+  SmallArgs sa{};
+  sa.nfun = c.nfun; sa.nfcore = c.nfcore; sa.ndcore = c.ndcore; sa.nact = c.nact; sa.ncore = c.ncore; sa.nelact = c.nelact;
+  sa.icomp = c.icomp; sa.dtime = dtime; sa.ene_fcore = c.ene_fcore; sa.mval = c.d_mval; sa.ent_index = c.ent_index;
+  sa.res = c.od.result; sa.den1 = c.den1; sa.den2 = c.den2; sa.rrden = c.rrden; sa.int1e = c.int1e; sa.int2e = c.int2e;
+  sa.xmat = c.xmat; sa.ene = c.ene;
+  smallmat_kernel<<<1, 256, 0, st>>>(sa);
+  c.launches++;
+  // CI sigma (ormas_xact2 -> ormas_hcic)
+  if (c.nact > 0) { rc |= launch_ci_sigma(ca, c.maxsec, st); c.launches += 2; }
+  else cudaMemsetAsync(hcic, 0, sizeof(cplx), st);
+  // dtorb
+  dtorb_kernel<<<(unsigned)((so + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, c.icomp, dtime, c.d_mval, c.orb,
+                                                             c.h0orb, c.h1orb, c.gorb, c.v2orb, c.xmat, hwfn);
+  c.launches++;
+  rc |= (int)cudaGetLastError();
+  return rc;
+}
+
+// ===========================================================================
+// RK4 (clcrk::prop, src/prop/clcrk.cpp:55-87; tableau set_coeff_04 221-235)
+// ===========================================================================
+// y += wy k ;  ynext = y0 + wn k   (orbitals and CI handled as two segments)
+__global__ void rk_combine_kernel(size_t n, cplx* __restrict__ y, const cplx* __restrict__ y0, const cplx* __restrict__ k,
+                                  cplx* __restrict__ ynext, double wy, double wn, int do_next) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  cplx kv = k[t];
+  cplx yv = y[t];
+  yv.x = fma(wy, kv.x, yv.x); yv.y = fma(wy, kv.y, yv.y);
+  y[t] = yv;
+  if (do_next) {
+    cplx a = y0[t];
+    a.x = fma(wn, kv.x, a.x); a.y = fma(wn, kv.y, a.y);
+    ynext[t] = a;
+  }
+}
+
+// wfn_mask (src/wfn/wfn_mask.F90:2-35): orb(irad, l, i) *= mask(irad) for
+// dynamic i, l >= |m_i|, irad >= min_irad
+__global__ void mask_kernel(int Nr, int L1, int nfun, int nfcore, int min_irad, const int* __restrict__ mval,
+                            const double* __restrict__ mask, cplx* __restrict__ y) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nb = (size_t)Nr * L1;
+  if (t >= nb * nfun) return;
+  const int f = (int)(t / nb);
+  const int l = (int)((t % nb) / Nr), r = (int)(t % Nr);
+  const int am = mval[f] < 0 ? -mval[f] : mval[f];
+  if (f < nfcore || l < am || r + 1 < min_irad) return;
+  y[t] = cscale(y[t], mask[r + 1]);
+}
+
+// copy the four stage fields of the current step from the table and advance
+__global__ void field_select_kernel(const double* __restrict__ tab, int* __restrict__ counter, int nstep,
+                                    double* __restrict__ cur) {
+  int s = *counter;
+  if (s >= nstep) s = nstep - 1;
+  for (int e = threadIdx.x; e < 36; e += blockDim.x) cur[e] = tab[(size_t)s * 36 + e];
+}
+__global__ void counter_inc_kernel(int* counter) { if (threadIdx.x == 0) *counter += 1; }
+
+// sin^2 pulse (clfield1.cpp:15-115 set-up, 253-300 E explicit, 472-500
+// A explicit, 573-620 E as the 6-point derivative of A in velocity1)
+struct Pulse { double famp, freq, period, numcyc, cep; int igauge; };
+double pulse_a(const Pulse& p, double t) {
+  if (!(t > 0 && t < p.numcyc * p.period)) return 0.0;
+  double env = std::sin(PI * t / (p.numcyc * p.period));
+  env *= env;
+  return env * p.famp / p.freq * std::sin(p.freq * t + p.cep);
+}
+double pulse_e(const Pulse& p, double t) {
+  if (!(t > 0 && t < p.numcyc * p.period)) return 0.0;
+  double env = std::sin(PI * t / (p.numcyc * p.period));
+  env *= env;
+  return env * p.famp * std::sin(p.freq * t + p.cep);
+}
+void pulse_lfield(const Pulse& p, double t, double* lf) {
+  for (int i = 0; i < 9; ++i) lf[i] = 0.0;
+  double A = pulse_a(p, t);
+  if (p.igauge == 1) {
+    const double dstep = 2 * PI / (1239.84190 / (800.0 * 27.2113845)) / 100000.0;
+    double e = 0;
+    e += pulse_a(p, t + 3 * dstep) / 60.0;
+    e -= pulse_a(p, t + 2 * dstep) / 20.0 * 3.0;
+    e += pulse_a(p, t + dstep) / 4.0 * 3.0;
+    e -= pulse_a(p, t - dstep) / 4.0 * 3.0;
+    e += pulse_a(p, t - 2 * dstep) / 20.0 * 3.0;
+    e -= pulse_a(p, t - 3 * dstep) / 60.0;
+    lf[2] = A; lf[5] = -e / dstep; lf[8] = A;
+  } else {
+    double E = pulse_e(p, t);
+    lf[2] = E; lf[5] = E; lf[8] = A;
+  }
+}
+
+struct RkBufs {
+  cplx *y0 = nullptr, *yt = nullptr, *k = nullptr;  // orbitals then CI, contiguous
+  double* lf_cur = nullptr;
+  int* counter = nullptr;
+  size_t cap = 0;
+};
+RkBufs g_rk;
+
+int rk_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int nstep) {
+  cudaStream_t st = c.st;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic;
+  RkBufs& b = g_rk;
+  const double wts[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+  const double anext[4] = {0.5, 0.5, 1.0, 0.0};
+  field_select_kernel<<<1, 64, 0, st>>>(c.field_tab, b.counter, nstep, b.lf_cur);
+  c.launches++;
+  cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(b.y0 + no, y_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  int rc = 0;
+  for (int is = 0; is < 4; ++is) {
+    const cplx* in = (is == 0) ? b.y0 : b.yt;
+    rc |= run_htot(c, b.lf_cur + 9 * is, in, in + no, b.k, b.k + no, 1.0);
+    const int nxt = is < 3 ? 1 : 0;
+    rk_combine_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(no, y_orb, b.y0, b.k, b.yt, dt * wts[is], dt * anext[is], nxt);
+    rk_combine_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(nc, y_cic, b.y0 + no, b.k + no, b.yt + no, dt * wts[is],
+                                                                  dt * anext[is], nxt);
+    c.launches += 2;
+  }
+  int min_irad = 1;
+  for (int ir = 1; ir <= c.Nr; ++ir) if (c.h_xrad[ir] > c.rmask) { min_irad = ir; break; }
+  mask_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, min_irad, c.d_mval, c.mask, y_orb);
+  counter_inc_kernel<<<1, 32, 0, st>>>(b.counter);
+  c.launches += 2;
+  rc |= (int)cudaGetLastError();
+  return rc;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+int td1c_gpu_bind_rad(int nfe, int ndvr, int nrad, const double* xrad, const double* wrad, const double* radp,
+                      const double* radk, const double* radk0, double rmask, const double* mask) {
+  Ctx& c = ctx();
+  c.nfe = nfe; c.nd = ndvr; c.nrad = nrad; c.Nr = nrad - 1; c.rmask = rmask;
+  const size_t n1 = nrad + 1, nb = (size_t)(2 * ndvr + 1) * n1;
+  c.h_xrad.assign(xrad, xrad + n1); c.h_wrad.assign(wrad, wrad + n1); c.h_mask.assign(mask, mask + n1);
+  c.h_radp.assign(radp, radp + nb); c.h_radk.assign(radk, radk + nb); c.h_radk0.assign(radk0, radk0 + nb);
+  c.have_rad = true;
+  return 0;
+}
+
+int td1c_gpu_bind_sph(int lmax1, int lmax2, int mmax1, int mmax2, int nlat, const double* wlat, const double* cost,
+                      const double* legf1, const double* legb1, const double* legf2, const double* legb2) {
+  Ctx& c = ctx();
+  c.lmax1 = lmax1; c.lmax2 = lmax2; c.mmax1 = mmax1; c.mmax2 = mmax2; c.nlat = nlat; c.L1 = lmax1 + 1; c.L2 = lmax2 + 1;
+  c.h_wlat.assign(wlat, wlat + nlat); c.h_cost.assign(cost, cost + nlat);
+  size_t s1 = (size_t)nlat * c.L1 * (2 * mmax1 + 1), s2 = (size_t)nlat * c.L2 * (2 * mmax2 + 1);
+  c.h_legf1.assign(legf1, legf1 + s1); c.h_legb1.assign(legb1, legb1 + s1);
+  c.h_legf2.assign(legf2, legf2 + s2); c.h_legb2.assign(legb2, legb2 + s2);
+  c.have_sph = true;
+  return 0;
+}
+
+int td1c_gpu_bind_bas(double znuc, int smul, int mtot, int nfun, const int* otype, const int* mval, const int* lval,
+                      int nela, int nelb) {
+  Ctx& c = ctx();
+  c.znuc = znuc; c.smul = smul; c.mtot = mtot; c.nfun = nfun; c.nela = nela; c.nelb = nelb;
+  c.otype.assign(otype, otype + nfun); c.mval.assign(mval, mval + nfun); c.lval.assign(lval, lval + nfun);
+  c.nfcore = c.ndcore = c.nact = 0;
+  for (int i = 0; i < nfun; ++i) {
+    if (otype[i] == -1) c.nfcore++;
+    else if (otype[i] == 0) c.ndcore++;
+    else if (otype[i] == 1) c.nact++;
+    else return ST_CONFIG;
+    if (i > 0 && otype[i] < otype[i - 1]) return ST_CONFIG;
+  }
+  c.ncore = c.nfcore + c.ndcore;
+  c.neltot = nela + nelb;
+  c.nelact = nela + nelb - 2 * c.ncore;
+  c.have_bas = true;
+  return 0;
+}
+
+int td1c_gpu_bind_control(int icomp, int igauge) {
+  Ctx& c = ctx();
+  c.icomp = icomp; c.igauge = igauge;
+  return 0;
+}
+
+void hprod_bind_(double* ene_fcore, double* ene_dcore, double* ene_core, double* ene_act, double* ene_tot, double* dip_exp,
+                 double* vel_exp, double* acc_exp, const bool* projhigh, const double* cutoff) {
+  Ctx& c = ctx();
+  c.p_ene_fcore = ene_fcore; c.p_ene_dcore = ene_dcore; c.p_ene_core = ene_core; c.p_ene_act = ene_act; c.p_ene_tot = ene_tot;
+  (void)dip_exp; (void)vel_exp; (void)acc_exp; (void)projhigh; (void)cutoff;
+}
+
+void hprod_init_(void) {
+  Ctx& c = ctx();
+  if (!c.have_rad || !c.have_sph || !c.have_bas) { c.status |= ST_CONFIG; return; }
+  if (c.nfun > 16) { c.status |= ST_CONFIG; return; }
+  if (!c.st) cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking);
+  int rc = build_tables(c);
+  rc |= build_pairs(c);
+  rc |= build_state(c);
+  rc |= build_ci(c);
+  rc |= build_batches(c);
+  rc |= build_reductions(c);
+  cudaDeviceSynchronize();
+  rc |= (int)cudaGetLastError();
+  if (rc) { c.status |= ST_CUDA; return; }
+  c.initialized = true;
+}
+
+void hprod_set_wfn0_(const double* wfn, const double* cic, const char* v2xfc_type, int len) {
+  Ctx& c = ctx();
+  (void)cic; (void)v2xfc_type; (void)len;
+  if (!c.initialized) { c.status |= ST_CONFIG; return; }
+  cudaStream_t st = c.st;
+  const size_t so = c.nbas * c.nfun;
+  cudaMemcpyAsync(c.orb0, wfn, so * sizeof(cplx), cudaMemcpyHostToDevice, st);
+  c.ene_fcore = 0;
+  if (c.nfcore == 0 || c.neltot < 2) {
+    cudaMemsetAsync(c.v2jfc, 0, c.Nr * sizeof(double), st);
+    cudaStreamSynchronize(st);
+    return;
+  }
+  // sph2ang1 of the stored frozen core (lfield = 0: no gauge phase)
+  launch_legendre_gemm(c.b_orbg0, c.nfcore, c.nlat, c.L1, 2 * c.Nr, false, st);
+  // frozen-core Hartree potential (hprod_mkrhofc, hprod_mkv2jfc)
+  int* d_lval = dupload(c.lval);
+  v2jfc_kernel<<<1, 1, 0, st>>>(c.Nr, c.nd, c.L1, c.nfcore, c.d_mval, d_lval, c.orb0, c.d2ll, c.d2rinv, c.rpl0, c.rpl1, c.invr,
+                                c.fac2, c.h_xrad[c.Nr + 1], c.v2jfc);
+  // frozen-core pair potentials and energy (hprod_v2fc_enefc): orb(fc) = orb0 projected,
+  // orbg(fc) = orbg0; fcfc pair densities, Poisson, l->theta
+  cudaMemcpyAsync(c.orbg, c.orbg0, c.nfcore * c.ngrid * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  if (c.igauge == 0) cudaMemcpyAsync(c.orb, c.orb0, c.nfcore * c.nbas * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  else launch_legendre_gemm(c.b_orbfc, c.nfcore, c.L1, c.nlat, 2 * c.Nr, false, st);  // orb(fc) = ang2sph1(orbg(fc))
+  launch_legendre_gemm(c.b_rho_fcfc, c.nfcfc, c.L2, c.nlat, 2 * c.Nr, true, st);
+  PoissonArgs pa{};
+  pa.Nr = c.Nr; pa.L2 = c.L2; pa.nd = c.nd; pa.npair = c.nfcfc; pa.d2ll = c.d2ll; pa.d2rinv = c.d2rinv;
+  pa.rpl0 = c.rpl0; pa.rpl1 = c.rpl1; pa.invr = c.invr; pa.fac2 = c.fac2; pa.fac1 = c.fac1; pa.pair_m = c.pair_m + c.npair;
+  pa.rho2 = c.rho2 + c.npair * c.nbas2; pa.v2sph = c.v2sph + c.npair * c.nbas2;
+  launch_poisson(pa, sizeof(double) * (size_t)c.Nr * (c.nd + 1), st);
+  launch_legendre_gemm(c.b_W_fcfc, c.nfcfc, c.nlat, c.L2, 2 * c.Nr, false, st);
+  // frozen-core energy: enefc = 2 Re <phi|h0|phi> + Re <phi| v2jfc - sum_j W(j,i) phi_j >
+  // with h0 from the bare kinetic table (before v2jfc is added)
+  OneBodyArgs ob{};
+  ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfcore; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = 0;
+  ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
+  ob.mval = c.d_mval; ob.orb = c.orb; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = c.lfield;
+  cudaMemsetAsync(c.lfield, 0, 9 * sizeof(double), st);
+  launch_onebody(ob, st);
+  dot_re_kernel<<<1, 256, 0, st>>>(c.orb, c.h0orb, c.nfcore * c.nbas, c.d_scalar);
+  const size_t nfcg = c.nfcore * c.ngrid;
+  fc_g_kernel<<<(unsigned)((nfcg + 255) / 256), 256, 0, st>>>(c.Nr, c.nlat, c.nfcore, c.nfun, c.orbg, c.W, c.pair_of,
+                                                              c.pair_cj, c.v2jfc, c.gorbg);
+  launch_legendre_gemm(c.b_gorbfc, c.nfcore, c.L1, c.nlat, 2 * c.Nr, false, st);
+  dot_re_kernel<<<1, 256, 0, st>>>(c.orb, c.gorb, c.nfcore * c.nbas, c.d_scalar + 1);
+  double es[2] = {0, 0};
+  cudaMemcpyAsync(es, c.d_scalar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  c.ene_fcore = 2.0 * es[0] + es[1];
+  // hprod_addfc_tmat: add v2jfc to the kinetic diagonal
+  tdiag_kernel<<<(c.Nr * c.L1 + 255) / 256, 256, 0, st>>>(c.Nr, c.L1, c.nd, c.znuc, c.xrad, c.radk, c.radk0, c.v2jfc, c.tdiag);
+  cudaStreamSynchronize(st);
+  if (cudaGetLastError() != cudaSuccess) c.status |= ST_CUDA;
+}
+
+void hprod_htot_(const double* dtime, const double* lfield, const double* wfn, const double* cic, double* hwfn, double* hcic) {
+  Ctx& c = ctx();
+  if (!c.initialized) { c.status |= ST_CONFIG; return; }
+  cudaStream_t st = c.st;
+  const size_t so = c.nbas * c.nfun;
+  cudaMemcpyAsync(c.lfield, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c.wfn_io, wfn, so * sizeof(cplx), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c.cic_io, cic, c.lcic * sizeof(cplx), cudaMemcpyHostToDevice, st);
+  int rc = run_htot(c, c.lfield, c.wfn_io, c.cic_io, c.hwfn_io, c.hcic_io, *dtime);
+  cudaMemcpyAsync(hwfn, c.hwfn_io, so * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(hcic, c.hcic_io, c.lcic * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(c.h_ene, c.ene, 5 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  int dst = 0;
+  cudaMemcpyAsync(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc || e != cudaSuccess) c.status |= ST_CUDA;
+  c.status |= dst;
+  if (c.p_ene_fcore) *c.p_ene_fcore = c.h_ene[0];
+  if (c.p_ene_dcore) *c.p_ene_dcore = c.h_ene[1];
+  if (c.p_ene_core) *c.p_ene_core = c.h_ene[2];
+  if (c.p_ene_act) *c.p_ene_act = c.h_ene[3];
+  if (c.p_ene_tot) *c.p_ene_tot = c.h_ene[4];
+}
+
+void hprod_final_(void) {
+  if (!g) return;
+  Ctx& c = *g;
+  for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  if (c.st) cudaStreamSynchronize(c.st);
+  for (void* p : g_allocs) cudaFree(p);
+  g_allocs.clear();
+  g_rk = RkBufs();
+  if (c.st) cudaStreamDestroy(c.st);
+  delete g;
+  g = nullptr;
+}
+
+int td1c_gpu_last_status(void) { return g ? g->status : 0; }
+
+int td1c_gpu_dims(int* d) {
+  Ctx& c = ctx();
+  int v[16] = {c.nrad, (int)c.nbas, (int)c.nbas2, (int)c.ngrid, c.nlat, c.lcic, c.nfcore, c.ndcore, c.nact, c.ncore,
+               c.nstr_a, c.nstr_b, c.npair, c.nd, c.lmax1, c.lmax2};
+  memcpy(d, v, sizeof(v));
+  return 0;
+}
+
+int td1c_gpu_ci_tables(unsigned* stra, unsigned* strb, int* detoff, int* afirst, int* acount) {
+  Ctx& c = ctx();
+  if (stra) std::copy(c.h_stra.begin(), c.h_stra.end(), stra);
+  if (strb) std::copy(c.h_strb.begin(), c.h_strb.end(), strb);
+  if (detoff) std::copy(c.h_detoff.begin(), c.h_detoff.end(), detoff);
+  if (afirst) std::copy(c.h_afirst.begin(), c.h_afirst.end(), afirst);
+  if (acount) std::copy(c.h_acount.begin(), c.h_acount.end(), acount);
+  return 0;
+}
+
+int td1c_gpu_energies(double* e) {
+  Ctx& c = ctx();
+  cudaMemcpy(c.h_ene, c.ene, 5 * sizeof(double), cudaMemcpyDeviceToHost);
+  memcpy(e, c.h_ene, sizeof(c.h_ene));
+  return 0;
+}
+
+int td1c_gpu_htot_dev(double dtime, const double* lfield, const void* d_wfn, const void* d_cic, void* d_hwfn, void* d_hcic) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  cudaMemcpyAsync(c.lfield, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, c.st);
+  int rc = run_htot(c, c.lfield, (const cplx*)d_wfn, (const cplx*)d_cic, (cplx*)d_hwfn, (cplx*)d_hcic, dtime);
+  return rc ? ST_CUDA : 0;
+}
+
+int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                 double cep, int use_graph) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  if (nstep <= 0) return 0;
+  cudaStream_t st = c.st;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic;
+  RkBufs& b = g_rk;
+  if (b.cap < no + nc) {
+    b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc);
+    if (!b.lf_cur) { b.lf_cur = dalloc<double>(36); b.counter = dalloc<int>(1); }
+    b.cap = no + nc;
+  }
+  // stage fields of every step (clcrk.cpp:62-73: t + dt * c_s)
+  Pulse p;
+  p.famp = std::sqrt(fint / 3.50944506E+16); p.freq = 1239.84190 / (wlen * 27.2113845);
+  p.period = 2 * PI / p.freq; p.numcyc = numcyc; p.cep = cep / 180.0 * PI; p.igauge = c.igauge;
+  std::vector<double> tab((size_t)nstep * 36);
+  const double nodes[4] = {0.0, 0.5, 0.5, 1.0};
+  for (int s = 0; s < nstep; ++s)
+    for (int is = 0; is < 4; ++is) pulse_lfield(p, t0 + dt * s + dt * nodes[is], &tab[(size_t)s * 36 + 9 * is]);
+  if (c.field_cap < nstep) {
+    c.field_tab = dalloc<double>((size_t)nstep * 36);
+    c.field_cap = nstep;
+  }
+  cudaMemcpyAsync(c.field_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(b.counter, 0, sizeof(int), st);
+  c.launches = 0;
+  cplx* y = (cplx*)d_wfn;
+  cplx* yc = (cplx*)d_cic;
+  int rc = 0;
+  int s0 = 0;
+  if (!use_graph) {
+    for (int s = 0; s < nstep; ++s) rc |= rk_step(c, y, yc, dt, nstep);
+  } else {
+    // first step eagerly (sets kernel attributes), then one captured step replayed
+    rc |= rk_step(c, y, yc, dt, nstep);
+    s0 = 1;
+    if (nstep > 1) {
+      if (c.graph_exec[0]) { cudaGraphExecDestroy(c.graph_exec[0]); c.graph_exec[0] = nullptr; }
+      long l0 = c.launches;
+      cudaGraph_t graph;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
+      rc |= rk_step(c, y, yc, dt, nstep);
+      if (cudaStreamEndCapture(st, &graph) != cudaSuccess) return ST_CUDA;
+      if (cudaGraphInstantiate(&c.graph_exec[0], graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
+      cudaGraphDestroy(graph);
+      long per = c.launches - l0;
+      c.launches = l0;
+      for (int s = s0; s < nstep; ++s) {
+        if (cudaGraphLaunch(c.graph_exec[0], st) != cudaSuccess) return ST_CUDA;
+        c.launches += per;
+      }
+    }
+  }
+  rc |= (int)cudaGetLastError();
+  return rc ? ST_CUDA : 0;
+}
+
+long td1c_gpu_launch_count(void) { return g ? g->launches : 0; }
+
+int td1c_gpu_sync(void) {
+  Ctx& c = ctx();
+  cudaError_t e = cudaStreamSynchronize(c.st);
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+long td1c_gpu_debug_get(const char* name, double* out, long cap) {
+  Ctx& c = ctx();
+  std::string n(name);
+  const void* src = nullptr;
+  size_t bytes = 0;
+  const size_t so = c.nbas * c.nfun * sizeof(cplx), sg = c.ngrid * c.nfun * sizeof(cplx);
+  if (n == "orb") { src = c.orb; bytes = so; }
+  else if (n == "orbg") { src = c.orbg; bytes = sg; }
+  else if (n == "h0orb") { src = c.h0orb; bytes = so; }
+  else if (n == "h1orb") { src = c.h1orb; bytes = so; }
+  else if (n == "gorb") { src = c.gorb; bytes = so; }
+  else if (n == "v2orb") { src = c.v2orb; bytes = so; }
+  else if (n == "gorbg") { src = c.gorbg; bytes = sg; }
+  else if (n == "v2orbg") { src = c.v2orbg; bytes = sg; }
+  else if (n == "rho2") { src = c.rho2; bytes = c.nbas2 * c.npair * sizeof(cplx); }
+  else if (n == "v2sph") { src = c.v2sph; bytes = c.nbas2 * c.npair * sizeof(cplx); }
+  else if (n == "W") { src = c.W; bytes = c.ngrid * c.npair * sizeof(cplx); }
+  else if (n == "den1") { src = c.den1; bytes = (size_t)c.nact * c.nact * sizeof(cplx); }
+  else if (n == "den2") { src = c.den2; bytes = (size_t)c.nact * c.nact * c.nact * c.nact * sizeof(cplx); }
+  else if (n == "rden") { src = c.rden; bytes = (size_t)c.nact * c.nact * sizeof(cplx); }
+  else if (n == "rrden") { src = c.rrden; bytes = (size_t)c.nact * c.nact * sizeof(cplx); }
+  else if (n == "int1e") { src = c.int1e; bytes = (size_t)c.nact * c.nact * sizeof(cplx); }
+  else if (n == "int2e") { src = c.int2e; bytes = (size_t)c.nact * c.nact * c.nact * c.nact * sizeof(cplx); }
+  else if (n == "xmat") { src = c.xmat; bytes = (size_t)c.nfun * c.nfun * sizeof(cplx); }
+  else if (n == "v2jfc") { src = c.v2jfc; bytes = c.Nr * sizeof(double); }
+  else if (n == "tdiag") { src = c.tdiag; bytes = (size_t)c.Nr * c.L1 * sizeof(double); }
+  else if (n == "d2ll") { src = c.d2ll; bytes = (size_t)c.Nr * c.L2 * (c.nd + 1) * sizeof(double); }
+  else return -1;
+  long nd = (long)(bytes / sizeof(double));
+  if (!out) return nd;
+  if (nd > cap) return -2;
+  cudaStreamSynchronize(c.st);
+  if (bytes) cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost);
+  return nd;
+}
+
+}  // extern "C"

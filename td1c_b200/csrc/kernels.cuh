@@ -1,0 +1,131 @@
+// kernels.cuh -- device data layout and kernel launchers of td1c_b200.
+//
+// HBM layout (all complex arrays are (re,im) double pairs, radial index
+// fastest, i.e. the reference's Fortran column-major order):
+//   orb, h0orb, h1orb, gorb, v2orb : [nfun][L1][Nr]        orb(irad, l, ifun)
+//   orbg, gorbg, v2orbg            : [nfun][nlat][Nr]      orbg(irad, ilat, ifun)
+//   rho2, v2sph                    : [npair][L2][Nr]       rho2(irad, l, a, b) for stored pair p = (a, b)
+//   v2ang (W)                      : [npair][nlat][Nr]     v2ang(irad, ilat, a, b)
+// Stored pairs are (a >= b, both dynamic) followed by (a dynamic, b frozen
+// core); the reference's Hermitian fill v2(.., b, a) = conj(v2(.., a, b))
+// (hprod_mkv2mf.F90:257-345) is never materialised -- consumers read the
+// stored pair with a conjugation flag.
+#pragma once
+#include "common.cuh"
+
+namespace td1c {
+
+struct LegGemmBatch {
+  const double* A;   // real table, M x K row-major (K contiguous)
+  const double* B0;  // slab (K rows x ldb reals) or conj operand for pair mode
+  const double* B1;  // second operand for pair mode
+  double* C;         // output, M rows x ldc reals
+  int ldb, ldc;
+};
+int launch_legendre_gemm(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair,
+                         cudaStream_t st);
+
+// ---- one-body: tprod + zprod/pzprod (hprod_tprod.F90, hprod_zprod.F90, hprod_pzprod.F90)
+struct OneBodyArgs {
+  int Nr, L1, nd, nfun, nfcore, mmax1, igauge;
+  const double* radk;    // (2nd+1) x (nrad+1) band, reference layout
+  const double* radk0;
+  const double* radp;
+  const double* tdiag;   // [L1][Nr] diagonal of tmat (centrifugal + nuclear + radk diag + v2jfc)
+  const double* xrad;    // [nrad+1]
+  const double* alph;    // [(2 mmax1 + 1)][L1]
+  const int* mval;       // [nfun]
+  const cplx* orb;
+  cplx* h0orb;
+  cplx* h1orb;
+  const double* lfield;  // device: lfield(1:3,1:3) column-major (9 doubles)
+};
+int launch_onebody(const OneBodyArgs& a, cudaStream_t st);
+
+// ---- Poisson (hprod_mkv2mf.F90:118-182): per (pair, l) banded Cholesky solve
+struct PoissonArgs {
+  int Nr, L2, nd, npair;
+  const double* d2ll;    // [L2][Nr][nd+1] band Cholesky factor (LAPACK 'L' storage per l)
+  const double* d2rinv;  // [L2][Nr] reciprocal diagonal of the factor
+  const double* rpl0;    // [L2][Nr]
+  const double* rpl1;
+  const double* invr;
+  const double* fac2;
+  const double* fac1;    // [L2]
+  const int* pair_m;     // [npair] m of the pair (m_b - m_a)
+  const cplx* rho2;      // [npair][L2][Nr]
+  cplx* v2sph;           // [npair][L2][Nr]
+};
+int launch_poisson(const PoissonArgs& a, size_t smem_bytes, cudaStream_t st);
+
+// ---- mean-field action on the (r, theta) grid (hprod_mfprod2.F90)
+struct Act2Entry {    // one m-allowed (ij, kl) term of the 2-RDM contraction
+  int ij, pair, conj, d2idx;
+  double cre, cim;    // den2(j,i,l,k), filled on the device each RHS
+};
+struct MfprodArgs {
+  int ngrid, nfun, npair;
+  const cplx* W;        // [npair][ngrid]
+  const cplx* orbg;     // [nfun][ngrid]
+  cplx* gorbg;          // [nfun][ngrid]
+  cplx* v2orbg;         // [nfun][ngrid]
+  Act2Entry* act2_list; int nact2;  // host-built m-allowed list, ordered by ij
+  // active-core terms (actj, actx) into v2orbg -- coefficients depend on den1 (device)
+  int nact, ncore, nfcore;
+  const cplx* den1;     // [nact][nact] (Fortran order)
+  const cplx* den2;     // [nact^4]
+  const cplx* rden;     // [nact][nact]
+  const int* mval;
+  const int* pair_of;   // [nfun][nfun]: stored pair index of (a, b) or of (b, a)
+  const int* pair_cj;   // [nfun][nfun]: 1 when (a, b) is read as conj of stored (b, a)
+  int nelact;           // total active electrons
+};
+int launch_mfprod(const MfprodArgs& a, cudaStream_t st);
+
+
+// ---- CI (ormas_*), full string-product formulation
+struct CiTables {
+  int nact, nstr_a, nstr_b, mtot, spin_sym;
+  int smin, nsec;         // sectors of total M: S = smin .. smin + nsec - 1
+  const unsigned* stra;   // [nstr_a] bit strings sorted by (M, mask)
+  const unsigned* strb;
+  const int* idx_a;       // [2^nact] mask -> string index
+  const int* idx_b;
+  const int* Ma;          // [nstr_a]
+  const int* Mb;
+  const int* sec_off;     // [nsec][nstr_b] offset of beta string block in sector, -1 if empty
+  const int* sec_first;   // [nsec][nstr_b] first alpha string index of the block
+  const int* sec_cnt;     // [nsec][nstr_b]
+  const int* sec_size;    // [nsec]
+  const long* dvec_off;   // [nact*nact] offset of D_pq in the D arrays (complex elements)
+  const int* det_b;       // [lcic] beta string of each determinant of the CI vector (sector mtot)
+  const int* det_a;       // [lcic]
+  const int* orb_m;       // [nact] m of active orbitals
+  int lcic;
+  const int* sec_detA;    // [sum of sector sizes] alpha string of each sector determinant
+  const int* sec_detB;
+  const int* sec_base;    // [nsec] start of each sector in sec_detA/B
+  const int* dgrp;        // pq indices grouped by m_p - m_q
+  const int* dgrp_off;    // [nsec + 1]
+  const int4* quads;      // m-allowed (p,q,r,s) of den2
+  int nquad;
+};
+struct CiArgs {
+  CiTables t;
+  const cplx* cic;
+  cplx* Da;       // alpha part of E_pq c, per pq in its sector
+  cplx* Db;
+  cplx* T;        // T_rs (same layout as D)
+  cplx* den1;     // [nact^2]
+  cplx* den2;     // [nact^4]
+  cplx* sigma;    // [lcic] (output hcic)
+  const cplx* int1e;
+  const cplx* int2e;
+  const double* ene_act;  // device scalar
+  double dtime; int icomp;
+};
+int launch_ci_dvec(const CiArgs& a, int maxsec, cudaStream_t st);
+int launch_ci_rdm(const CiArgs& a, cudaStream_t st);
+int launch_ci_sigma(const CiArgs& a, int maxsec, cudaStream_t st);
+
+}  // namespace td1c

@@ -1,0 +1,184 @@
+// reductions.cu -- orbital matrix elements and MO integrals of the RHS.
+//
+// orbdots: for every (j, i) with m_j = m_i, i dynamic, over the nbas basis
+//   A(j,i) = <phi_j | (g + h1 + h0) phi_i>          hprod_mkint1_sph.F90:2-103
+//   B(j,i) = <phi_j | v2 phi_i>                      (A + B = <phi_j|F phi_i>,
+//                                                    hprod_htot_mkxmat.F90 _cc/_ca/_aa1)
+//   C(j,i) = <(h0 + h1) phi_j | phi_i>, j frozen     hprod_htot_mkxmat.F90:2-77
+//   E(i)   = <phi_i | (h0 + h1) phi_i>, i dynamic core   hprod_ene_dcore.F90
+//   GV(j,i) = <phi_j | (g + v2) phi_i>, j frozen     hprod_htot_mkxmat.F90:2-77
+// as deterministic two-pass reductions (per-chunk partials, then a fixed-
+// order sum), the race-free pattern of the reference's per-thread partial
+// arrays.
+//
+// int2e (hprod_mkint2_sph.F90:2-100): int2e(i,j,k,l) = sum_{r,L} rho2_ij v2sph_kl
+// for i >= j active and m_i + m_k = m_j + m_l.  The m rule splits the
+// (ij) x (kl) matrix into dense blocks by delta = m_i - m_j; each block is a
+// complex GEMM over K = Nr (lmax2 + 1) split across CTAs, with A/B chunks
+// staged in shared memory; partials are summed in a fixed order and the
+// i < j half is filled by int2e(i,j,k,l) = conj(int2e(j,i,l,k)).
+#include "common.cuh"
+#include "kernels.cuh"
+#include "reductions.cuh"
+
+namespace td1c {
+
+constexpr int OD_CHUNK = 128;
+
+__global__ void __launch_bounds__(256) orbdots_kernel(OrbdotsArgs a) {
+  extern __shared__ cplx sm[];
+  const int nfun = a.nfun, C = OD_CHUNK;
+  cplx* so = sm;                       // [nfun][C] orb
+  cplx* sf = so + (size_t)nfun * C;    // [nfun][C] g + h1 + h0
+  cplx* sv = sf + (size_t)nfun * C;    // [nfun][C] v2
+  cplx* sh = sv + (size_t)nfun * C;    // [nfun][C] h0 + h1
+  cplx* sgv = sh + (size_t)nfun * C;   // [nfun][C] g + v2
+  const size_t base = (size_t)blockIdx.x * C;
+  for (int e = threadIdx.x; e < nfun * C; e += blockDim.x) {
+    int f = e / C, k = e % C;
+    size_t g = base + k;
+    cplx o = mkc(0, 0), fv = mkc(0, 0), v = mkc(0, 0), h = mkc(0, 0), gv = mkc(0, 0);
+    if (g < (size_t)a.nbas) {
+      size_t idx = (size_t)f * a.nbas + g;
+      o = a.orb[idx];
+      cplx h0 = a.h0orb[idx], h1 = a.h1orb[idx], gg = a.gorb[idx];
+      fv = cadd(cadd(gg, h1), h0);
+      v = a.v2orb[idx];
+      h = cadd(h0, h1);
+      gv = cadd(gg, v);
+    }
+    so[e] = o; sf[e] = fv; sv[e] = v; sh[e] = h; sgv[e] = gv;
+  }
+  __syncthreads();
+  cplx* out = a.partial + (size_t)blockIdx.x * a.nent;
+  for (int t = threadIdx.x; t < a.nent; t += blockDim.x) {
+    const int4 en = a.ent[t];  // (kind, j, i, 0)
+    const int kind = en.x, j = en.y, i = en.z;
+    cplx s = mkc(0, 0);
+    const cplx* x; const cplx* y;
+    if (kind == 0) { x = so + j * C; y = sf + i * C; }        // A
+    else if (kind == 1) { x = so + j * C; y = sv + i * C; }   // B
+    else if (kind == 2) { x = sh + j * C; y = so + i * C; }   // C
+    else if (kind == 3) { x = so + i * C; y = sh + i * C; }   // E
+    else { x = so + j * C; y = sgv + i * C; }                 // <phi_j|(g+v2) phi_i>
+    for (int k = 0; k < C; ++k) {
+      cplx xv = x[k], yv = y[k];
+      s.x = fma(xv.x, yv.x, fma(xv.y, yv.y, s.x));
+      s.y = fma(xv.x, yv.y, fma(-xv.y, yv.x, s.y));
+    }
+    out[t] = s;
+  }
+}
+
+// fixed-order sum of the per-chunk partials
+__global__ void sum_partials_kernel(const cplx* __restrict__ partial, int nchunk, int nent, cplx* __restrict__ out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nent) return;
+  cplx s = mkc(0, 0);
+  for (int c = 0; c < nchunk; ++c) s = cadd(s, partial[(size_t)c * nent + t]);
+  out[t] = s;
+}
+
+int launch_orbdots(const OrbdotsArgs& a, cudaStream_t st) {
+  const int nchunk = (a.nbas + OD_CHUNK - 1) / OD_CHUNK;
+  size_t smem = sizeof(cplx) * 5 * (size_t)a.nfun * OD_CHUNK;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(orbdots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  orbdots_kernel<<<nchunk, 256, smem, st>>>(a);
+  sum_partials_kernel<<<(a.nent + 127) / 128, 128, 0, st>>>(a.partial, nchunk, a.nent, a.result);
+  return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// int2e block GEMM
+// ---------------------------------------------------------------------------
+constexpr int I2_KC = 16;
+
+__global__ void __launch_bounds__(256) int2e_block_kernel(Int2eArgs a) {
+  __shared__ cplx sA[32][I2_KC + 1];
+  __shared__ cplx sB[96][I2_KC + 1];
+  const Int2eBlock blk = a.blocks[blockIdx.y];
+  const int nr = blk.nrow, nc = blk.ncol;
+  const int ncg = (nc + 2) / 3;             // column groups of 3
+  const int t = threadIdx.x;
+  const int r = t / ncg, cg = t % ncg;
+  const bool active = r < nr;
+  const size_t K = a.K;
+  const size_t kper = (K + gridDim.x - 1) / gridDim.x;
+  const size_t k0 = (size_t)blockIdx.x * kper, k1 = min(K, k0 + kper);
+  cplx acc[3] = {mkc(0, 0), mkc(0, 0), mkc(0, 0)};
+  for (size_t kc = k0; kc < k1; kc += I2_KC) {
+    const int kn = (int)min((size_t)I2_KC, k1 - kc);
+    for (int e = t; e < nr * I2_KC; e += blockDim.x) {
+      int rr = e / I2_KC, kk = e % I2_KC;
+      cplx v = mkc(0, 0);
+      if (kk < kn) v = __ldg(a.rho2 + (size_t)a.row_pair[blk.row0 + rr] * K + kc + kk);
+      sA[rr][kk] = v;
+    }
+    for (int e = t; e < nc * I2_KC; e += blockDim.x) {
+      int cc = e / I2_KC, kk = e % I2_KC;
+      cplx v = mkc(0, 0);
+      if (kk < kn) {
+        int2 pc = a.col_pair[blk.col0 + cc];
+        v = __ldg(a.v2sph + (size_t)pc.x * K + kc + kk);
+        if (pc.y) v = cconj(v);
+      }
+      sB[cc][kk] = v;
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll 4
+      for (int kk = 0; kk < kn; ++kk) {
+        cplx av = sA[r][kk];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          int c = cg * 3 + u;
+          if (c < nc) cfma(acc[u], av, sB[c][kk]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    for (int u = 0; u < 3; ++u) {
+      int c = cg * 3 + u;
+      if (c < nc) a.partial[((size_t)blockIdx.x * a.nblkent) + blk.ent0 + r * nc + c] = acc[u];
+    }
+  }
+}
+
+__global__ void int2e_sum_kernel(Int2eArgs a, int nsplit) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.nblkent) return;
+  cplx s = mkc(0, 0);
+  for (int c = 0; c < nsplit; ++c) s = cadd(s, a.partial[(size_t)c * a.nblkent + t]);
+  int4 d = a.ent_dst[t];  // (i, j, k, l) active indices
+  const int n = a.nact;
+  a.int2e[d.x + n * (d.y + n * (d.z + n * d.w))] = s;
+}
+
+__global__ void int2e_fill_kernel(Int2eArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.nact;
+  if (t >= n * n * n * n) return;
+  int i = t % n, j = (t / n) % n, k = (t / (n * n)) % n, l = t / (n * n * n);
+  if (i < j) a.int2e[t] = cconj(a.int2e[j + n * (i + n * (l + n * k))]);
+}
+
+int launch_int2e(const Int2eArgs& a, int nsplit, cudaStream_t st) {
+  const int n = a.nact, n4 = n * n * n * n;
+  if (n4 == 0) return 0;
+  cudaMemsetAsync(a.int2e, 0, sizeof(cplx) * n4, st);
+  if (a.nblocks > 0) {
+    dim3 grid(nsplit, a.nblocks);
+    int2e_block_kernel<<<grid, 256, 0, st>>>(a);
+    int2e_sum_kernel<<<(a.nblkent + 127) / 128, 128, 0, st>>>(a, nsplit);
+  }
+  int2e_fill_kernel<<<(n4 + 127) / 128, 128, 0, st>>>(a);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace td1c

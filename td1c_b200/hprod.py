@@ -1,0 +1,151 @@
+"""Python host mirror of td1c's clhprod (src/hprod/clhprod.cpp) over the C-ABI.
+
+clhprod::gen binds the energy outputs and calls hprod_init_; set_wfn0 calls
+hprod_set_wfn0_; htot calls hprod_htot_ (clhprod.cpp:29-82).  The grid and
+tables are bound first, as clbas::gen does through bas_rad_bind_ /
+bas_sph_bind_ / bas_bas_bind_ (clbas.cpp:52-146).  All arithmetic happens in
+libtd1c_b200.so on the GPU; this module only moves host buffers.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as _libmod
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class StatusError(RuntimeError):
+    pass
+
+
+class HProd:
+    """One GPU RHS instance (the library holds a single context, like td1c's
+    clhprod singleton, clhprod.cpp:32-34)."""
+
+    def __init__(self, wl, rad, ang):
+        self.lib = _libmod.load()
+        self.wl = wl
+        lib = self.lib
+        orbs = wl["orbitals"]
+        self.nfun = len(orbs)
+        self._keep = []
+
+        def keep(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            self._keep.append(a)
+            return a
+
+        xrad, wrad, mask = keep(rad["xrad"]), keep(rad["wrad"]), keep(rad["mask"])
+        radk, radk0, radp = keep(rad["radk"]), keep(rad["radk0"]), keep(rad["radp"])
+        self._check(lib.td1c_gpu_bind_rad(rad["nfe"], rad["ndvr"], rad["nrad"], _dp(xrad), _dp(wrad), _dp(radp),
+                                          _dp(radk), _dp(radk0), float(rad["rmask"]), _dp(mask)))
+        wlat, cost = keep(ang["wlat"]), keep(ang["cost"])
+        lf1, lb1, lf2, lb2 = keep(ang["legf1"]), keep(ang["legb1"]), keep(ang["legf2"]), keep(ang["legb2"])
+        self._check(lib.td1c_gpu_bind_sph(ang["lmax1"], ang["lmax2"], ang["mmax1"], ang["mmax2"], ang["nlat"],
+                                          _dp(wlat), _dp(cost), _dp(lf1), _dp(lb1), _dp(lf2), _dp(lb2)))
+        ot = np.array([o[3] for o in orbs], dtype=np.int32)
+        mv = np.array([o[2] for o in orbs], dtype=np.int32)
+        lv = np.array([o[1] for o in orbs], dtype=np.int32)
+        self._keep += [ot, mv, lv]
+        self._check(lib.td1c_gpu_bind_bas(float(wl["znuc"]), int(wl.get("smul", 1)), int(wl.get("mtot", 0)),
+                                          self.nfun, _ip(ot), _ip(mv), _ip(lv), int(wl["nela"]), int(wl["nelb"])))
+        self._check(lib.td1c_gpu_bind_control(int(wl.get("icomp", 1)), int(wl["igauge"])))
+        self.ene = np.zeros(8)
+        projhigh = ctypes.c_bool(False)
+        cutoff = ctypes.c_double(0.0)
+        e = self.ene
+        lib.hprod_bind_(*[e[i:].ctypes.data_as(_DP) for i in range(8)], ctypes.byref(projhigh), ctypes.byref(cutoff))
+        self._projhigh, self._cutoff = projhigh, cutoff
+        lib.hprod_init_()
+        self._status()
+        d = (ctypes.c_int * 16)()
+        lib.td1c_gpu_dims(d)
+        names = ["nrad", "nbas", "nbas2", "ngrid", "nlat", "lcic", "nfcore", "ndcore", "nact", "ncore",
+                 "nstr_a", "nstr_b", "npair", "ndvr", "lmax1", "lmax2"]
+        self.dims = dict(zip(names, list(d)))
+
+    def _check(self, rc):
+        if rc != 0:
+            raise StatusError("td1c_b200 call failed with status %d" % rc)
+
+    def _status(self):
+        st = self.lib.td1c_gpu_last_status()
+        if st != 0:
+            raise StatusError("td1c_b200 status %d" % st)
+
+    def ci_tables(self):
+        d = self.dims
+        na, nb = max(d["nstr_a"], 1), max(d["nstr_b"], 1)
+        stra = np.zeros(na, dtype=np.uint32)
+        strb = np.zeros(nb, dtype=np.uint32)
+        detoff = np.zeros(nb, dtype=np.int32)
+        afirst = np.zeros(nb, dtype=np.int32)
+        acount = np.zeros(nb, dtype=np.int32)
+        up = ctypes.POINTER(ctypes.c_uint)
+        self.lib.td1c_gpu_ci_tables(stra.ctypes.data_as(up), strb.ctypes.data_as(up), _ip(detoff), _ip(afirst),
+                                    _ip(acount))
+        return dict(stra=stra[:d["nstr_a"]], strb=strb[:d["nstr_b"]], detoff=detoff[:d["nstr_b"]],
+                    afirst=afirst[:d["nstr_b"]], acount=acount[:d["nstr_b"]])
+
+    def set_wfn0(self, wfn, cic):
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
+        cic = np.ascontiguousarray(cic, dtype=np.complex128)
+        t = b"read"
+        self.lib.hprod_set_wfn0_(_dp(wfn.view(np.float64)), _dp(cic.view(np.float64)), t, len(t))
+        self._status()
+
+    def htot(self, dtime, lfield, wfn, cic):
+        """hprod_htot_ on host buffers; returns (hwfn, hcic)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
+        cic = np.ascontiguousarray(cic, dtype=np.complex128)
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        hw = np.zeros_like(wfn)
+        hc = np.zeros_like(cic)
+        dt = ctypes.c_double(dtime)
+        self.lib.hprod_htot_(ctypes.byref(dt), _dp(lf), _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)),
+                             _dp(hw.view(np.float64)), _dp(hc.view(np.float64)))
+        self._status()
+        return hw, hc
+
+    def energies(self):
+        """ene_fcore, ene_dcore, ene_core, ene_act, ene_tot bound by hprod_bind_."""
+        return dict(zip(["ene_fcore", "ene_dcore", "ene_core", "ene_act", "ene_tot"], self.ene[:5].tolist()))
+
+    def debug(self, name, complex_=True):
+        n = self.lib.td1c_gpu_debug_get(name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        self.lib.td1c_gpu_debug_get(name.encode(), _dp(out), n)
+        return out.view(np.complex128) if complex_ else out
+
+    # device-resident paths (pointers are CUDA device addresses, e.g. torch tensors' data_ptr())
+    def htot_dev(self, dtime, lfield, d_wfn, d_cic, d_hwfn, d_hcic):
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        self._check(self.lib.td1c_gpu_htot_dev(float(dtime), _dp(lf), ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic),
+                                               ctypes.c_void_p(d_hwfn), ctypes.c_void_p(d_hcic)))
+
+    def rk4_dev(self, d_wfn, d_cic, t0, dt, nstep, use_graph=True):
+        wl = self.wl
+        self._check(self.lib.td1c_gpu_rk4(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(t0), float(dt),
+                                          int(nstep), float(wl["fint"]), float(wl["wlen"]), float(wl["numcyc"]),
+                                          float(wl.get("cep", 0.0)), 1 if use_graph else 0))
+
+    def sync(self):
+        self._check(self.lib.td1c_gpu_sync())
+        self._status()
+
+    def launch_count(self):
+        return int(self.lib.td1c_gpu_launch_count())
+
+    def final(self):
+        self.lib.hprod_final_()
