@@ -101,10 +101,22 @@ long td1c_gpu_debug_get(const char* name, double* out, long capacity);
  * per step when use_graph != 0. */
 int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep,
                  double fint, double wlen, double numcyc, double cep, int use_graph);
+/* Make every following td1c_gpu_rk4 step start from the given device state
+ * (NULL, NULL to switch off): each step then performs the complete update on
+ * the same input, for throughput measurement of a fixed synthetic state. */
+int td1c_gpu_rk4_reset(const void* d_wfn0, const void* d_cic0);
 /* Synchronise the library stream. */
 int td1c_gpu_sync(void);
 /* Number of kernel launches issued by the last td1c_gpu_rk4 call. */
 long td1c_gpu_launch_count(void);
+/* The library's CUDA stream (a cudaStream_t), for callers that time or
+ * order their own work against it. */
+void* td1c_gpu_stream(void);
+/* Run the RHS reps times with CUDA events between its phases and return the
+ * mean phase durations in ms[] (phase names comma-separated in names);
+ * returns the number of phases or a status > 0 on failure. */
+int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d_wfn, const void* d_cic,
+                     void* d_hwfn, void* d_hcic, double* ms, char* names, int names_cap);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,10 @@ def load():
     lib.td1c_gpu_rk4.argtypes = [vp, vp, c_double, c_double, c_int, c_double, c_double, c_double, c_double, c_int]
     lib.td1c_gpu_sync.restype = c_int
     lib.td1c_gpu_launch_count.restype = c_long
+    lib.td1c_gpu_stream.restype = vp
+    lib.td1c_gpu_rk4_reset.argtypes = [vp, vp]
+    lib.td1c_gpu_profile.restype = c_int
+    lib.td1c_gpu_profile.argtypes = [c_int, c_double, dp, vp, vp, vp, vp, dp, ctypes.c_char_p, c_int]
     _lib = lib
     return lib
 
@@ -78,4 +82,5 @@ EXPORTED = [
     "hprod_bind_", "hprod_init_", "hprod_set_wfn0_", "hprod_htot_", "hprod_final_",
     "td1c_gpu_last_status", "td1c_gpu_dims", "td1c_gpu_ci_tables", "td1c_gpu_energies",
     "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
+    "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset",
 ]

@@ -101,8 +101,11 @@ struct Ctx {
   std::vector<int4> h_ent;
   int* ent_index = nullptr;  // [5][nfun][nfun] -> entry id or -1 (A, B, C, E, GV)
   Int2eArgs i2{};
-  int i2_nsplit = 64;
-  Act2Entry* act2_list = nullptr; int nact2 = 0;
+  int i2_nsplit = 128;
+  // act2 blocks
+  int a2_nblk = 0, a2_nrow = 0, a2_ncol = 0, a2_ncoef = 0;
+  Act2Block* a2_blk = nullptr; int2* a2_rows = nullptr; int2* a2_cols = nullptr;
+  Act2Coef* a2_map = nullptr; cplx* a2_coef = nullptr;
   // ---- small matrices
   cplx *xmat = nullptr;
   double* ene = nullptr;  // device [5]
@@ -122,7 +125,16 @@ struct Ctx {
   int status = 0;
   int* d_status = nullptr;  // device status word (ST_* bits)
   double* d_scalar = nullptr;
+  // phase timing (off during graph capture)
+  bool profile = false;
+  cudaEvent_t ev[16] = {};
+  int nev = 0;
 };
+
+// phases of run_htot, in order (td1c_gpu_profile reports their durations)
+const char* kPhaseNames[] = {"orbin", "ci_rdm", "onebody", "rho_gemm", "poisson", "w_gemm", "mfprod",
+                             "gorb_gemm", "orbdots", "int2e", "smallmat", "ci_sigma", "dtorb"};
+const int kNumPhases = 13;
 
 Ctx* g = nullptr;
 Ctx& ctx() {
@@ -673,9 +685,9 @@ int build_reductions(Ctx& c) {
         for (int la = 0; la < n; ++la)
           if (c.mval[nc + la] - c.mval[nc + ka] == d) cc.push_back({ka, la});
       if (rr.empty() || cc.empty()) continue;
-      // split into chunks: rows <= 32, cols <= 96, rows * ceil(cols/3) <= 256
-      const int cchunk = std::min((int)cc.size(), 96);
-      const int rchunk = std::max(1, std::min(32, 256 / ((cchunk + 2) / 3)));
+      // split into chunks: rows <= 24, cols <= 36 (the int2e kernel's CTA tile)
+      const int cchunk = std::min((int)cc.size(), 36);
+      const int rchunk = 24;
       for (size_t r0 = 0; r0 < rr.size(); r0 += rchunk)
         for (size_t c0 = 0; c0 < cc.size(); c0 += cchunk) {
           int nr = (int)std::min((size_t)rchunk, rr.size() - r0), ncl = (int)std::min((size_t)cchunk, cc.size() - c0);
@@ -711,28 +723,55 @@ int build_reductions(Ctx& c) {
   c.i2.partial = dalloc<cplx>((size_t)c.i2_nsplit * std::max(1, c.i2.nblkent));
   c.int2e = dalloc<cplx>((size_t)std::max(1, n * n * n * n));
   c.i2.int2e = c.int2e;
-  // act2 entry list (m-allowed (ij, kl), ordered by ij as in hprod_mfprod2_act2)
-  std::vector<Act2Entry> al;
-  int ij = 0;
-  for (int ia = 0; ia < n; ++ia)
-    for (int ja = 0; ja <= ia; ++ja, ++ij)
+  // act2 dense blocks: rows ij (i >= j, m_i - m_j = d) in the reference's
+  // (i outer, j inner) order, columns kl (m_l - m_k = d) in (k outer, l inner)
+  // order, rows chunked by 24
+  {
+    std::vector<Act2Block> blks;
+    std::vector<int2> rws, cls;
+    std::vector<Act2Coef> map;
+    int coff = 0;
+    int dmax = 0;
+    for (int a = 0; a < n; ++a) for (int b = 0; b < n; ++b) dmax = std::max(dmax, std::abs(c.mval[nc + a] - c.mval[nc + b]));
+    for (int d = -dmax; d <= dmax && n > 0; ++d) {
+      std::vector<int2> rr, cc;
+      for (int ia = 0; ia < n; ++ia)
+        for (int ja = 0; ja <= ia; ++ja)
+          if (c.mval[nc + ia] - c.mval[nc + ja] == d) rr.push_back(make_int2(ia, ja));
       for (int ka = 0; ka < n; ++ka)
-        for (int la = 0; la < n; ++la) {
-          int ifn = nc + ia, jfn = nc + ja, kfn = nc + ka, lfn = nc + la;
-          if (c.mval[ifn] + c.mval[kfn] != c.mval[jfn] + c.mval[lfn]) continue;
-          Act2Entry e{};
-          e.ij = ij;
-          int p = -1, cj = 0;
-          for (int q = 0; q < c.npair; ++q) {
-            if (c.pa[q] == kfn && c.pb[q] == lfn) { p = q; cj = 0; }
-            if (c.pa[q] == lfn && c.pb[q] == kfn) { p = q; cj = 1; }
-          }
-          e.pair = p; e.conj = cj;
-          e.d2idx = ja + n * (ia + n * (la + n * ka));
-          al.push_back(e);
+        for (int la = 0; la < n; ++la)
+          if (c.mval[nc + la] - c.mval[nc + ka] == d) cc.push_back(make_int2(ka, la));
+      if (rr.empty() || cc.empty()) continue;
+      const int col0 = (int)cls.size();
+      for (auto& kl : cc) {
+        int kf = nc + kl.x, lf = nc + kl.y, p = -1, cj = 0;
+        for (int q = 0; q < c.npair; ++q) {
+          if (c.pa[q] == kf && c.pb[q] == lf) { p = q; cj = 0; }
+          if (c.pa[q] == lf && c.pb[q] == kf) { p = q; cj = 1; }
         }
-  c.nact2 = (int)al.size();
-  c.act2_list = dupload(al);
+        cls.push_back(make_int2(p, cj));
+      }
+      for (size_t r0 = 0; r0 < rr.size(); r0 += 24) {
+        Act2Block bk{};
+        bk.row0 = (int)rws.size(); bk.nrow = (int)std::min((size_t)24, rr.size() - r0);
+        bk.col0 = col0; bk.ncol = (int)cc.size(); bk.coff = coff;
+        for (int x = 0; x < bk.nrow; ++x) rws.push_back(rr[r0 + x]);
+        for (int y = 0; y < bk.ncol; ++y)
+          for (int x = 0; x < bk.nrow; ++x) {
+            int ia = rr[r0 + x].x, ja = rr[r0 + x].y, ka = cc[y].x, la = cc[y].y;
+            Act2Coef m{};
+            m.d2idx = ja + n * (ia + n * (la + n * ka));
+            m.dst = coff + y * bk.nrow + x;
+            map.push_back(m);
+          }
+        coff += bk.nrow * bk.ncol;
+        blks.push_back(bk);
+      }
+    }
+    c.a2_nblk = (int)blks.size(); c.a2_nrow = (int)rws.size(); c.a2_ncol = (int)cls.size(); c.a2_ncoef = coff;
+    c.a2_blk = dupload(blks); c.a2_rows = dupload(rws); c.a2_cols = dupload(cls); c.a2_map = dupload(map);
+    c.a2_coef = dalloc<cplx>(std::max(1, coff));
+  }
   return 0;
 }
 
@@ -844,20 +883,28 @@ int gemm(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
   return launch_legendre_gemm(b, nb, M, K, 2 * c.Nr, pair, c.st);
 }
 
+// report the first failing launcher of an RHS (status ST_CUDA is set by the caller)
+int chk(const char* what, int rc) {
+  if (rc != 0) fprintf(stderr, "td1c_b200: %s failed: %s\n", what, cudaGetErrorString((cudaError_t)rc));
+  return rc;
+}
+
 // d_lf: device lfield[9]; wfn/cic device inputs; hwfn/hcic device outputs
 int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cplx* hwfn, cplx* hcic, double dtime) {
   cudaStream_t st = c.st;
   const size_t so = c.nbas * c.nfun, sg = c.ngrid * c.nfun;
   int rc = 0;
+  int iev = 0;
+  auto mark = [&]() { if (c.profile && iev < 16) cudaEventRecord(c.ev[iev++], st); };
+  mark();
   // scratch initialisation (hprod_htot_init.F90)
-  cudaMemsetAsync(c.gorbg, 0, sg * sizeof(cplx), st);
-  cudaMemsetAsync(c.v2orbg, 0, sg * sizeof(cplx), st);
+  (void)sg;  // gorbg / v2orbg rows of dynamic orbitals are fully written by mfprod
   cudaMemsetAsync(c.gorb, 0, so * sizeof(cplx), st);
   cudaMemsetAsync(c.v2orb, 0, so * sizeof(cplx), st);
   // orbitals (hprod_orbin.F90)
   cudaMemcpyAsync(c.orb + c.nfcore * c.nbas, wfn + c.nfcore * c.nbas, (so - c.nfcore * c.nbas) * sizeof(cplx),
                   cudaMemcpyDeviceToDevice, st);
-  if (c.n_orbg) rc |= gemm(c, c.b_orbg, c.n_orbg, c.nlat, c.L1, false);
+  if (c.n_orbg) rc |= chk("orbg gemm", gemm(c, c.b_orbg, c.n_orbg, c.nlat, c.L1, false));
   if (c.nfcore > 0) {
     if (c.igauge == 0) {
       cudaMemcpyAsync(c.orb, c.orb0, c.nfcore * c.nbas * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
@@ -866,50 +913,64 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
       size_t nfc = c.ngrid * c.nfcore;
       fc_phase_kernel<<<(unsigned)((nfc + 255) / 256), 256, 0, st>>>(c.Nr, c.nlat, c.nfcore, c.xrad, c.cost, d_lf, c.orbg0, c.orbg);
       c.launches++;
-      rc |= gemm(c, c.b_orbfc, c.n_orbfc, c.L1, c.nlat, false);
+      rc |= chk("fc gemm", gemm(c, c.b_orbfc, c.n_orbfc, c.L1, c.nlat, false));
     }
   }
+  mark();  // end orbin
   // RDMs (ormas_mkden1/2, hprod_invden)
   CiArgs ca{};
   ca.t = c.cit; ca.cic = cic_in; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
   ca.sigma = hcic; ca.int1e = c.int1e; ca.int2e = c.int2e; ca.ene_act = c.ene + 3; ca.dtime = dtime; ca.icomp = c.icomp;
   if (c.nact > 0) {
-    rc |= launch_ci_dvec(ca, c.maxsec, st);
-    rc |= launch_ci_rdm(ca, st);
+    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, st));
+    rc |= chk("ci rdm", launch_ci_rdm(ca, st));
     int need_rr = (c.ncore > 0 && c.nact * 2 != c.nelact) ? 1 : 0;
     invden_kernel<<<1, 64, 0, st>>>(c.nact, need_rr, c.den1, c.rden, c.rrden, c.d_status);
     c.launches += 6;
   }
+  mark();  // end ci_rdm
   // one-body
   OneBodyArgs ob{};
   ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = c.igauge;
   ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
   ob.mval = c.d_mval; ob.orb = c.orb; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = d_lf;
-  rc |= launch_onebody(ob, st);
+  rc |= chk("onebody", launch_onebody(ob, st));
   c.launches++;
+  mark();  // end onebody
   // mean field
   if (c.neltot >= 2 && c.npair > 0) {
-    rc |= gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true);
+    rc |= chk("rho gemm", gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true));
+    mark();  // end rho_gemm
     PoissonArgs pa{};
     pa.Nr = c.Nr; pa.L2 = c.L2; pa.nd = c.nd; pa.npair = c.npair; pa.d2ll = c.d2ll; pa.d2rinv = c.d2rinv;
     pa.rpl0 = c.rpl0; pa.rpl1 = c.rpl1; pa.invr = c.invr; pa.fac2 = c.fac2; pa.fac1 = c.fac1; pa.pair_m = c.pair_m;
     pa.rho2 = c.rho2; pa.v2sph = c.v2sph;
-    rc |= launch_poisson(pa, sizeof(double) * (size_t)c.Nr * (c.nd + 1), st);
+    rc |= chk("poisson", launch_poisson(pa, 0, st));
     c.launches++;
-    rc |= gemm(c, c.b_W, c.npair, c.nlat, c.L2, false);
+    mark();  // end poisson
+    rc |= chk("W gemm", gemm(c, c.b_W, c.npair, c.nlat, c.L2, false));
+    mark();  // end w_gemm
     MfprodArgs mf{};
-    mf.ngrid = (int)c.ngrid; mf.nfun = c.nfun; mf.npair = c.npair; mf.W = c.W; mf.orbg = c.orbg; mf.gorbg = c.gorbg;
-    mf.v2orbg = c.v2orbg; mf.act2_list = c.act2_list; mf.nact2 = c.nact2; mf.nact = c.nact; mf.ncore = c.ncore;
+    mf.ngrid = c.ngrid; mf.nfun = c.nfun; mf.npair = c.npair; mf.W = c.W; mf.orbg = c.orbg; mf.gorbg = c.gorbg;
+    mf.v2orbg = c.v2orbg; mf.nact = c.nact; mf.ncore = c.ncore;
+    mf.nblk = c.a2_nblk; mf.nrow = c.a2_nrow; mf.ncol = c.a2_ncol; mf.ncoef = c.a2_ncoef; mf.blk = c.a2_blk;
+    mf.rows = c.a2_rows; mf.cols = c.a2_cols; mf.coef_map = c.a2_map; mf.coef = c.a2_coef;
     mf.nfcore = c.nfcore; mf.den1 = c.den1; mf.den2 = c.den2; mf.rden = c.rden; mf.mval = c.d_mval;
     mf.pair_of = c.pair_of; mf.pair_cj = c.pair_cj; mf.nelact = c.nelact;
-    rc |= launch_mfprod(mf, st);
+    rc |= chk("mfprod", launch_mfprod(mf, st));
     c.launches += 2;
-    rc |= gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false);
+    mark();  // end mfprod
+    rc |= chk("gorb gemm", gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false));
+  } else {
+    mark(); mark(); mark(); mark();
   }
+  mark();  // end gorb_gemm
   // integrals
-  rc |= launch_orbdots(c.od, st);
+  rc |= chk("orbdots", launch_orbdots(c.od, st));
   c.launches += 2;
-  if (c.nact > 0) { rc |= launch_int2e(c.i2, c.i2_nsplit, st); c.launches += 3; }
+  mark();  // end orbdots
+  if (c.nact > 0) { rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st)); c.launches += 3; }
+  mark();  // end int2e
   SmallArgs sa{};
   sa.nfun = c.nfun; sa.nfcore = c.nfcore; sa.ndcore = c.ndcore; sa.nact = c.nact; sa.ncore = c.ncore; sa.nelact = c.nelact;
   sa.icomp = c.icomp; sa.dtime = dtime; sa.ene_fcore = c.ene_fcore; sa.mval = c.d_mval; sa.ent_index = c.ent_index;
@@ -917,14 +978,18 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   sa.xmat = c.xmat; sa.ene = c.ene;
   smallmat_kernel<<<1, 256, 0, st>>>(sa);
   c.launches++;
+  mark();  // end smallmat
   // CI sigma (ormas_xact2 -> ormas_hcic)
-  if (c.nact > 0) { rc |= launch_ci_sigma(ca, c.maxsec, st); c.launches += 2; }
+  if (c.nact > 0) { rc |= chk("ci sigma", launch_ci_sigma(ca, c.maxsec, st)); c.launches += 2; }
   else cudaMemsetAsync(hcic, 0, sizeof(cplx), st);
+  mark();  // end ci_sigma
   // dtorb
   dtorb_kernel<<<(unsigned)((so + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, c.icomp, dtime, c.d_mval, c.orb,
                                                              c.h0orb, c.h1orb, c.gorb, c.v2orb, c.xmat, hwfn);
   c.launches++;
-  rc |= (int)cudaGetLastError();
+  mark();  // end dtorb
+  c.nev = iev;
+  rc |= chk("rhs tail", (int)cudaGetLastError());
   return rc;
 }
 
@@ -962,10 +1027,10 @@ __global__ void mask_kernel(int Nr, int L1, int nfun, int nfcore, int min_irad, 
 }
 
 // copy the four stage fields of the current step from the table and advance
-__global__ void field_select_kernel(const double* __restrict__ tab, int* __restrict__ counter, int nstep,
+__global__ void field_select_kernel(const double* __restrict__ tab, int* __restrict__ counter, int unused,
                                     double* __restrict__ cur) {
-  int s = *counter;
-  if (s >= nstep) s = nstep - 1;
+  int s = counter[0];
+  if (s >= counter[1]) s = counter[1] - 1;  // counter[1] = steps staged in the table
   for (int e = threadIdx.x; e < 36; e += blockDim.x) cur[e] = tab[(size_t)s * 36 + e];
 }
 __global__ void counter_inc_kernel(int* counter) { if (threadIdx.x == 0) *counter += 1; }
@@ -1009,6 +1074,12 @@ struct RkBufs {
   double* lf_cur = nullptr;
   int* counter = nullptr;
   size_t cap = 0;
+  const cplx* reset_orb = nullptr;  // optional: every step starts from this state
+  const cplx* reset_cic = nullptr;
+  // cached graph of one step and what it was captured with
+  const void* g_y = nullptr; const void* g_yc = nullptr; const void* g_tab = nullptr;
+  const void* g_ro = nullptr; double g_dt = 0; long g_per = 0;
+  int h_counter[2] = {0, 0};
 };
 RkBufs g_rk;
 
@@ -1020,6 +1091,10 @@ int rk_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int nstep) {
   const double anext[4] = {0.5, 0.5, 1.0, 0.0};
   field_select_kernel<<<1, 64, 0, st>>>(c.field_tab, b.counter, nstep, b.lf_cur);
   c.launches++;
+  if (b.reset_orb) {
+    cudaMemcpyAsync(y_orb, b.reset_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(y_cic, b.reset_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  }
   cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(b.y0 + no, y_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
   int rc = 0;
@@ -1108,7 +1183,11 @@ void hprod_init_(void) {
   Ctx& c = ctx();
   if (!c.have_rad || !c.have_sph || !c.have_bas) { c.status |= ST_CONFIG; return; }
   if (c.nfun > 16) { c.status |= ST_CONFIG; return; }
-  if (!c.st) cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking);
+  // one library stream for the process lifetime: callers may hold it
+  // (td1c_gpu_stream) beyond hprod_final_
+  static cudaStream_t lib_stream = nullptr;
+  if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
+  c.st = lib_stream;
   int rc = build_tables(c);
   rc |= build_pairs(c);
   rc |= build_state(c);
@@ -1170,6 +1249,7 @@ void hprod_set_wfn0_(const double* wfn, const double* cic, const char* v2xfc_typ
   cudaMemcpyAsync(es, c.d_scalar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
   c.ene_fcore = 2.0 * es[0] + es[1];
+  cudaMemsetAsync(c.gorbg, 0, c.nfcore * c.ngrid * sizeof(cplx), st);  // scratch of the energy only
   // hprod_addfc_tmat: add v2jfc to the kinetic diagonal
   tdiag_kernel<<<(c.Nr * c.L1 + 255) / 256, 256, 0, st>>>(c.Nr, c.L1, c.nd, c.znuc, c.xrad, c.radk, c.radk0, c.v2jfc, c.tdiag);
   cudaStreamSynchronize(st);
@@ -1208,7 +1288,6 @@ void hprod_final_(void) {
   for (void* p : g_allocs) cudaFree(p);
   g_allocs.clear();
   g_rk = RkBufs();
-  if (c.st) cudaStreamDestroy(c.st);
   delete g;
   g = nullptr;
 }
@@ -1258,7 +1337,7 @@ int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doub
   RkBufs& b = g_rk;
   if (b.cap < no + nc) {
     b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc);
-    if (!b.lf_cur) { b.lf_cur = dalloc<double>(36); b.counter = dalloc<int>(1); }
+    if (!b.lf_cur) { b.lf_cur = dalloc<double>(36); b.counter = dalloc<int>(2); }
     b.cap = no + nc;
   }
   // stage fields of every step (clcrk.cpp:62-73: t + dt * c_s)
@@ -1270,23 +1349,27 @@ int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doub
   for (int s = 0; s < nstep; ++s)
     for (int is = 0; is < 4; ++is) pulse_lfield(p, t0 + dt * s + dt * nodes[is], &tab[(size_t)s * 36 + 9 * is]);
   if (c.field_cap < nstep) {
-    c.field_tab = dalloc<double>((size_t)nstep * 36);
-    c.field_cap = nstep;
+    const int cap = std::max(nstep, 65536);  // keep the table address stable across calls
+    c.field_tab = dalloc<double>((size_t)cap * 36);
+    c.field_cap = cap;
   }
   cudaMemcpyAsync(c.field_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(b.counter, 0, sizeof(int), st);
+  b.h_counter[0] = 0; b.h_counter[1] = nstep;
+  cudaMemcpyAsync(b.counter, b.h_counter, 2 * sizeof(int), cudaMemcpyHostToDevice, st);
   c.launches = 0;
   cplx* y = (cplx*)d_wfn;
   cplx* yc = (cplx*)d_cic;
   int rc = 0;
-  int s0 = 0;
   if (!use_graph) {
     for (int s = 0; s < nstep; ++s) rc |= rk_step(c, y, yc, dt, nstep);
   } else {
-    // first step eagerly (sets kernel attributes), then one captured step replayed
-    rc |= rk_step(c, y, yc, dt, nstep);
-    s0 = 1;
-    if (nstep > 1) {
+    int s0 = 0;
+    const bool cached = c.graph_exec[0] && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt &&
+                        b.g_ro == b.reset_orb;
+    if (!cached) {
+      // one eager step (kernel attributes, first-call set-up), then capture one step
+      rc |= rk_step(c, y, yc, dt, nstep);
+      s0 = 1;
       if (c.graph_exec[0]) { cudaGraphExecDestroy(c.graph_exec[0]); c.graph_exec[0] = nullptr; }
       long l0 = c.launches;
       cudaGraph_t graph;
@@ -1295,12 +1378,13 @@ int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doub
       if (cudaStreamEndCapture(st, &graph) != cudaSuccess) return ST_CUDA;
       if (cudaGraphInstantiate(&c.graph_exec[0], graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
       cudaGraphDestroy(graph);
-      long per = c.launches - l0;
+      b.g_per = c.launches - l0;
       c.launches = l0;
-      for (int s = s0; s < nstep; ++s) {
-        if (cudaGraphLaunch(c.graph_exec[0], st) != cudaSuccess) return ST_CUDA;
-        c.launches += per;
-      }
+      b.g_y = y; b.g_yc = yc; b.g_tab = c.field_tab; b.g_dt = dt; b.g_ro = b.reset_orb;
+    }
+    for (int s = s0; s < nstep; ++s) {
+      if (cudaGraphLaunch(c.graph_exec[0], st) != cudaSuccess) return ST_CUDA;
+      c.launches += b.g_per;
     }
   }
   rc |= (int)cudaGetLastError();
@@ -1308,6 +1392,47 @@ int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doub
 }
 
 long td1c_gpu_launch_count(void) { return g ? g->launches : 0; }
+
+int td1c_gpu_rk4_reset(const void* d_wfn0, const void* d_cic0) {
+  g_rk.reset_orb = (const cplx*)d_wfn0;
+  g_rk.reset_cic = (const cplx*)d_cic0;
+  return 0;
+}
+
+void* td1c_gpu_stream(void) { return g ? (void*)g->st : nullptr; }
+
+int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d_wfn, const void* d_cic, void* d_hwfn,
+                     void* d_hcic, double* ms, char* names, int names_cap) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  for (int i = 0; i < 16; ++i) if (!c.ev[i]) cudaEventCreate(&c.ev[i]);
+  cudaMemcpyAsync(c.lfield, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, c.st);
+  std::vector<double> acc(kNumPhases, 0.0);
+  c.profile = true;
+  int rc = 0;
+  for (int r = 0; r < reps; ++r) {
+    rc |= run_htot(c, c.lfield, (const cplx*)d_wfn, (const cplx*)d_cic, (cplx*)d_hwfn, (cplx*)d_hcic, dtime);
+    cudaStreamSynchronize(c.st);
+    for (int k = 0; k + 1 < c.nev && k < kNumPhases; ++k) {
+      float t = 0;
+      cudaError_t e = cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]);
+      if (e != cudaSuccess) {
+        fprintf(stderr, "td1c_b200: phase timing %d failed: %s (nev %d)\n", k, cudaGetErrorString(e), c.nev);
+        rc |= ST_CUDA;
+      }
+      acc[k] += t;
+    }
+  }
+  c.profile = false;
+  for (int k = 0; k < kNumPhases; ++k) ms[k] = acc[k] / std::max(reps, 1);
+  if (names) {
+    std::string all;
+    for (int k = 0; k < kNumPhases; ++k) { all += kPhaseNames[k]; all += (k + 1 < kNumPhases) ? "," : ""; }
+    strncpy(names, all.c_str(), names_cap - 1);
+    names[names_cap - 1] = 0;
+  }
+  return rc ? -ST_CUDA : kNumPhases;
+}
 
 int td1c_gpu_sync(void) {
   Ctx& c = ctx();

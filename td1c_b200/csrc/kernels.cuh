@@ -59,18 +59,19 @@ struct PoissonArgs {
 int launch_poisson(const PoissonArgs& a, size_t smem_bytes, cudaStream_t st);
 
 // ---- mean-field action on the (r, theta) grid (hprod_mfprod2.F90)
-struct Act2Entry {    // one m-allowed (ij, kl) term of the 2-RDM contraction
-  int ij, pair, conj, d2idx;
-  double cre, cim;    // den2(j,i,l,k), filled on the device each RHS
+struct Act2Block {     // one dense (ij) x (kl) block of the 2-RDM contraction
+  int row0, nrow;      // rows: (ia, ja) entries rows[row0 .. row0+nrow)
+  int col0, ncol;      // cols: (pair, conj) entries cols[col0 .. col0+ncol)
+  int coff, pad0, pad1, pad2;  // coefficient offset, coef[coff + kl * nrow + ij]
 };
+struct Act2Coef { int d2idx, dst; };  // den2 element -> coefficient slot
 struct MfprodArgs {
-  int ngrid, nfun, npair;
+  size_t ngrid;
+  int nfun, npair;
   const cplx* W;        // [npair][ngrid]
   const cplx* orbg;     // [nfun][ngrid]
-  cplx* gorbg;          // [nfun][ngrid]
-  cplx* v2orbg;         // [nfun][ngrid]
-  Act2Entry* act2_list; int nact2;  // host-built m-allowed list, ordered by ij
-  // active-core terms (actj, actx) into v2orbg -- coefficients depend on den1 (device)
+  cplx* gorbg;          // [nfun][ngrid] (fully written for dynamic orbitals)
+  cplx* v2orbg;         // [nfun][ngrid] (fully written for dynamic orbitals)
   int nact, ncore, nfcore;
   const cplx* den1;     // [nact][nact] (Fortran order)
   const cplx* den2;     // [nact^4]
@@ -79,6 +80,13 @@ struct MfprodArgs {
   const int* pair_of;   // [nfun][nfun]: stored pair index of (a, b) or of (b, a)
   const int* pair_cj;   // [nfun][nfun]: 1 when (a, b) is read as conj of stored (b, a)
   int nelact;           // total active electrons
+  // act2 blocks (host-built), coefficients filled on the device each RHS
+  int nblk, nrow, ncol, ncoef;
+  const Act2Block* blk;
+  const int2* rows;
+  const int2* cols;
+  const Act2Coef* coef_map;
+  cplx* coef;
 };
 int launch_mfprod(const MfprodArgs& a, cudaStream_t st);
 

@@ -93,60 +93,93 @@ int launch_orbdots(const OrbdotsArgs& a, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// int2e block GEMM
+// int2e block GEMM: C(ij, kl) = sum_x A_ij[x] B_kl[x] over x in [0, K)
+// CTA = (K split, block); 192 threads = 2 K slices x (8 row groups x 12
+// column groups), each thread a 3 x 3 complex register tile; K chunks of 32
+// staged in shared memory with a one-chunk register prefetch.
 // ---------------------------------------------------------------------------
-constexpr int I2_KC = 16;
+constexpr int I2_KC = 32, I2_R = 24, I2_C = 36, I2_NT = 192;
 
-__global__ void __launch_bounds__(256) int2e_block_kernel(Int2eArgs a) {
-  __shared__ cplx sA[32][I2_KC + 1];
-  __shared__ cplx sB[96][I2_KC + 1];
+__global__ void __launch_bounds__(I2_NT) int2e_block_kernel(Int2eArgs a) {
+  __shared__ cplx sA[I2_R][I2_KC + 1];
+  __shared__ cplx sB[I2_C][I2_KC + 1];
+  cplx (*sred)[9] = reinterpret_cast<cplx (*)[9]>(&sB[0][0]);  // reuses sB after the K loop
   const Int2eBlock blk = a.blocks[blockIdx.y];
   const int nr = blk.nrow, nc = blk.ncol;
-  const int ncg = (nc + 2) / 3;             // column groups of 3
   const int t = threadIdx.x;
-  const int r = t / ncg, cg = t % ncg;
-  const bool active = r < nr;
+  const int slice = t / 96, tt = t % 96;
+  const int rg = tt / 12, cg = tt % 12;
   const size_t K = a.K;
-  const size_t kper = (K + gridDim.x - 1) / gridDim.x;
+  const size_t kper = ((K + gridDim.x - 1) / gridDim.x + I2_KC - 1) / I2_KC * I2_KC;
   const size_t k0 = (size_t)blockIdx.x * kper, k1 = min(K, k0 + kper);
-  cplx acc[3] = {mkc(0, 0), mkc(0, 0), mkc(0, 0)};
-  for (size_t kc = k0; kc < k1; kc += I2_KC) {
-    const int kn = (int)min((size_t)I2_KC, k1 - kc);
-    for (int e = t; e < nr * I2_KC; e += blockDim.x) {
+  cplx acc[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc[i][j] = mkc(0, 0);
+  // each thread stages up to 4 A and 6 B elements per chunk
+  constexpr int NA = (I2_R * I2_KC + I2_NT - 1) / I2_NT, NB = (I2_C * I2_KC + I2_NT - 1) / I2_NT;
+  cplx ra[NA], rb[NB];
+  auto load = [&](size_t kc) {
+#pragma unroll
+    for (int u = 0; u < NA; ++u) {
+      int e = t + u * I2_NT;
       int rr = e / I2_KC, kk = e % I2_KC;
       cplx v = mkc(0, 0);
-      if (kk < kn) v = __ldg(a.rho2 + (size_t)a.row_pair[blk.row0 + rr] * K + kc + kk);
-      sA[rr][kk] = v;
+      if (rr < nr && kc + kk < k1) v = __ldg(a.rho2 + (size_t)a.row_pair[blk.row0 + rr] * K + kc + kk);
+      ra[u] = v;
     }
-    for (int e = t; e < nc * I2_KC; e += blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      int e = t + u * I2_NT;
       int cc = e / I2_KC, kk = e % I2_KC;
       cplx v = mkc(0, 0);
-      if (kk < kn) {
+      if (cc < nc && kc + kk < k1) {
         int2 pc = a.col_pair[blk.col0 + cc];
         v = __ldg(a.v2sph + (size_t)pc.x * K + kc + kk);
         if (pc.y) v = cconj(v);
       }
-      sB[cc][kk] = v;
+      rb[u] = v;
     }
-    __syncthreads();
-    if (active) {
-#pragma unroll 4
-      for (int kk = 0; kk < kn; ++kk) {
-        cplx av = sA[r][kk];
+  };
+  if (k0 < k1) load(k0);
+  for (size_t kc = k0; kc < k1; kc += I2_KC) {
 #pragma unroll
-        for (int u = 0; u < 3; ++u) {
-          int c = cg * 3 + u;
-          if (c < nc) cfma(acc[u], av, sB[c][kk]);
-        }
-      }
+    for (int u = 0; u < NA; ++u) { int e = t + u * I2_NT; if (e < I2_R * I2_KC) sA[e / I2_KC][e % I2_KC] = ra[u]; }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) { int e = t + u * I2_NT; if (e < I2_C * I2_KC) sB[e / I2_KC][e % I2_KC] = rb[u]; }
+    __syncthreads();
+    if (kc + I2_KC < k1) load(kc + I2_KC);
+#pragma unroll 4
+    for (int kk = slice; kk < I2_KC; kk += 2) {
+      cplx av[3], bv[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) av[i] = sA[rg * 3 + i][kk];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) bv[j] = sB[cg * 3 + j][kk];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) cfma(acc[i][j], av[i], bv[j]);
     }
     __syncthreads();
   }
-  if (active) {
-    for (int u = 0; u < 3; ++u) {
-      int c = cg * 3 + u;
-      if (c < nc) a.partial[((size_t)blockIdx.x * a.nblkent) + blk.ent0 + r * nc + c] = acc[u];
-    }
+  if (slice == 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) sred[tt][i * 3 + j] = acc[i][j];
+  }
+  __syncthreads();
+  if (slice == 0) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        int r = rg * 3 + i, c = cg * 3 + j;
+        if (r < nr && c < nc)
+          a.partial[((size_t)blockIdx.x * a.nblkent) + blk.ent0 + r * nc + c] = cadd(acc[i][j], sred[tt][i * 3 + j]);
+      }
   }
 }
 
@@ -171,11 +204,19 @@ __global__ void int2e_fill_kernel(Int2eArgs a) {
 int launch_int2e(const Int2eArgs& a, int nsplit, cudaStream_t st) {
   const int n = a.nact, n4 = n * n * n * n;
   if (n4 == 0) return 0;
-  cudaMemsetAsync(a.int2e, 0, sizeof(cplx) * n4, st);
+  cudaError_t e = cudaMemsetAsync(a.int2e, 0, sizeof(cplx) * n4, st);
+  if (e != cudaSuccess) { fprintf(stderr, "td1c_b200: int2e memset: %s\n", cudaGetErrorString(e)); return (int)e; }
   if (a.nblocks > 0) {
     dim3 grid(nsplit, a.nblocks);
-    int2e_block_kernel<<<grid, 256, 0, st>>>(a);
+    int2e_block_kernel<<<grid, I2_NT, 0, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      fprintf(stderr, "td1c_b200: int2e block kernel (grid %d x %d): %s\n", nsplit, a.nblocks, cudaGetErrorString(e));
+      return (int)e;
+    }
     int2e_sum_kernel<<<(a.nblkent + 127) / 128, 128, 0, st>>>(a, nsplit);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { fprintf(stderr, "td1c_b200: int2e sum: %s\n", cudaGetErrorString(e)); return (int)e; }
   }
   int2e_fill_kernel<<<(n4 + 127) / 128, 128, 0, st>>>(a);
   return (int)cudaGetLastError();

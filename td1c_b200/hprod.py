@@ -140,6 +140,23 @@ class HProd:
                                           int(nstep), float(wl["fint"]), float(wl["wlen"]), float(wl["numcyc"]),
                                           float(wl.get("cep", 0.0)), 1 if use_graph else 0))
 
+    def rk4_reset(self, d_wfn0, d_cic0):
+        self._check(self.lib.td1c_gpu_rk4_reset(ctypes.c_void_p(d_wfn0) if d_wfn0 else None,
+                                                ctypes.c_void_p(d_cic0) if d_cic0 else None))
+
+    def stream(self):
+        return int(self.lib.td1c_gpu_stream() or 0)
+
+    def profile(self, reps, lfield, d_wfn, d_cic, d_hwfn, d_hcic, dtime=1.0):
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        ms = np.zeros(16)
+        names = ctypes.create_string_buffer(512)
+        n = self.lib.td1c_gpu_profile(int(reps), float(dtime), _dp(lf), ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic),
+                                      ctypes.c_void_p(d_hwfn), ctypes.c_void_p(d_hcic), _dp(ms), names, 512)
+        if n <= 0 or n > 16:
+            raise StatusError("td1c_gpu_profile failed (%d)" % n)
+        return dict(zip(names.value.decode().split(","), ms[:n].tolist()))
+
     def sync(self):
         self._check(self.lib.td1c_gpu_sync())
         self._status()

@@ -56,6 +56,8 @@ def ci_blocks(wl, stra, strb):
 def rel_err(a, b):
     a = np.asarray(a).ravel()
     b = np.asarray(b).ravel()
+    if b.size == 0:
+        return 0.0
     den = np.abs(b).max()
     if den == 0:
         return float(np.abs(a).max())
