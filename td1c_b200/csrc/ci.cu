@@ -162,6 +162,8 @@ __global__ void ci_tvec_kernel(CiArgs a) {
 // sigma_J = sum_rs k_rs D_rs[J] + 1/2 sum_rs (E_rs T_rs)[J]; then
 // hcic = fac (sigma - E_act c)
 __global__ void __launch_bounds__(128) ci_sigma_kernel(CiArgs a) {
+  // one warp per determinant J, lanes over the (r, s) pairs, fixed-order
+  // shuffle reduction
   const CiTables& t = a.t;
   const int n = t.nact;
   __shared__ cplx sk[16 * 16];
@@ -172,31 +174,34 @@ __global__ void __launch_bounds__(128) ci_sigma_kernel(CiArgs a) {
     sk[e] = k;
   }
   __syncthreads();
-  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int J = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (J >= t.lcic) return;
   const int ja = t.det_a[J], jb = t.det_b[J];
+  const unsigned sa = t.stra[ja], sbs = t.strb[jb];
   cplx sig = mkc(0, 0);
-  for (int s = 0; s < n; ++s)
-    for (int r = 0; r < n; ++r) {
-      const int rs = r + n * s;
-      const long o = t.dvec_off[rs];
-      if (t.orb_m[r] == t.orb_m[s]) cfma(sig, sk[rs], cadd(a.Da[o + J], a.Db[o + J]));
-      const int sec = t.mtot + t.orb_m[s] - t.orb_m[r] - t.smin;
-      if (sec < 0 || sec >= t.nsec) continue;
-      const long ot = t.dvec_off[s + n * r];
-      int sg;
-      // K = E_sr J (alpha)
-      unsigned ka = excite_str(t.stra[ja], s, r, sg);
-      if (ka != ~0u) {
-        int K = det_in_sector(t, sec, t.idx_a[ka], jb);
-        if (K >= 0) { cplx v = cscale(a.T[ot + K], 0.5 * sg); sig = cadd(sig, v); }
-      }
-      unsigned kb = excite_str(t.strb[jb], s, r, sg);
-      if (kb != ~0u) {
-        int K = det_in_sector(t, sec, ja, t.idx_b[kb]);
-        if (K >= 0) { cplx v = cscale(a.T[ot + K], 0.5 * sg); sig = cadd(sig, v); }
-      }
+  for (int rs = lane; rs < n * n; rs += 32) {
+    const int r = rs % n, s = rs / n;
+    const long o = t.dvec_off[rs];
+    if (t.orb_m[r] == t.orb_m[s]) cfma(sig, sk[rs], cadd(a.Da[o + J], a.Db[o + J]));
+    const int sec = t.mtot + t.orb_m[s] - t.orb_m[r] - t.smin;
+    if (sec < 0 || sec >= t.nsec) continue;
+    const long ot = t.dvec_off[s + n * r];
+    int sg;
+    // K = E_sr J (alpha), then beta
+    unsigned ka = excite_str(sa, s, r, sg);
+    if (ka != ~0u) {
+      int K = det_in_sector(t, sec, t.idx_a[ka], jb);
+      if (K >= 0) sig = cadd(sig, cscale(a.T[ot + K], 0.5 * sg));
     }
+    unsigned kb = excite_str(sbs, s, r, sg);
+    if (kb != ~0u) {
+      int K = det_in_sector(t, sec, ja, t.idx_b[kb]);
+      if (K >= 0) sig = cadd(sig, cscale(a.T[ot + K], 0.5 * sg));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) { sig.x += __shfl_xor_sync(0xffffffff, sig.x, o); sig.y += __shfl_xor_sync(0xffffffff, sig.y, o); }
+  if (lane != 0) return;
   const double e = *a.ene_act;
   cplx c = a.cic[J];
   sig = csub(sig, cscale(c, e));
@@ -224,7 +229,7 @@ int launch_ci_sigma(const CiArgs& a, int maxsec, cudaStream_t st) {
   const int n = a.t.nact;
   dim3 grid((maxsec + 127) / 128, n * n);
   ci_tvec_kernel<<<grid, 128, 0, st>>>(a);
-  ci_sigma_kernel<<<(a.t.lcic + 127) / 128, 128, 0, st>>>(a);
+  ci_sigma_kernel<<<(a.t.lcic + 3) / 4, 128, 0, st>>>(a);
   return (int)cudaGetLastError();
 }
 

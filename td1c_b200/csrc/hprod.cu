@@ -275,46 +275,81 @@ __global__ void fc_phase_kernel(int Nr, int nlat, int nfcore, const double* __re
   orbg[t] = cmul(orbg0[t], mkc(c, -s));
 }
 
-// Hermitian regularised inverse U diag(d/(d^2+thr)) U^H by a one-warp cyclic
-// complex Jacobi (hprod_invden.F90:62-107; zheev replaced).  Matrix n <= 16.
+// Hermitian regularised inverse U diag(d/(d^2+thr)) U^H (hprod_invden.F90:62-107;
+// zheev replaced by a complex Jacobi).  One warp; the rotations of a sweep are
+// grouped into rounds of disjoint (p,q) pairs (round-robin ordering), so each
+// round applies all its rotations at once: columns (A U, V U) then rows
+// (U^H A).  n <= 16.
 __device__ void herm_reg_inverse_warp(int n, double thr, const cplx* a, cplx* inv, cplx* A, cplx* V, int* status) {
   const int lane = threadIdx.x & 31;
+  __shared__ double rc[2][8], rs[2][8];
+  __shared__ cplx re[2][8];
+  __shared__ int rp[2][8], rq[2][8];
+  const int wsel = (threadIdx.x >> 5) & 1;
   for (int e = lane; e < n * n; e += 32) { A[e] = a[e]; V[e] = mkc((e % n) == (e / n) ? 1.0 : 0.0, 0.0); }
   __syncwarp();
-  bool conv = false;
+  const int N = (n + 1) & ~1;  // players of the round-robin schedule (one dummy if n is odd)
+  bool conv = (n <= 1);
   for (int sweep = 0; sweep < 60 && !conv; ++sweep) {
     double off = 0, dg = 0;
     for (int e = lane; e < n * n; e += 32) { if ((e % n) != (e / n)) off += cabs2(A[e]); else dg += cabs2(A[e]); }
     for (int o = 16; o > 0; o >>= 1) { off += __shfl_xor_sync(0xffffffff, off, o); dg += __shfl_xor_sync(0xffffffff, dg, o); }
     if (off <= 1e-32 * fmax(dg, 1e-300)) { conv = true; break; }
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        cplx apq = A[p + n * q];
-        double b = sqrt(cabs2(apq));
-        if (b < 1e-300) continue;
-        cplx e = cscale(apq, 1.0 / b);
-        double app = A[p + n * p].x, aqq = A[q + n * q].x;
-        double tau = (aqq - app) / (2 * b);
-        double tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
-        double c = 1 / sqrt(1 + tt * tt), s = tt * c;
-        cplx em = cconj(e);
-        __syncwarp();
-        for (int k = lane; k < n; k += 32) {
-          cplx akp = A[k + n * p], akq = A[k + n * q];
-          A[k + n * p] = csub(cscale(akp, c), cscale(cmul(em, akq), s));
-          A[k + n * q] = cadd(cscale(akp, s), cscale(cmul(em, akq), c));
-          cplx vkp = V[k + n * p], vkq = V[k + n * q];
-          V[k + n * p] = csub(cscale(vkp, c), cscale(cmul(em, vkq), s));
-          V[k + n * q] = cadd(cscale(vkp, s), cscale(cmul(em, vkq), c));
+    for (int rnd = 0; rnd < N - 1; ++rnd) {
+      // rotation parameters of this round's disjoint pairs
+      if (lane < N / 2) {
+        const int i = lane;
+        auto player = [&](int pos) { return pos == 0 ? 0 : ((pos - 1 + rnd) % (N - 1)) + 1; };
+        int p = player(i), q = player(N - 1 - i);
+        if (p > q) { int tt = p; p = q; q = tt; }
+        double c = 1.0, sn = 0.0;
+        cplx e = mkc(1.0, 0.0);
+        bool valid = q < n;
+        if (valid) {
+          cplx apq = A[p + n * q];
+          double b = sqrt(cabs2(apq));
+          if (b < 1e-300) valid = false;
+          else {
+            e = cscale(apq, 1.0 / b);
+            double app = A[p + n * p].x, aqq = A[q + n * q].x;
+            double tau = (aqq - app) / (2 * b);
+            double tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+            c = 1 / sqrt(1 + tt * tt); sn = tt * c;
+          }
         }
-        __syncwarp();
-        for (int k = lane; k < n; k += 32) {
-          cplx apk = A[p + n * k], aqk = A[q + n * k];
-          A[p + n * k] = csub(cscale(apk, c), cscale(cmul(e, aqk), s));
-          A[q + n * k] = cadd(cscale(apk, s), cscale(cmul(e, aqk), c));
-        }
-        __syncwarp();
+        rp[wsel][i] = valid ? p : -1; rq[wsel][i] = q; rc[wsel][i] = c; rs[wsel][i] = sn; re[wsel][i] = e;
       }
+      __syncwarp();
+      // columns: A <- A U, V <- V U
+      for (int w = lane; w < (N / 2) * n; w += 32) {
+        const int i = w / n, k = w % n;
+        const int p = rp[wsel][i];
+        if (p < 0) continue;
+        const int q = rq[wsel][i];
+        const double c = rc[wsel][i], sn = rs[wsel][i];
+        const cplx em = cconj(re[wsel][i]);
+        cplx akp = A[k + n * p], akq = A[k + n * q];
+        A[k + n * p] = csub(cscale(akp, c), cscale(cmul(em, akq), sn));
+        A[k + n * q] = cadd(cscale(akp, sn), cscale(cmul(em, akq), c));
+        cplx vkp = V[k + n * p], vkq = V[k + n * q];
+        V[k + n * p] = csub(cscale(vkp, c), cscale(cmul(em, vkq), sn));
+        V[k + n * q] = cadd(cscale(vkp, sn), cscale(cmul(em, vkq), c));
+      }
+      __syncwarp();
+      // rows: A <- U^H A
+      for (int w = lane; w < (N / 2) * n; w += 32) {
+        const int i = w / n, k = w % n;
+        const int p = rp[wsel][i];
+        if (p < 0) continue;
+        const int q = rq[wsel][i];
+        const double c = rc[wsel][i], sn = rs[wsel][i];
+        const cplx e = re[wsel][i];
+        cplx apk = A[p + n * k], aqk = A[q + n * k];
+        A[p + n * k] = csub(cscale(apk, c), cscale(cmul(e, aqk), sn));
+        A[q + n * k] = cadd(cscale(apk, sn), cscale(cmul(e, aqk), c));
+      }
+      __syncwarp();
+    }
   }
   if (!conv && lane == 0) atomicOr(status, ST_JACOBI);
   __syncwarp();

@@ -11,9 +11,9 @@
 // smem, the derivative is kept in smem, and the l <-> l+-1 laser coupling is
 // formed from smem -- orbitals are read from HBM once and h0/h1 written once.
 // The band coefficients come from the (2nd+1) x nrad radk/radk0/radp tables
-// (L2-resident) plus a per-(l, r) diagonal, instead of the reference's
-// (2nd+1) x Nr x L1 tmat (19 MB for Ne).  Summation runs over r' in
-// ascending order like zdotu.
+// (the tile's rows staged in smem) plus a per-(l, r) diagonal, instead of the
+// reference's (2nd+1) x Nr x L1 tmat (19 MB for Ne).  Summation runs over r'
+// in ascending order like zdotu.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -27,8 +27,20 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
   const int W = OB_TILE + 2 * nd;
   cplx* so = reinterpret_cast<cplx*>(smem_d);  // [L1][W]
   cplx* sdw = so + (size_t)L1 * W;             // [L1][OB_TILE]
+  double* sb = reinterpret_cast<double*>(sdw + (size_t)L1 * OB_TILE);  // [3][bw][OB_TILE] radk, radk0, radp rows
   const int f = blockIdx.y;
   const int r0 = blockIdx.x * OB_TILE;
+  for (int e = threadIdx.x; e < OB_TILE * bw; e += blockDim.x) {
+    const int q = e / bw, jb = e % bw;
+    const int ir = r0 + q + 1;
+    double k0 = 0.0, k1 = 0.0, pp = 0.0;
+    if (ir <= Nr) {
+      const size_t o = (size_t)bw * ir + jb;
+      k0 = a.radk[o]; k1 = a.radk0[o]; pp = a.radp[o];
+    }
+    const int d = jb * OB_TILE + q;  // band index major: lanes (q) hit consecutive banks
+    sb[d] = k0; sb[OB_TILE * bw + d] = k1; sb[2 * OB_TILE * bw + d] = pp;
+  }
   const int m = a.mval[f];
   const int am = m < 0 ? -m : m;
   const cplx* __restrict__ orb = a.orb + (size_t)f * L1 * Nr;
@@ -54,16 +66,16 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
     const int jll = max(1, ir - nd), jul = min(Nr, ir + nd);
     cplx hs = mkc(0.0, 0.0), ds = mkc(0.0, 0.0);
     if (l >= am) {
-      const double* __restrict__ rk = (l == 0 ? a.radk : a.radk0) + (size_t)bw * ir;
-      const double* __restrict__ rp = a.radp + (size_t)bw * ir;
+      const double* rk = sb + (l == 0 ? 0 : OB_TILE * bw) + q;
+      const double* rp = sb + 2 * OB_TILE * bw + q;
       const double td = a.tdiag[(size_t)l * Nr + r];
       const cplx* srow = so + (size_t)l * W + (nd + q);  // srow[k] = orb(r + k)
       for (int jr = jll; jr <= jul; ++jr) {
         int jb = nd + jr - ir;
         cplx w = srow[jr - ir];
-        double t = (jr == ir) ? td : __ldg(rk + jb);
+        double t = (jr == ir) ? td : rk[jb * OB_TILE];
         hs.x = fma(w.x, t, hs.x); hs.y = fma(w.y, t, hs.y);
-        if (vel) { double p = __ldg(rp + jb); ds.x = fma(w.x, p, ds.x); ds.y = fma(w.y, p, ds.y); }
+        if (vel) { double p = rp[jb * OB_TILE]; ds.x = fma(w.x, p, ds.x); ds.y = fma(w.y, p, ds.y); }
       }
     }
     h0[(size_t)l * Nr + r] = hs;
@@ -119,7 +131,7 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
 
 int launch_onebody(const OneBodyArgs& a, cudaStream_t st) {
   const int W = OB_TILE + 2 * a.nd;
-  size_t smem = sizeof(cplx) * ((size_t)a.L1 * W + (size_t)a.L1 * OB_TILE);
+  size_t smem = sizeof(cplx) * ((size_t)a.L1 * W + (size_t)a.L1 * OB_TILE) + sizeof(double) * 3 * OB_TILE * (2 * a.nd + 1);
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(onebody_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

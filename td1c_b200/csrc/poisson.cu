@@ -7,15 +7,18 @@
 // solves  L_l L_l^T x = rhs  with the dpbtrf factor of
 // [l(l+1)/r^2 + 2 T] (band nd) by dpbtrs, and returns
 //     v2sph = (x + t r^(l+1) sqrt(w_r)) 4 pi / ((2l+1) r sqrt(w_r)).
-// One CTA owns one l.  Shared memory holds that l's band factor with the
-// diagonal replaced by its reciprocal (Nr x (nd+1) doubles, 201 KB for Ne)
-// plus the r^l/(2 pi) and (2l+1)/(2 pi r sqrt w) columns; every thread runs
-// the forward and back substitution of one (pair, re|im) right-hand side.
-// The substitution is sequential in r, so the kernel is latency-bound: the
-// last nd solution values live in registers (nd is a template parameter),
-// the terms are summed oldest-first as dtbsv does so only the newest value
-// sits on the critical path, and each block of nd inputs is loaded one block
-// ahead (register double buffer) so no global access waits inside the chain.
+// One CTA owns one l; every thread runs the forward and back substitution of
+// one (pair, re|im) right-hand side.  The substitution is sequential in r and
+// the SM holds only a few warps, so the loop is written to be branch-free:
+// shared memory holds the l's band factor (diagonal replaced by its
+// reciprocal) framed by nd zero rows on each side and identity rows that
+// round Nr up to a multiple of nd, so no step needs a bounds test; the last
+// nd solution values live in registers (nd is a template parameter); the
+// band terms of older values are summed (oldest first, as dtbsv) into four
+// independent partial sums so only the newest value's FMA and the
+// reciprocal multiply sit on the recurrence; inputs and the final scaling
+// columns are loaded one block of nd rows ahead.  The homogeneous boundary
+// term and the final scaling are fused into the back substitution.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -26,20 +29,29 @@ __global__ void __launch_bounds__(128) poisson_kernel(PoissonArgs a) {
   extern __shared__ double sm[];
   const int l = blockIdx.x;
   const int Nr = a.Nr;
-  double* sL = sm;                          // [Nr][ND+1], sL[(ND+1) j] = 1 / L(j,j)
-  double* s0 = sm + (size_t)Nr * (ND + 1);  // [Nr] r^l / (2 pi)
-  double* sI = s0 + Nr;                     // [Nr] (2l+1) / (2 pi r sqrt w)
-  const double* __restrict__ gL = a.d2ll + (size_t)l * Nr * (ND + 1);
-  for (int e = threadIdx.x; e < Nr * (ND + 1); e += blockDim.x) sL[e] = gL[e];
-  __syncthreads();
-  for (int j = threadIdx.x; j < Nr; j += blockDim.x) {
-    sL[(size_t)(ND + 1) * j] = a.d2rinv[(size_t)l * Nr + j];
-    s0[j] = a.rpl0[(size_t)l * Nr + j];
-    sI[j] = a.invr[(size_t)l * Nr + j];
+  const int nb = (Nr + ND - 1) / ND;
+  const int Np = nb * ND;                          // padded rows
+  constexpr int LD = ND + 1;
+  double* sL = sm + (size_t)ND * LD;               // row j at sL + LD j, rows -ND .. Np+ND-1
+  double* s0 = sm + (size_t)(Np + 2 * ND) * LD;    // [Np] r^l / (2 pi)
+  double* sI = s0 + Np;                            // [Np] (2l+1) / (2 pi r sqrt w)
+  const double* __restrict__ gL = a.d2ll + (size_t)l * Nr * LD;
+  for (int e = threadIdx.x; e < (Np + 2 * ND) * LD; e += blockDim.x) {
+    const int row = e / LD - ND, k = e % LD;
+    double v = 0.0;
+    if (row >= 0 && row < Nr) v = (k == 0) ? a.d2rinv[(size_t)l * Nr + row] : gL[(size_t)row * LD + k];
+    else if (row >= Nr && row < Np && k == 0) v = 1.0;  // identity padding rows
+    sm[e] = v;
+  }
+  for (int j = threadIdx.x; j < Np; j += blockDim.x) {
+    s0[j] = j < Nr ? a.rpl0[(size_t)l * Nr + j] : 0.0;
+    sI[j] = j < Nr ? a.invr[(size_t)l * Nr + j] : 0.0;
   }
   __syncthreads();
   const int nsys = 2 * a.npair;
-  const int nb = (Nr + ND - 1) / ND;
+  const double fac1 = a.fac1[l];
+  const double* __restrict__ rpl1 = a.rpl1 + (size_t)l * Nr;
+  const double* __restrict__ fac2 = a.fac2 + (size_t)l * Nr;
   for (int s = threadIdx.x + blockIdx.y * blockDim.x; s < nsys; s += blockDim.x * gridDim.y) {
     const int p = s >> 1, c = s & 1;
     const int m = a.pair_m[p];
@@ -53,73 +65,80 @@ __global__ void __launch_bounds__(128) poisson_kernel(PoissonArgs a) {
     double t = 0.0;
     double win[ND], cur[ND], nxt[ND];
 #pragma unroll
-    for (int k = 0; k < ND; ++k) { win[k] = 0.0; cur[k] = (k < Nr) ? __ldg(in + 2 * k) : 0.0; }
-    // forward substitution  L y = rhs  (y stored into out)
+    for (int k = 0; k < ND; ++k) { win[k] = 0.0; cur[k] = __ldg(in + 2 * min(k, Nr - 1)); }
+    // ---- forward substitution  L y = rhs  (y kept in out for the back pass)
     for (int b = 0; b < nb; ++b) {
       const int jb = b * ND;
 #pragma unroll
-      for (int u = 0; u < ND; ++u) { const int jn = jb + ND + u; nxt[u] = (jn < Nr) ? __ldg(in + 2 * jn) : 0.0; }
+      for (int u = 0; u < ND; ++u) nxt[u] = __ldg(in + 2 * min(jb + ND + u, Nr - 1));
 #pragma unroll
       for (int u = 0; u < ND; ++u) {
         const int j = jb + u;
-        if (j < Nr) {
-          const double rho = cur[u];
-          t = fma(rho, s0[j], t);
-          double sacc = rho * sI[j];
-          const double* Lr = sL + (size_t)(ND + 1) * j;
+        const double rho = cur[u];
+        t = fma(rho, s0[j], t);
+        const double* Lr = sL + (size_t)LD * j;
+        // L(j, j-k) = ab[k + LD (j-k)] = Lr[-ND k]; y_{j-k} in win[(u-k) mod ND]
+        double pa = rho * sI[j], pb = 0.0, pc = 0.0, pd = 0.0;
 #pragma unroll
-          for (int k = ND; k >= 1; --k) {  // oldest first, as dtbsv's column sweep
-            // L(j, j-k) = ab[k + (ND+1)(j-k)] = Lr[k - (ND+1) k] ; y_{j-k} in win[(u-k) mod ND]
-            if (j - k >= 0) sacc = fma(-Lr[k - (ND + 1) * k], win[(u - k + ND) % ND], sacc);
-          }
-          const double y = sacc * Lr[0];
-          win[u] = y;
-          out[2 * j] = y;
+        for (int k = ND; k >= 2; --k) {
+          const double term = Lr[-ND * k] * win[(u - k + ND) % ND];
+          const int g = (ND - k) & 3;
+          if (g == 0) pa -= term; else if (g == 1) pb -= term; else if (g == 2) pc -= term; else pd -= term;
         }
+        const double sacc = fma(-Lr[-ND], win[(u - 1 + ND) % ND], (pa + pb) + (pc + pd));
+        const double y = sacc * Lr[0];
+        win[u] = y;
+        if (j < Nr) out[2 * j] = y;
       }
 #pragma unroll
       for (int u = 0; u < ND; ++u) cur[u] = nxt[u];
     }
-    // back substitution  L^T x = y  (reads back the thread's own forward values)
+    // ---- back substitution  L^T x = y  fused with the boundary term and scaling
+    //      v2sph = (x + t fac1 r^(l+1) sqrt(w)) 4 pi / ((2l+1) r sqrt(w))
+    t *= fac1;
+    double c1[ND], c2[ND], n1[ND], n2[ND];
 #pragma unroll
     for (int k = 0; k < ND; ++k) win[k] = 0.0;
     {
       const int jb = (nb - 1) * ND;
 #pragma unroll
-      for (int u = 0; u < ND; ++u) cur[u] = (jb + u < Nr) ? out[2 * (jb + u)] : 0.0;
+      for (int u = 0; u < ND; ++u) {
+        const int jj = min(jb + u, Nr - 1);
+        cur[u] = (jb + u < Nr) ? out[2 * jj] : 0.0;
+        c1[u] = __ldg(rpl1 + jj); c2[u] = __ldg(fac2 + jj);
+      }
     }
     for (int b = nb - 1; b >= 0; --b) {
       const int jb = b * ND;
       if (b > 0) {
 #pragma unroll
-        for (int u = 0; u < ND; ++u) nxt[u] = out[2 * (jb - ND + u)];
+        for (int u = 0; u < ND; ++u) {
+          const int jj = jb - ND + u;
+          nxt[u] = out[2 * jj]; n1[u] = __ldg(rpl1 + jj); n2[u] = __ldg(fac2 + jj);
+        }
       }
 #pragma unroll
       for (int u = ND - 1; u >= 0; --u) {
         const int j = jb + u;
-        if (j < Nr) {
-          double sacc = cur[u];
-          const double* Lc = sL + (size_t)(ND + 1) * j;
+        const double* Lc = sL + (size_t)LD * j;
+        // L(j+k, j) = ab[k + LD j] = Lc[k]; x_{j+k} in win[(u+k) mod ND]; farthest first
+        double pa = cur[u], pb = 0.0, pc = 0.0, pd = 0.0;
 #pragma unroll
-          for (int k = ND; k >= 1; --k) {  // farthest first, as dtbsv('T')
-            // L(j+k, j) = ab[k + (ND+1) j] = Lc[k] ; x_{j+k} in win[(u+k) mod ND]
-            if (j + k < Nr) sacc = fma(-Lc[k], win[(u + k) % ND], sacc);
-          }
-          const double x = sacc * Lc[0];
-          win[u] = x;
-          out[2 * j] = x;
+        for (int k = ND; k >= 2; --k) {
+          const double term = Lc[k] * win[(u + k) % ND];
+          const int g = (ND - k) & 3;
+          if (g == 0) pa -= term; else if (g == 1) pb -= term; else if (g == 2) pc -= term; else pd -= term;
         }
+        const double sacc = fma(-Lc[1], win[(u + 1) % ND], (pa + pb) + (pc + pd));
+        const double x = sacc * Lc[0];
+        win[u] = x;
+        if (j < Nr) out[2 * j] = fma(t, c1[u], x) * c2[u];
       }
       if (b > 0) {
 #pragma unroll
-        for (int u = 0; u < ND; ++u) cur[u] = nxt[u];
+        for (int u = 0; u < ND; ++u) { cur[u] = nxt[u]; c1[u] = n1[u]; c2[u] = n2[u]; }
       }
     }
-    // homogeneous boundary term and scaling
-    t *= a.fac1[l];
-    const double* __restrict__ rpl1 = a.rpl1 + (size_t)l * Nr;
-    const double* __restrict__ fac2 = a.fac2 + (size_t)l * Nr;
-    for (int r = 0; r < Nr; ++r) out[2 * r] = fma(t, __ldg(rpl1 + r), out[2 * r]) * __ldg(fac2 + r);
   }
 }
 
@@ -130,7 +149,8 @@ static int launch_nd(const PoissonArgs& a, cudaStream_t st) {
     cudaFuncSetAttribute(poisson_kernel<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     attr = true;
   }
-  const size_t smem = sizeof(double) * ((size_t)a.Nr * (ND + 1) + 2 * (size_t)a.Nr);
+  const int Np = (a.Nr + ND - 1) / ND * ND;
+  const size_t smem = sizeof(double) * ((size_t)(Np + 2 * ND) * (ND + 1) + 2 * (size_t)Np);
   if (smem > 227 * 1024) return (int)cudaErrorInvalidValue;
   int nsys = 2 * a.npair;
   int ysplit = (nsys + 127) / 128;

@@ -51,22 +51,26 @@ __global__ void __launch_bounds__(256) orbdots_kernel(OrbdotsArgs a) {
   }
   __syncthreads();
   cplx* out = a.partial + (size_t)blockIdx.x * a.nent;
-  for (int t = threadIdx.x; t < a.nent; t += blockDim.x) {
+  // one warp per entry, lanes over the chunk (conflict-free), fixed-order
+  // shuffle reduction
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int t = wid; t < a.nent; t += nw) {
     const int4 en = a.ent[t];  // (kind, j, i, 0)
     const int kind = en.x, j = en.y, i = en.z;
-    cplx s = mkc(0, 0);
     const cplx* x; const cplx* y;
     if (kind == 0) { x = so + j * C; y = sf + i * C; }        // A
     else if (kind == 1) { x = so + j * C; y = sv + i * C; }   // B
     else if (kind == 2) { x = sh + j * C; y = so + i * C; }   // C
     else if (kind == 3) { x = so + i * C; y = sh + i * C; }   // E
     else { x = so + j * C; y = sgv + i * C; }                 // <phi_j|(g+v2) phi_i>
-    for (int k = 0; k < C; ++k) {
+    cplx s = mkc(0, 0);
+    for (int k = lane; k < C; k += 32) {
       cplx xv = x[k], yv = y[k];
       s.x = fma(xv.x, yv.x, fma(xv.y, yv.y, s.x));
       s.y = fma(xv.x, yv.y, fma(-xv.y, yv.x, s.y));
     }
-    out[t] = s;
+    for (int o = 16; o > 0; o >>= 1) { s.x += __shfl_xor_sync(0xffffffff, s.x, o); s.y += __shfl_xor_sync(0xffffffff, s.y, o); }
+    if (lane == 0) out[t] = s;
   }
 }
 
@@ -108,7 +112,11 @@ __global__ void __launch_bounds__(I2_NT) int2e_block_kernel(Int2eArgs a) {
   const int nr = blk.nrow, nc = blk.ncol;
   const int t = threadIdx.x;
   const int slice = t / 96, tt = t % 96;
-  const int rg = tt / 12, cg = tt % 12;
+  // compact 3 x 3 tiles over the block's actual shape: only ceil(nr/3) x
+  // ceil(nc/3) threads of a slice compute, so small blocks occupy few warps
+  const int ncg = (nc + 2) / 3, nrg = (nr + 2) / 3;
+  const bool act = tt < nrg * ncg;
+  const int rg = act ? tt / ncg : 0, cg = act ? tt % ncg : 0;
   const size_t K = a.K;
   const size_t kper = ((K + gridDim.x - 1) / gridDim.x + I2_KC - 1) / I2_KC * I2_KC;
   const size_t k0 = (size_t)blockIdx.x * kper, k1 = min(K, k0 + kper);
@@ -151,7 +159,7 @@ __global__ void __launch_bounds__(I2_NT) int2e_block_kernel(Int2eArgs a) {
     __syncthreads();
     if (kc + I2_KC < k1) load(kc + I2_KC);
 #pragma unroll 4
-    for (int kk = slice; kk < I2_KC; kk += 2) {
+    for (int kk = slice; act && kk < I2_KC; kk += 2) {
       cplx av[3], bv[3];
 #pragma unroll
       for (int i = 0; i < 3; ++i) av[i] = sA[rg * 3 + i][kk];
@@ -164,14 +172,14 @@ __global__ void __launch_bounds__(I2_NT) int2e_block_kernel(Int2eArgs a) {
     }
     __syncthreads();
   }
-  if (slice == 1) {
+  if (slice == 1 && act) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) sred[tt][i * 3 + j] = acc[i][j];
   }
   __syncthreads();
-  if (slice == 0) {
+  if (slice == 0 && act) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll

@@ -1,0 +1,165 @@
+"""Known-answer checks that pin the CPU oracle (no GPU needed).
+
+The reference ships no tests or golden outputs and cannot be built here, so
+the oracle is pinned by analytic properties of the restated algorithm:
+hydrogenic spectra of the FEDVR one-body table, Legendre-table
+orthonormality, the Poisson solve of a closed-form density, Hermiticity and
+conservation properties of the RHS, RDM traces, and LAPACK cross-checks.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+from oracle.oracle import Oracle
+from td1c_b200 import workloads as W
+
+from .helpers import oracle_state
+
+
+def band_to_dense(band, Nr, nd):
+    A = np.zeros((Nr, Nr))
+    for i in range(Nr):
+        for jb in range(2 * nd + 1):
+            j = i + jb - nd
+            if 0 <= j < Nr:
+                A[i, j] = band[i, jb]
+    return A
+
+
+@pytest.fixture(scope="module")
+def he():
+    return Oracle(W.HE_TDHF)
+
+
+def test_hydrogenic_spectrum(he):
+    """tmat (bas_gen_tmat.F90) at l = 0, 1 reproduces -Z^2 / 2 n^2 for Z = 2."""
+    d = he.dims
+    Nr, nd, L1 = d["nrad"] - 1, d["ndvr"], d["lmax1"] + 1
+    tm = he.get("tmat").reshape(L1, Nr, 2 * nd + 1)
+    for l in (0, 1):
+        A = band_to_dense(tm[l], Nr, nd)
+        assert np.abs(A - A.T).max() < 1e-10
+        ev = np.linalg.eigvalsh(A)
+        for k, n in enumerate(range(l + 1, l + 4)):
+            assert abs(ev[k] + 2.0 / n ** 2) < 2e-6, (l, n, ev[k])
+
+
+def test_legendre_orthonormal(he):
+    """sum_theta legb(theta, l, m) legf(l', theta, m) = delta_ll' (sph_gen.F90)."""
+    d = he.dims
+    nlat, L1, L2 = d["nlat"], d["lmax1"] + 1, d["lmax2"] + 1
+    lf2 = he.get("legf2").reshape(-1, nlat, L2)
+    lb2 = he.get("legb2").reshape(-1, L2, nlat)
+    for mi in range(lf2.shape[0]):
+        G = lb2[mi] @ lf2[mi]
+        nz = np.abs(np.diag(G)) > 0
+        assert np.abs(G[np.ix_(nz, nz)] - np.eye(nz.sum())).max() < 1e-12
+
+
+def test_gauss_lobatto_against_dsyev():
+    """Lobatto interior nodes = eigenvalues of the cldvr.cpp:82-139 Jacobi matrix."""
+    from td1c_b200.basis import lobatto
+    o = Oracle(W.HE_SMALL)
+    x = o.get("xrad")
+    # first element of the oracle grid on [0, 2] mapped back to [-1, 1]
+    nd = o.dims["ndvr"]
+    xe = x[: nd + 1] - 1.0
+    xl, _ = lobatto(nd)
+    assert np.abs(xe - xl).max() < 1e-14
+
+
+def test_poisson_against_lapack_and_slater():
+    """d2ll (bas_gen_d2ll.F90) equals scipy's dpbtrf factor, and the frozen-core
+    Hartree potential of a doubly occupied hydrogen 1s core (density 4 r^2
+    e^{-2r} per electron) is the closed form 2 [1/r - (1 + 1/r) e^{-2r}]
+    (hprod_mkv2jfc in hprod_set_wfn0.F90)."""
+    wl = dict(W.NE_SMALL, rmax=30.0, nfe=15, ndvr=10, orbitals=[(1, 0, 0, -1), (2, 0, 0, 1)], nela=2, nelb=2,
+              znuc=1.0, rmask=25.0)
+    o = Oracle(wl)
+    d = o.dims
+    Nr, nd = d["nrad"] - 1, d["ndvr"]
+    xr, wr = o.get("xrad"), o.get("wrad")
+    radk = o.get("radk").reshape(-1, 2 * nd + 1)
+    d2ll = o.get("d2ll").reshape(d["lmax2"] + 1, Nr, nd + 1)
+    for l in (0, 3):
+        A = np.zeros((nd + 1, Nr))
+        A[0] = l * (l + 1) / xr[1:Nr + 1] ** 2
+        for ir in range(1, Nr + 1):
+            for jr in range(ir, min(Nr, ir + nd) + 1):
+                A[jr - ir, ir - 1] += 2.0 * radk[ir, jr - ir + nd]
+        ref, info = sl.lapack.dpbtrf(A, lower=1)
+        assert info == 0
+        assert np.abs(ref - d2ll[l].T).max() < 1e-10 * np.abs(ref).max()
+    # hydrogen 1s frozen core: rho(r) = 4 r^2 e^{-2r} (unit norm), V = 1/r - (1 + 1/r) e^{-2r}
+    r = xr[1:Nr + 1]
+    orb = np.zeros((2, d["lmax1"] + 1, Nr), dtype=np.complex128)
+    orb[0, 0] = 2.0 * r * np.exp(-r) * np.sqrt(wr[1:Nr + 1])
+    orb[1, 0] = orb[0, 0]
+    o.set_wfn0(orb, np.ones(1, dtype=np.complex128))
+    v = o.get("v2jfc", True).real
+    exact = 2.0 * (1.0 / r - (1.0 + 1.0 / r) * np.exp(-2 * r))
+    inner = r < 20
+    assert np.abs(v[inner] - exact[inner]).max() < 1e-7  # FEDVR discretisation error of the 1s density
+
+
+@pytest.mark.parametrize("wl", [W.NE_SMALL, W.MIXED_SMALL, W.OPEN_SMALL], ids=lambda w: w["name"])
+def test_rhs_structure(wl):
+    """Properties of hprod_htot that hold exactly: zero field preserves orbital
+    norms (Re <phi|dphi/dt> = 0 with the Q projector), the CI derivative is
+    orthogonal to c for the Hermitian sigma, den1 is Hermitian with trace
+    N_active, frozen-core rows of hwfn vanish, int1e / int2e symmetries."""
+    o = Oracle(wl)
+    d = o.dims
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    hw, hc = o.htot(1.0, np.zeros(9), orb, cic)
+    nf = len(wl["orbitals"])
+    hw2, orb2 = hw.reshape(nf, -1), orb.reshape(nf, -1)
+    nfc = d["nfcore"]
+    assert np.abs(hw2[:nfc]).max() == 0.0
+    for f in range(nfc, nf):
+        assert abs(np.vdot(orb2[f], hw2[f]).real) < 1e-12
+    assert abs(np.vdot(cic, hc).real) < 1e-12
+    n = d["nact"]
+    D = o.get("den1", True).reshape(n, n).T
+    assert np.abs(D - D.conj().T).max() < 1e-13
+    nel_act = wl["nela"] + wl["nelb"] - 2 * d["ncore"]
+    assert abs(np.trace(D).real - nel_act) < 1e-12
+    I1 = o.get("int1e", True).reshape(n, n).T
+    assert np.abs(I1 - I1.conj().T).max() < 1e-12
+    I2 = o.get("int2e", True).reshape(n, n, n, n, order="F")
+    assert np.abs(I2 - np.conj(I2.transpose(1, 0, 3, 2))).max() < 1e-11
+    e = o.energies()
+    assert abs(e["ene_tot"] - (e["ene_core"] + e["ene_act"])) < 1e-12
+
+
+def test_hermitian_regularised_inverse():
+    """invden: U diag(d/(d^2 + 1e-15)) U^H equals scipy's eigh-based value."""
+    wl = W.NE_SMALL
+    o = Oracle(wl)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    o.htot(1.0, np.zeros(9), orb, cic)
+    n = o.dims["nact"]
+    D = o.get("den1", True).reshape(n, n).T
+    R = o.get("rden", True).reshape(n, n).T
+    w, U = np.linalg.eigh(D)
+    ref = (U * (w / (w * w + 1e-15))) @ U.conj().T
+    assert np.abs(R - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+def test_field_sin2_velocity():
+    """clfield1 velocity1: A = env F0/w sin(w t + cep), E = -dA/dt (6-point rule)."""
+    wl = W.NE_CAS
+    o = Oracle(wl)
+    famp = np.sqrt(wl["fint"] / 3.50944506e16)
+    w = 1239.84190 / (wl["wlen"] * 27.2113845)
+    T = wl["numcyc"] * 2 * np.pi / w
+    for t in (0.1 * T, 0.37 * T, 0.5 * T):
+        env = np.sin(np.pi * t / T) ** 2
+        A = env * famp / w * np.sin(w * t)
+        dA = famp / w * (2 * np.sin(np.pi * t / T) * np.cos(np.pi * t / T) * np.pi / T * np.sin(w * t)
+                         + env * w * np.cos(w * t))
+        lf = o.field(t)
+        assert abs(lf[2] - A) < 1e-14 and abs(lf[8] - A) < 1e-14
+        assert abs(lf[5] + dA) < 1e-8 * famp
