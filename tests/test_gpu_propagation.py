@@ -73,7 +73,8 @@ def test_full_size_rhs(cuda_ok, wl):
         nf = len(wl["orbitals"])
         nfc = o.dims["nfcore"]
         hw2, o2 = hw.reshape(nf, -1), orb.reshape(nf, -1)
-        assert np.abs(hw2[:nfc]).max() == 0.0
+        if nfc:
+            assert np.abs(hw2[:nfc]).max() == 0.0
         for f in range(nfc, nf):
             assert abs(np.vdot(o2[f], hw2[f]).real) < 1e-11 * np.linalg.norm(hw2[f])
         if o.dims["nact"]:
