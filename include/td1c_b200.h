@@ -118,6 +118,41 @@ void* td1c_gpu_stream(void);
 int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d_wfn, const void* d_cic,
                      void* d_hwfn, void* d_hcic, double* ms, char* names, int names_cap);
 
+/* MO two-electron integrals for callers that cannot allocate GPU memory.
+ * No counterpart in the reference.
+ *
+ * Computes int2e(i,j,k,l) = sum_x rho2_ij[x] v2sph_kl[x] (x over K complex
+ * basis values, m_i + m_k = m_j + m_l, int2e(i,j,k,l) = conj(int2e(j,i,l,k)))
+ * like the integrals of hprod_htot_, and needs no bound context and no
+ * device allocation.  It is meant for hosts whose GPU memory belongs to
+ * their own pool allocator, real-time loops that must not call cudaMalloc
+ * (which synchronises the device and can fail), and frameworks that lend
+ * only their own buffers.
+ *
+ *   nact        active orbitals, 1..16
+ *   mval        host array [nact], m of each active orbital
+ *   K           complex values per pair (Nr (lmax2 + 1) in the RHS)
+ *   d_rho2      device [nact(nact+1)/2][K] complex: pair densities of
+ *               (a, b), a >= b, in the packed lower triangle stored by
+ *               columns, (0,0) (1,0) .. (n-1,0) (1,1) (2,1) ..
+ *   d_v2sph     device, same layout: pair potentials
+ *   d_int2e     device [nact^4] complex output, int2e(i,j,k,l) at
+ *               i + n (j + n (k + n l)); cleared by the call
+ *   stream      cudaStream_t the work is queued on (NULL: legacy stream)
+ *
+ * Scratch (block tables and split-K partial sums) lives in one 8 MiB device
+ * array built into the library, held by every GPU that loads it until the
+ * process exits.  All calls on a device share that array, and it keeps the
+ * last call's contents: calls whose GPU work overlaps (different streams or
+ * unordered host threads) race and give wrong results.  The first call on
+ * each device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.  Returns 0 on
+ * success, 16 with a message on stderr when a size exceeds these limits or
+ * an argument is null, 8 when a CUDA call fails.  The work is asynchronous
+ * on the stream. */
+int td1c_gpu_int2e_static(int nact, const int* mval, long K, const double* d_rho2, const double* d_v2sph,
+                          double* d_int2e, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
