@@ -31,6 +31,7 @@ enum : int {
   ST_NONFINITE = 4,    // non-finite value detected in an output
   ST_CUDA = 8,         // a CUDA API call failed on the host side
   ST_CONFIG = 16,      // unsupported configuration
+  ST_TIMEOUT = 32,     // a bounded wait on an asynchronous copy ran out
 };
 
 }  // namespace td1c

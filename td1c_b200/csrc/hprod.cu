@@ -77,6 +77,8 @@ struct Ctx {
   double *xrad = nullptr, *mask = nullptr, *radk = nullptr, *radk0 = nullptr, *radp = nullptr, *cost = nullptr;
   double *legf1 = nullptr, *legb1 = nullptr, *legf2 = nullptr, *legb2 = nullptr, *alph = nullptr;
   double *tdiag = nullptr, *d2ll = nullptr, *d2rinv = nullptr, *rpl0 = nullptr, *rpl1 = nullptr, *invr = nullptr, *fac2 = nullptr, *fac1 = nullptr;
+  double *ps_tabf = nullptr, *ps_tabb = nullptr;  // Poisson row tables (forward, backward)
+  PoissonArgs ps_main{}, ps_fcfc{};  // Poisson arguments with encoded tensor maps (RHS pairs, fcfc pairs)
   int* d_mval = nullptr;
   // ---- pairs
   int npair = 0, npair_all = 0, nfcfc = 0;
@@ -526,6 +528,18 @@ __global__ void dtorb_kernel(int Nr, int L1, int nfun, int nfcore, int icomp, do
 // ===========================================================================
 // host set-up helpers
 // ===========================================================================
+// Poisson arguments for the stored pairs pair0 .. pair0 + npair - 1
+PoissonArgs poisson_args(const Ctx& c, int npair, int pair0) {
+  PoissonArgs pa{};
+  pa.Nr = c.Nr; pa.L2 = c.L2; pa.nd = c.nd; pa.npair = npair; pa.d2ll = c.d2ll; pa.d2rinv = c.d2rinv;
+  pa.rpl0 = c.rpl0; pa.rpl1 = c.rpl1; pa.invr = c.invr; pa.fac2 = c.fac2; pa.fac1 = c.fac1;
+  pa.pair_m = c.pair_m ? c.pair_m + pair0 : nullptr;
+  pa.rho2 = c.rho2 ? c.rho2 + (size_t)pair0 * c.nbas2 : nullptr;
+  pa.v2sph = c.v2sph ? c.v2sph + (size_t)pair0 * c.nbas2 : nullptr;
+  pa.tabf = c.ps_tabf; pa.tabb = c.ps_tabb; pa.status = c.d_status;
+  return pa;
+}
+
 int build_tables(Ctx& c) {
   const int bw = 2 * c.nd + 1;
   c.xrad = dupload(c.h_xrad);
@@ -571,6 +585,13 @@ int build_tables(Ctx& c) {
   int hst = 0;
   cudaMemcpy(&hst, dstat, sizeof(int), cudaMemcpyDeviceToHost);
   if (hst) { fprintf(stderr, "td1c_b200: Poisson band factorisation failed\n"); return ST_CHOLESKY; }
+  {
+    const size_t nrow = (size_t)c.L2 * ((Nr + c.nd - 1) / c.nd * c.nd) * poisson_row_width(c.nd);
+    c.ps_tabf = dalloc<double>(nrow);
+    c.ps_tabb = dalloc<double>(nrow);
+    PoissonArgs pa = poisson_args(c, c.npair, 0);
+    if (launch_poisson_tables(pa, c.ps_tabf, c.ps_tabb, 0)) return ST_CUDA;
+  }
   c.tdiag = dalloc<double>((size_t)Nr * c.L1);
   c.v2jfc = dalloc<double>(Nr);
   tdiag_kernel<<<(Nr * c.L1 + 255) / 256, 256>>>(Nr, c.L1, c.nd, c.znuc, c.xrad, c.radk, c.radk0, nullptr, c.tdiag);
@@ -618,6 +639,9 @@ int build_state(Ctx& c) {
   c.d_status = dalloc<int>(1);
   c.d_scalar = dalloc<double>(4);
   if (!c.orb || !c.W || !c.rho2 || !c.v2sph) return ST_CUDA;
+  c.ps_main = poisson_args(c, c.npair, 0);
+  c.ps_fcfc = poisson_args(c, c.nfcfc, c.npair);
+  if (poisson_encode_maps(c.ps_main) || poisson_encode_maps(c.ps_fcfc)) return ST_CUDA;
   return 0;
 }
 
@@ -976,11 +1000,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   if (c.neltot >= 2 && c.npair > 0) {
     rc |= chk("rho gemm", gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true));
     mark();  // end rho_gemm
-    PoissonArgs pa{};
-    pa.Nr = c.Nr; pa.L2 = c.L2; pa.nd = c.nd; pa.npair = c.npair; pa.d2ll = c.d2ll; pa.d2rinv = c.d2rinv;
-    pa.rpl0 = c.rpl0; pa.rpl1 = c.rpl1; pa.invr = c.invr; pa.fac2 = c.fac2; pa.fac1 = c.fac1; pa.pair_m = c.pair_m;
-    pa.rho2 = c.rho2; pa.v2sph = c.v2sph;
-    rc |= chk("poisson", launch_poisson(pa, 0, st));
+    rc |= chk("poisson", launch_poisson(c.ps_main, st));
     c.launches++;
     mark();  // end poisson
     rc |= chk("W gemm", gemm(c, c.b_W, c.npair, c.nlat, c.L2, false));
@@ -1260,11 +1280,7 @@ void hprod_set_wfn0_(const double* wfn, const double* cic, const char* v2xfc_typ
   if (c.igauge == 0) cudaMemcpyAsync(c.orb, c.orb0, c.nfcore * c.nbas * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
   else launch_legendre_gemm(c.b_orbfc, c.nfcore, c.L1, c.nlat, 2 * c.Nr, false, st);  // orb(fc) = ang2sph1(orbg(fc))
   launch_legendre_gemm(c.b_rho_fcfc, c.nfcfc, c.L2, c.nlat, 2 * c.Nr, true, st);
-  PoissonArgs pa{};
-  pa.Nr = c.Nr; pa.L2 = c.L2; pa.nd = c.nd; pa.npair = c.nfcfc; pa.d2ll = c.d2ll; pa.d2rinv = c.d2rinv;
-  pa.rpl0 = c.rpl0; pa.rpl1 = c.rpl1; pa.invr = c.invr; pa.fac2 = c.fac2; pa.fac1 = c.fac1; pa.pair_m = c.pair_m + c.npair;
-  pa.rho2 = c.rho2 + c.npair * c.nbas2; pa.v2sph = c.v2sph + c.npair * c.nbas2;
-  launch_poisson(pa, sizeof(double) * (size_t)c.Nr * (c.nd + 1), st);
+  launch_poisson(c.ps_fcfc, st);
   launch_legendre_gemm(c.b_W_fcfc, c.nfcfc, c.nlat, c.L2, 2 * c.Nr, false, st);
   // frozen-core energy: enefc = 2 Re <phi|h0|phi> + Re <phi| v2jfc - sum_j W(j,i) phi_j >
   // with h0 from the bare kinetic table (before v2jfc is added)

@@ -11,6 +11,8 @@
 // (hprod_mkv2mf.F90:257-345) is never materialised -- consumers read the
 // stored pair with a conjugation flag.
 #pragma once
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace td1c {
@@ -55,8 +57,18 @@ struct PoissonArgs {
   const int* pair_m;     // [npair] m of the pair (m_b - m_a)
   const cplx* rho2;      // [npair][L2][Nr]
   cplx* v2sph;           // [npair][L2][Nr]
+  const double* tabf;    // [L2][Np][W] forward row tables (launch_poisson_tables)
+  const double* tabb;    // [L2][Np][W] backward row tables
+  int* status;           // device status word (ST_TIMEOUT on a stalled copy)
+  int boxp;              // pairs per TMA box (min(16, npair)), set by poisson_encode_maps
+  CUtensorMap tm_rho;    // rho2 viewed as [npair][L2][2 Nr] float64, box (2 nd, 1, boxp)
+  CUtensorMap tm_v2;     // v2sph, same view
 };
-int launch_poisson(const PoissonArgs& a, size_t smem_bytes, cudaStream_t st);
+// doubles per row of the Poisson row tables: nd band values + 3, even
+__host__ __device__ inline int poisson_row_width(int nd) { return (nd + 5) / 2 * 2; }
+int poisson_encode_maps(PoissonArgs& a);  // fills boxp, tm_rho, tm_v2 from rho2, v2sph, npair
+int launch_poisson_tables(const PoissonArgs& a, double* tabf, double* tabb, cudaStream_t st);
+int launch_poisson(const PoissonArgs& a, cudaStream_t st);
 
 // ---- mean-field action on the (r, theta) grid (hprod_mfprod2.F90)
 struct Act2Block {     // one dense (ij) x (kl) block of the 2-RDM contraction

@@ -7,159 +7,355 @@
 // solves  L_l L_l^T x = rhs  with the dpbtrf factor of
 // [l(l+1)/r^2 + 2 T] (band nd) by dpbtrs, and returns
 //     v2sph = (x + t r^(l+1) sqrt(w_r)) 4 pi / ((2l+1) r sqrt(w_r)).
-// One CTA owns one l; every thread runs the forward and back substitution of
-// one (pair, re|im) right-hand side.  The substitution is sequential in r and
-// the SM holds only a few warps, so the loop is written to be branch-free:
-// shared memory holds the l's band factor (diagonal replaced by its
-// reciprocal) framed by nd zero rows on each side and identity rows that
-// round Nr up to a multiple of nd, so no step needs a bounds test; the last
-// nd solution values live in registers (nd is a template parameter); the
-// band terms of older values are summed (oldest first, as dtbsv) into four
-// independent partial sums so only the newest value's FMA and the
-// reciprocal multiply sit on the recurrence; inputs and the final scaling
-// columns are loaded one block of nd rows ahead.  The homogeneous boundary
-// term and the final scaling are fused into the back substitution.
+//
+// Layout of the work: one warp per (l, group of 16 pairs); lane 2P+c solves
+// the real (c = 0) or imaginary (c = 1) part of pair P.  The substitutions
+// run row by row in the order of dtbsv (forward: band terms oldest first,
+// backward: farthest first), with the last nd solution values in registers
+// and the older band terms summed into four partial sums so only the newest
+// term sits on the recurrence.  Everything a row needs from the matrix side
+// -- the nd band values, the reciprocal diagonal and the two per-row scaling
+// factors -- is one row of a per-l table (tabf for the forward sweep, tabb
+// for the backward one), so a row costs a handful of 128-bit broadcast loads
+// from shared memory.  Blocks of nd rows move between HBM and shared memory
+// by the TMA: per block one bulk copy of the table rows and one tensor copy
+// of the 16 pairs' nd complex values (a 3-d box over [pair][l][2 Nr], rows
+// past Nr zero-filled) land in a 4-stage ring tracked by mbarriers, and the
+// forward result y and the final v2sph leave through one tensor store per
+// block (clipped at Nr).  y is parked in the v2sph buffer between the
+// sweeps.  Every mbarrier wait is bounded; a wait that runs out sets
+// ST_TIMEOUT in the status word and the warp drains and returns.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace td1c {
 
+namespace {
+
+constexpr int PS_PAIRS = 16;      // pairs per warp
+constexpr int PS_STAGES = 4;      // depth of the load ring
+constexpr unsigned long long PS_WAIT_NS = 1000000000ull;  // bound of one mbarrier wait: 1 s
+
+__device__ __forceinline__ unsigned su32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(su32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// bounded wait; false when PS_WAIT_NS ran out
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  while (globaltimer_ns() - t0 < PS_WAIT_NS)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(su32(dst)),
+               "l"(src), "r"(bytes), "r"(su32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tensor_load(void* dst, const CUtensorMap* tm, int x, int y, int z, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          su32(dst)),
+      "l"(tm), "r"(x), "r"(y), "r"(z), "r"(su32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tensor_store(const CUtensorMap* tm, int x, int y, int z, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm), "r"(x),
+               "r"(y), "r"(z), "r"(su32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// byte offset of the staged-block ring: 128 bytes of mbarriers, the table
+// stages, rounded up to the 128-byte alignment of a TMA box
+__host__ __device__ constexpr size_t poisson_rbuf_offset(int nd, int w) {
+  return (128 + (size_t)PS_STAGES * nd * w * 8 + 127) / 128 * 128;
+}
+
+}  // namespace
+
+// Row tables of width W = ND + 4 rounded up to even (16-byte rows):
+//   tabf[l][j] = { L(j, j-ND) .. L(j, j-1), 1/L(j,j), invr(j), rpl0(j), 0.. }
+//   tabb[l][j] = { L(j+ND, j) .. L(j+1, j), 1/L(j,j), rpl1(j), fac2(j), 0.. }
+// for j < Np (Nr rounded up to a multiple of ND); rows j >= Nr are identity
+// rows (band 0, reciprocal diagonal 1, factors 0), band entries that fall
+// outside 0..Nr-1 are 0.
+__global__ void poisson_tables_kernel(PoissonArgs a, double* __restrict__ tabf, double* __restrict__ tabb) {
+  const int ND = a.nd, LD = ND + 1, W = poisson_row_width(ND), Nr = a.Nr;
+  const int Np = (Nr + ND - 1) / ND * ND;
+  const size_t n = (size_t)a.L2 * Np;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int l = (int)(e / Np), j = (int)(e % Np);
+    const double* gL = a.d2ll + (size_t)l * Nr * LD;
+    double* f = tabf + e * W;
+    double* b = tabb + e * W;
+    for (int i = 0; i < W; ++i) { f[i] = 0.0; b[i] = 0.0; }
+    if (j >= Nr) { f[ND] = 1.0; b[ND] = 1.0; continue; }
+    const size_t lr = (size_t)l * Nr + j;
+    for (int i = 0; i < ND; ++i) {
+      const int k = ND - i;
+      if (j - k >= 0) f[i] = gL[(size_t)(j - k) * LD + k];
+      if (j + k < Nr) b[i] = gL[(size_t)j * LD + k];
+    }
+    f[ND] = a.d2rinv[lr]; f[ND + 1] = a.invr[lr]; f[ND + 2] = a.rpl0[lr];
+    b[ND] = a.d2rinv[lr]; b[ND + 1] = a.rpl1[lr]; b[ND + 2] = a.fac2[lr];
+  }
+}
+
 template <int ND>
-__global__ void __launch_bounds__(128) poisson_kernel(PoissonArgs a) {
-  extern __shared__ double sm[];
+__global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ PoissonArgs a) {
+  constexpr int W = (ND + 5) / 2 * 2;  // table row width (doubles)
+  constexpr int BOX = 2 * ND;          // doubles per pair in a staged block
+  extern __shared__ __align__(128) unsigned char ps_smem[];
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(ps_smem);  // [PS_STAGES]
+  double* fbuf = reinterpret_cast<double*>(ps_smem + 128);                   // [S][ND][W]
+  double* rbuf = reinterpret_cast<double*>(ps_smem + poisson_rbuf_offset(ND, W));  // [S][16][BOX]
+  double* ybuf = rbuf + PS_STAGES * PS_PAIRS * BOX;                                 // [2][16][BOX]
+
   const int l = blockIdx.x;
+  const int lane = threadIdx.x;
   const int Nr = a.Nr;
-  const int nb = (Nr + ND - 1) / ND;
-  const int Np = nb * ND;                          // padded rows
-  constexpr int LD = ND + 1;
-  double* sL = sm + (size_t)ND * LD;               // row j at sL + LD j, rows -ND .. Np+ND-1
-  double* s0 = sm + (size_t)(Np + 2 * ND) * LD;    // [Np] r^l / (2 pi)
-  double* sI = s0 + Np;                            // [Np] (2l+1) / (2 pi r sqrt w)
-  const double* __restrict__ gL = a.d2ll + (size_t)l * Nr * LD;
-  for (int e = threadIdx.x; e < (Np + 2 * ND) * LD; e += blockDim.x) {
-    const int row = e / LD - ND, k = e % LD;
-    double v = 0.0;
-    if (row >= 0 && row < Nr) v = (k == 0) ? a.d2rinv[(size_t)l * Nr + row] : gL[(size_t)row * LD + k];
-    else if (row >= Nr && row < Np && k == 0) v = 1.0;  // identity padding rows
-    sm[e] = v;
+  const int nb = (Nr + ND - 1) / ND, Np = nb * ND;
+  const int p0 = blockIdx.y * PS_PAIRS;
+  const int np = min(PS_PAIRS, a.npair - p0);
+  const int P = lane >> 1, c = lane & 1;
+  bool active = P < np;
+  if (active) {
+    const int m = a.pair_m[p0 + P];
+    active = l >= (m < 0 ? -m : m);
   }
-  for (int j = threadIdx.x; j < Np; j += blockDim.x) {
-    s0[j] = j < Nr ? a.rpl0[(size_t)l * Nr + j] : 0.0;
-    sI[j] = j < Nr ? a.invr[(size_t)l * Nr + j] : 0.0;
+  const double* tabf_l = a.tabf + (size_t)l * Np * W;
+  const double* tabb_l = a.tabb + (size_t)l * Np * W;
+  // box bytes: rows past Nr and pairs past npair arrive zero-filled and count
+  const unsigned tx_bytes = (unsigned)(ND * W * 8) + (unsigned)(BOX * a.boxp * 8);
+
+  if (lane == 0) {
+    for (int s = 0; s < PS_STAGES; ++s) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
-  const int nsys = 2 * a.npair;
-  const double fac1 = a.fac1[l];
-  const double* __restrict__ rpl1 = a.rpl1 + (size_t)l * Nr;
-  const double* __restrict__ fac2 = a.fac2 + (size_t)l * Nr;
-  for (int s = threadIdx.x + blockIdx.y * blockDim.x; s < nsys; s += blockDim.x * gridDim.y) {
-    const int p = s >> 1, c = s & 1;
-    const int m = a.pair_m[p];
-    const int am = m < 0 ? -m : m;
-    double* __restrict__ out = reinterpret_cast<double*>(a.v2sph + ((size_t)p * a.L2 + l) * Nr) + c;
-    if (l < am) {
-      for (int r = 0; r < Nr; ++r) out[2 * r] = 0.0;
-      continue;
+  __syncwarp();
+
+  // issue the loads of task q (forward block q, or backward block 2 nb - 1 - q)
+  auto issue = [&](int q) {
+    if (lane == 0) {
+      const bool fwd = q < nb;
+      const int b = fwd ? q : 2 * nb - 1 - q;
+      const int s = q % PS_STAGES;
+      mbar_expect_tx(&bar[s], tx_bytes);
+      bulk_load(fbuf + (size_t)s * ND * W, (fwd ? tabf_l : tabb_l) + (size_t)b * ND * W, ND * W * 8, &bar[s]);
+      tensor_load(rbuf + (size_t)s * PS_PAIRS * BOX, fwd ? &a.tm_rho : &a.tm_v2, 2 * b * ND, l, p0, &bar[s]);
     }
-    const double* __restrict__ in = reinterpret_cast<const double*>(a.rho2 + ((size_t)p * a.L2 + l) * Nr) + c;
-    double t = 0.0;
-    double win[ND], cur[ND], nxt[ND];
+  };
+  // store ybuf half h to the rows of block b (rows past Nr and pairs past
+  // npair are clipped by the tensor map)
+  auto store = [&](int h, int b) {
+    fence_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tensor_store(&a.tm_v2, 2 * b * ND, l, p0, ybuf + (size_t)h * PS_PAIRS * BOX);
+      bulk_commit();
+    }
+  };
+  auto wait_task = [&](int q) -> bool {  // warp-uniform result
+    const bool r = mbar_wait(&bar[q % PS_STAGES], (unsigned)((q / PS_STAGES) & 1));
+    return __all_sync(0xffffffffu, r);
+  };
+
+  bool ok = true;
+  int issued = 0, consumed = 0;  // tasks issued / consumed
+  double win[ND];
+  double t = 0.0;
+
+  // ---- forward substitution  L y = rhs
+  for (; issued < min(PS_STAGES, nb); ++issued) issue(issued);
 #pragma unroll
-    for (int k = 0; k < ND; ++k) { win[k] = 0.0; cur[k] = __ldg(in + 2 * min(k, Nr - 1)); }
-    // ---- forward substitution  L y = rhs  (y kept in out for the back pass)
-    for (int b = 0; b < nb; ++b) {
-      const int jb = b * ND;
+  for (int k = 0; k < ND; ++k) win[k] = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    if (!wait_task(b)) { ok = false; break; }
+    consumed = b + 1;
+    if (lane == 0) bulk_wait_read_1();  // ybuf half (b & 1) no longer read by the store of block b - 2
+    __syncwarp();
+    const int s = b % PS_STAGES, h = b & 1;
+    const double* __restrict__ fb = fbuf + (size_t)s * ND * W;
+    const double* __restrict__ rb = rbuf + (size_t)(s * PS_PAIRS + P) * BOX + c;
+    double* __restrict__ yb = ybuf + (size_t)(h * PS_PAIRS + P) * BOX + c;
+    // the block's inputs first and its results after it, so no shared-memory
+    // store sits between the rows and the loads of later rows can be hoisted
+    double in[ND];
 #pragma unroll
-      for (int u = 0; u < ND; ++u) nxt[u] = __ldg(in + 2 * min(jb + ND + u, Nr - 1));
+    for (int u = 0; u < ND; ++u) in[u] = active ? rb[2 * u] : 0.0;
 #pragma unroll
-      for (int u = 0; u < ND; ++u) {
-        const int j = jb + u;
-        const double rho = cur[u];
-        t = fma(rho, s0[j], t);
-        const double* Lr = sL + (size_t)LD * j;
-        // L(j, j-k) = ab[k + LD (j-k)] = Lr[-ND k]; y_{j-k} in win[(u-k) mod ND]
-        double pa = rho * sI[j], pb = 0.0, pc = 0.0, pd = 0.0;
+    for (int u = 0; u < ND; ++u) {
+      double fr[W];
 #pragma unroll
-        for (int k = ND; k >= 2; --k) {
-          const double term = Lr[-ND * k] * win[(u - k + ND) % ND];
-          const int g = (ND - k) & 3;
-          if (g == 0) pa -= term; else if (g == 1) pb -= term; else if (g == 2) pc -= term; else pd -= term;
-        }
-        const double sacc = fma(-Lr[-ND], win[(u - 1 + ND) % ND], (pa + pb) + (pc + pd));
-        const double y = sacc * Lr[0];
-        win[u] = y;
-        if (j < Nr) out[2 * j] = y;
+      for (int i = 0; i < W / 2; ++i) {
+        const double2 v = reinterpret_cast<const double2*>(fb + u * W)[i];
+        fr[2 * i] = v.x; fr[2 * i + 1] = v.y;
       }
+      const double rho = in[u];
+      t = fma(rho, fr[ND + 2], t);
+      // L(j, j-k) = fr[ND - k]; y_{j-k} in win[(u - k) mod ND]
+      double pa = rho * fr[ND + 1], pb = 0.0, pc = 0.0, pd = 0.0;
 #pragma unroll
-      for (int u = 0; u < ND; ++u) cur[u] = nxt[u];
+      for (int k = ND; k >= 2; --k) {
+        const double term = fr[ND - k] * win[(u - k + ND) % ND];
+        const int g = (ND - k) & 3;
+        if (g == 0) pa -= term; else if (g == 1) pb -= term; else if (g == 2) pc -= term; else pd -= term;
+      }
+      const double sacc = fma(-fr[ND - 1], win[(u - 1 + ND) % ND], (pa + pb) + (pc + pd));
+      win[u] = sacc * fr[ND];
     }
-    // ---- back substitution  L^T x = y  fused with the boundary term and scaling
-    //      v2sph = (x + t fac1 r^(l+1) sqrt(w)) 4 pi / ((2l+1) r sqrt(w))
-    t *= fac1;
-    double c1[ND], c2[ND], n1[ND], n2[ND];
+#pragma unroll
+    for (int u = 0; u < ND; ++u) yb[2 * u] = win[u];
+    store(h, b);
+    if (issued < nb) issue(issued++);
+  }
+  // all y stores complete and visible before the backward sweep reads them back
+  if (lane == 0) bulk_wait_all();
+  fence_async_global();
+  __syncwarp();
+
+  // ---- back substitution  L^T x = y, fused with the boundary term and scaling
+  //      v2sph = (x + t fac1 r^(l+1) sqrt(w)) 4 pi / ((2l+1) r sqrt(w))
+  if (ok) {
+    t *= a.fac1[l];
 #pragma unroll
     for (int k = 0; k < ND; ++k) win[k] = 0.0;
-    {
-      const int jb = (nb - 1) * ND;
+    for (; issued < min(nb + PS_STAGES, 2 * nb); ++issued) issue(issued);
+    for (int i = 0; i < nb; ++i) {
+      const int q = nb + i, b = nb - 1 - i;
+      if (!wait_task(q)) { ok = false; break; }
+      consumed = q + 1;
+      if (lane == 0) bulk_wait_read_1();
+      __syncwarp();
+      const int s = q % PS_STAGES, h = q & 1;
+      const double* __restrict__ fb = fbuf + (size_t)s * ND * W;
+      const double* __restrict__ rb = rbuf + (size_t)(s * PS_PAIRS + P) * BOX + c;
+      double* __restrict__ yb = ybuf + (size_t)(h * PS_PAIRS + P) * BOX + c;
+      double in[ND];
 #pragma unroll
-      for (int u = 0; u < ND; ++u) {
-        const int jj = min(jb + u, Nr - 1);
-        cur[u] = (jb + u < Nr) ? out[2 * jj] : 0.0;
-        c1[u] = __ldg(rpl1 + jj); c2[u] = __ldg(fac2 + jj);
-      }
-    }
-    for (int b = nb - 1; b >= 0; --b) {
-      const int jb = b * ND;
-      if (b > 0) {
-#pragma unroll
-        for (int u = 0; u < ND; ++u) {
-          const int jj = jb - ND + u;
-          nxt[u] = out[2 * jj]; n1[u] = __ldg(rpl1 + jj); n2[u] = __ldg(fac2 + jj);
-        }
-      }
+      for (int u = 0; u < ND; ++u) in[u] = active ? rb[2 * u] : 0.0;
 #pragma unroll
       for (int u = ND - 1; u >= 0; --u) {
-        const int j = jb + u;
-        const double* Lc = sL + (size_t)LD * j;
-        // L(j+k, j) = ab[k + LD j] = Lc[k]; x_{j+k} in win[(u+k) mod ND]; farthest first
-        double pa = cur[u], pb = 0.0, pc = 0.0, pd = 0.0;
+        double fr[W];
+#pragma unroll
+        for (int k2 = 0; k2 < W / 2; ++k2) {
+          const double2 v = reinterpret_cast<const double2*>(fb + u * W)[k2];
+          fr[2 * k2] = v.x; fr[2 * k2 + 1] = v.y;
+        }
+        const double yv = in[u];
+        // L(j+k, j) = fr[ND - k]; x_{j+k} in win[(u + k) mod ND]; farthest first
+        double pa = yv, pb = 0.0, pc = 0.0, pd = 0.0;
 #pragma unroll
         for (int k = ND; k >= 2; --k) {
-          const double term = Lc[k] * win[(u + k) % ND];
+          const double term = fr[ND - k] * win[(u + k) % ND];
           const int g = (ND - k) & 3;
           if (g == 0) pa -= term; else if (g == 1) pb -= term; else if (g == 2) pc -= term; else pd -= term;
         }
-        const double sacc = fma(-Lc[1], win[(u + 1) % ND], (pa + pb) + (pc + pd));
-        const double x = sacc * Lc[0];
-        win[u] = x;
-        if (j < Nr) out[2 * j] = fma(t, c1[u], x) * c2[u];
+        const double sacc = fma(-fr[ND - 1], win[(u + 1) % ND], (pa + pb) + (pc + pd));
+        win[u] = sacc * fr[ND];
       }
-      if (b > 0) {
 #pragma unroll
-        for (int u = 0; u < ND; ++u) { cur[u] = nxt[u]; c1[u] = n1[u]; c2[u] = n2[u]; }
+      for (int u = 0; u < ND; ++u) {
+        yb[2 * u] = fma(t, fb[u * W + ND + 1], win[u]) * fb[u * W + ND + 2];
       }
+      store(h, b);
+      if (issued < 2 * nb) issue(issued++);
     }
   }
+  if (!ok) {
+    if (lane == 0) atomicOr(a.status, ST_TIMEOUT);
+    // let the loads still in flight land before the shared memory is released
+    for (int q = consumed; q < issued; ++q) (void)wait_task(q);
+  }
+  if (lane == 0) bulk_wait_all();
 }
 
 template <int ND>
 static int launch_nd(const PoissonArgs& a, cudaStream_t st) {
+  constexpr int W = (ND + 5) / 2 * 2, BOX = 2 * ND;
+  const size_t smem = poisson_rbuf_offset(ND, W) + sizeof(double) * (size_t)(PS_STAGES + 2) * PS_PAIRS * BOX;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(poisson_kernel<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(poisson_kernel<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  const int Np = (a.Nr + ND - 1) / ND * ND;
-  const size_t smem = sizeof(double) * ((size_t)(Np + 2 * ND) * (ND + 1) + 2 * (size_t)Np);
-  if (smem > 227 * 1024) return (int)cudaErrorInvalidValue;
-  int nsys = 2 * a.npair;
-  int ysplit = (nsys + 127) / 128;
-  dim3 grid(a.L2, ysplit);
-  poisson_kernel<ND><<<grid, 128, smem, st>>>(a);
+  if (a.npair <= 0) return 0;
+  if (a.boxp != std::min(PS_PAIRS, a.npair)) return (int)cudaErrorInvalidValue;  // maps not encoded
+  dim3 grid(a.L2, (a.npair + PS_PAIRS - 1) / PS_PAIRS);
+  poisson_kernel<ND><<<grid, 32, smem, st>>>(a);
   return (int)cudaGetLastError();
 }
 
-int launch_poisson(const PoissonArgs& a, size_t, cudaStream_t st) {
+// 3-d views [npair][L2][2 Nr] of rho2 and v2sph with a box of one block of
+// nd complex rows x one l x up to 16 pairs
+int poisson_encode_maps(PoissonArgs& a) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      fprintf(stderr, "td1c_b200: cuTensorMapEncodeTiled is not available\n");
+      return (int)cudaErrorNotSupported;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  if (a.npair <= 0) { a.boxp = 0; return 0; }
+  a.boxp = std::min(PS_PAIRS, a.npair);
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * a.Nr, (cuuint64_t)a.L2, (cuuint64_t)a.npair};
+  const cuuint64_t strides[2] = {(cuuint64_t)a.Nr * 16, (cuuint64_t)a.L2 * a.Nr * 16};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * a.nd), 1u, (cuuint32_t)a.boxp};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  CUtensorMap* maps[2] = {&a.tm_rho, &a.tm_v2};
+  const void* bases[2] = {a.rho2, a.v2sph};
+  for (int i = 0; i < 2; ++i) {
+    CUresult r = encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(bases[i]), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      fprintf(stderr, "td1c_b200: cuTensorMapEncodeTiled (Poisson %s) failed: %d\n", i ? "v2sph" : "rho2", (int)r);
+      return (int)cudaErrorInvalidValue;
+    }
+  }
+  return 0;
+}
+
+int launch_poisson_tables(const PoissonArgs& a, double* tabf, double* tabb, cudaStream_t st) {
+  const int Np = (a.Nr + a.nd - 1) / a.nd * a.nd;
+  const size_t n = (size_t)a.L2 * Np;
+  poisson_tables_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, tabf, tabb);
+  return (int)cudaGetLastError();
+}
+
+int launch_poisson(const PoissonArgs& a, cudaStream_t st) {
   switch (a.nd) {
     case 4: return launch_nd<4>(a, st);
     case 6: return launch_nd<6>(a, st);
