@@ -79,6 +79,7 @@ struct Ctx {
   double *tdiag = nullptr, *d2ll = nullptr, *d2rinv = nullptr, *rpl0 = nullptr, *rpl1 = nullptr, *invr = nullptr, *fac2 = nullptr, *fac1 = nullptr;
   double *ps_tabf = nullptr, *ps_tabb = nullptr;  // Poisson row tables (forward, backward)
   PoissonArgs ps_main{}, ps_fcfc{};  // Poisson arguments with encoded tensor maps (RHS pairs, fcfc pairs)
+  MfprodArgs mf{};  // mean-field action arguments with encoded tensor maps
   int* d_mval = nullptr;
   // ---- pairs
   int npair = 0, npair_all = 0, nfcfc = 0;
@@ -104,6 +105,8 @@ struct Ctx {
   int* ent_index = nullptr;  // [5][nfun][nfun] -> entry id or -1 (A, B, C, E, GV)
   Int2eArgs i2{};
   int i2_nsplit = 128;
+  I2dArgs i2d{};          // int2e on the FP64 tensor cores
+  bool i2_dmma = false;   // the DMMA plan fits in shared memory
   // act2 blocks
   int a2_nblk = 0, a2_nrow = 0, a2_ncol = 0, a2_ncoef = 0;
   Act2Block* a2_blk = nullptr; int2* a2_rows = nullptr; int2* a2_cols = nullptr;
@@ -779,9 +782,91 @@ int build_reductions(Ctx& c) {
   c.i2.nact = n; c.i2.nblocks = (int)blocks.size(); c.i2.nblkent = (int)dst.size(); c.i2.K = c.nbas2;
   c.i2.blocks = dupload(blocks); c.i2.row_pair = dupload(rows); c.i2.col_pair = dupload(cols); c.i2.ent_dst = dupload(dst);
   c.i2.rho2 = c.rho2; c.i2.v2sph = c.v2sph;
-  c.i2.partial = dalloc<cplx>((size_t)c.i2_nsplit * std::max(1, c.i2.nblkent));
   c.int2e = dalloc<cplx>((size_t)std::max(1, n * n * n * n));
   c.i2.int2e = c.int2e;
+  // the same entries as DMMA tiles: per Delta the rows ij (i >= j) padded to
+  // m-tiles of 8 pairs, the columns kl padded to n-tiles of 8, the entry of
+  // (row r, column y) at ent0 + r ncol + y in the (i outer, j inner) x
+  // (k outer, l inner) order of the block list above; groups (m-tile x up
+  // to I2D_NTMAX n-tiles) are spread over the warps so that the four
+  // schedulers of an SM get similar numbers of n-tiles
+  {
+    std::vector<int> a_pair, a_ent, b_col;
+    std::vector<int2> b_pair;
+    std::vector<I2dGroup> groups;
+    std::vector<int4> dst2;
+    int dmax = 0;
+    for (int x = 0; x < n; ++x) for (int y = 0; y < n; ++y) dmax = std::max(dmax, std::abs(c.mval[nc + x] - c.mval[nc + y]));
+    for (int d = -dmax; d <= dmax && n > 0; ++d) {
+      std::vector<std::pair<int, int>> rr, cc;
+      for (int ia = 0; ia < n; ++ia)
+        for (int ja = 0; ja <= ia; ++ja)
+          if (c.mval[nc + ia] - c.mval[nc + ja] == d) rr.push_back({ia, ja});
+      for (int ka = 0; ka < n; ++ka)
+        for (int la = 0; la < n; ++la)
+          if (c.mval[nc + la] - c.mval[nc + ka] == d) cc.push_back({ka, la});
+      if (rr.empty() || cc.empty()) continue;
+      const int ent0 = (int)dst2.size(), ncl = (int)cc.size();
+      const int arow0 = (int)a_pair.size(), brow0 = (int)b_pair.size();
+      for (size_t r = 0; r < rr.size(); ++r) {
+        int p = -1;
+        for (int q = 0; q < c.npair; ++q) if (c.pa[q] == nc + rr[r].first && c.pb[q] == nc + rr[r].second) p = q;
+        a_pair.push_back(p); a_ent.push_back(ent0 + (int)r * ncl);
+        for (int y = 0; y < ncl; ++y) dst2.push_back(make_int4(rr[r].first, rr[r].second, cc[y].first, cc[y].second));
+      }
+      while ((a_pair.size() - arow0) % 8) { a_pair.push_back(-1); a_ent.push_back(-1); }
+      for (int y = 0; y < ncl; ++y) {
+        const int kf = nc + cc[y].first, lf = nc + cc[y].second;
+        int p = -1, cj = 0;
+        for (int q = 0; q < c.npair; ++q) {
+          if (c.pa[q] == kf && c.pb[q] == lf) { p = q; cj = 0; }
+          if (c.pa[q] == lf && c.pb[q] == kf) { p = q; cj = 1; }
+        }
+        b_pair.push_back(make_int2(p, cj)); b_col.push_back(y);
+      }
+      while ((b_pair.size() - brow0) % 8) { b_pair.push_back(make_int2(-1, 0)); b_col.push_back(-1); }
+      const int mtiles = ((int)a_pair.size() - arow0) / 8, ntiles = ((int)b_pair.size() - brow0) / 8;
+      for (int mt = 0; mt < mtiles; ++mt)
+        for (int nt = 0; nt < ntiles; nt += I2D_NTMAX)
+          groups.push_back(I2dGroup{arow0 + 8 * mt, brow0 + 8 * nt, std::min(I2D_NTMAX, ntiles - nt), 0});
+    }
+    if (dst2.size() != dst.size()) return ST_CONFIG;
+    // warp slots: sets of I2D_NW warps x I2D_MAXG groups; within a set the
+    // largest groups go first to the scheduler (warp % 4) with the least work
+    std::vector<int> order(groups.size());
+    for (size_t g = 0; g < order.size(); ++g) order[g] = (int)g;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return groups[x].nnt > groups[y].nnt; });
+    const int slots = I2D_NW * I2D_MAXG;
+    const int nsets = std::max(1, ((int)groups.size() + slots - 1) / slots);
+    std::vector<int> wgrp((size_t)nsets * slots, -1);
+    for (int set = 0; set < nsets; ++set) {
+      int load[4] = {0, 0, 0, 0}, used[I2D_NW] = {0};
+      for (int k = set * slots; k < std::min((int)order.size(), (set + 1) * slots); ++k) {
+        const int g = order[k];
+        int best = -1;
+        for (int w = 0; w < I2D_NW; ++w)
+          if (used[w] < I2D_MAXG && (best < 0 || load[w % 4] < load[best % 4])) best = w;
+        wgrp[((size_t)set * I2D_NW + best) * I2D_MAXG + used[best]++] = g;
+        load[best % 4] += groups[g].nnt;
+      }
+    }
+    I2dArgs& d2 = c.i2d;
+    d2.nra = (int)a_pair.size(); d2.nrb = (int)b_pair.size(); d2.ngroups = (int)groups.size(); d2.nblkent = (int)dst2.size();
+    d2.K = c.nbas2; d2.rho2 = c.rho2; d2.v2sph = c.v2sph; d2.nsets = nsets;
+    d2.a_pair = dupload(a_pair); d2.a_ent = dupload(a_ent); d2.b_pair = dupload(b_pair); d2.b_col = dupload(b_col);
+    d2.groups = dupload(groups); d2.warp_group = dupload(wgrp);
+    c.i2_dmma = n > 0 && int2e_dmma_fits(d2);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (c.i2_dmma) {
+      // the DMMA plan's entries replace the block list's (same count, its own order)
+      c.i2_nsplit = nsm;
+      c.i2.ent_dst = dupload(dst2);
+    }
+    c.i2.partial = dalloc<cplx>((size_t)c.i2_nsplit * std::max(1, c.i2.nblkent));
+    d2.partial = reinterpret_cast<double*>(c.i2.partial);
+  }
   // act2 dense blocks: rows ij (i >= j, m_i - m_j = d) in the reference's
   // (i outer, j inner) order, columns kl (m_l - m_k = d) in (k outer, l inner)
   // order, rows chunked by 24
@@ -831,6 +916,14 @@ int build_reductions(Ctx& c) {
     c.a2_blk = dupload(blks); c.a2_rows = dupload(rws); c.a2_cols = dupload(cls); c.a2_map = dupload(map);
     c.a2_coef = dalloc<cplx>(std::max(1, coff));
   }
+  // mean-field action arguments (fixed buffers; the tensor maps bind W and orbg)
+  MfprodArgs& mf = c.mf;
+  mf.ngrid = c.ngrid; mf.nfun = c.nfun; mf.npair = c.npair; mf.W = c.W; mf.orbg = c.orbg; mf.gorbg = c.gorbg;
+  mf.v2orbg = c.v2orbg; mf.nact = c.nact; mf.ncore = c.ncore;
+  mf.nblk = c.a2_nblk; mf.nrow = c.a2_nrow; mf.ncol = c.a2_ncol; mf.ncoef = c.a2_ncoef; mf.blk = c.a2_blk;
+  mf.rows = c.a2_rows; mf.cols = c.a2_cols; mf.coef_map = c.a2_map; mf.coef = c.a2_coef;
+  mf.nfcore = c.nfcore; mf.den1 = c.den1; mf.den2 = c.den2; mf.rden = c.rden; mf.mval = c.d_mval;
+  mf.pair_of = c.pair_of; mf.pair_cj = c.pair_cj; mf.nelact = c.nelact;
   return 0;
 }
 
@@ -1005,14 +1098,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     mark();  // end poisson
     rc |= chk("W gemm", gemm(c, c.b_W, c.npair, c.nlat, c.L2, false));
     mark();  // end w_gemm
-    MfprodArgs mf{};
-    mf.ngrid = c.ngrid; mf.nfun = c.nfun; mf.npair = c.npair; mf.W = c.W; mf.orbg = c.orbg; mf.gorbg = c.gorbg;
-    mf.v2orbg = c.v2orbg; mf.nact = c.nact; mf.ncore = c.ncore;
-    mf.nblk = c.a2_nblk; mf.nrow = c.a2_nrow; mf.ncol = c.a2_ncol; mf.ncoef = c.a2_ncoef; mf.blk = c.a2_blk;
-    mf.rows = c.a2_rows; mf.cols = c.a2_cols; mf.coef_map = c.a2_map; mf.coef = c.a2_coef;
-    mf.nfcore = c.nfcore; mf.den1 = c.den1; mf.den2 = c.den2; mf.rden = c.rden; mf.mval = c.d_mval;
-    mf.pair_of = c.pair_of; mf.pair_cj = c.pair_cj; mf.nelact = c.nelact;
-    rc |= chk("mfprod", launch_mfprod(mf, st));
+    rc |= chk("mfprod", launch_mfprod(c.mf, st));
     c.launches += 2;
     mark();  // end mfprod
     rc |= chk("gorb gemm", gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false));
@@ -1024,7 +1110,11 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   rc |= chk("orbdots", launch_orbdots(c.od, st));
   c.launches += 2;
   mark();  // end orbdots
-  if (c.nact > 0) { rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st)); c.launches += 3; }
+  if (c.nact > 0) {
+    if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
+    else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
+    c.launches += 3;
+  }
   mark();  // end int2e
   SmallArgs sa{};
   sa.nfun = c.nfun; sa.nfcore = c.nfcore; sa.ndcore = c.ndcore; sa.nact = c.nact; sa.ncore = c.ncore; sa.nelact = c.nelact;

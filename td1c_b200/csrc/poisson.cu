@@ -25,12 +25,11 @@
 // block (clipped at Nr).  y is parked in the v2sph buffer between the
 // sweeps.  Every mbarrier wait is bounded; a wait that runs out sets
 // ST_TIMEOUT in the status word and the warp drains and returns.
-#include <cudaTypedefs.h>
-
 #include <algorithm>
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace td1c {
 
@@ -38,60 +37,6 @@ namespace {
 
 constexpr int PS_PAIRS = 16;      // pairs per warp
 constexpr int PS_STAGES = 4;      // depth of the load ring
-constexpr unsigned long long PS_WAIT_NS = 1000000000ull;  // bound of one mbarrier wait: 1 s
-
-__device__ __forceinline__ unsigned su32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(su32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// bounded wait; false when PS_WAIT_NS ran out
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer_ns();
-  while (globaltimer_ns() - t0 < PS_WAIT_NS)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(su32(dst)),
-               "l"(src), "r"(bytes), "r"(su32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void tensor_load(void* dst, const CUtensorMap* tm, int x, int y, int z, unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
-          su32(dst)),
-      "l"(tm), "r"(x), "r"(y), "r"(z), "r"(su32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tensor_store(const CUtensorMap* tm, int x, int y, int z, const void* src) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm), "r"(x),
-               "r"(y), "r"(z), "r"(su32(src))
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
 // byte offset of the staged-block ring: 128 bytes of mbarriers, the table
 // stages, rounded up to the 128-byte alignment of a TMA box
@@ -158,7 +103,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
 
   if (lane == 0) {
     for (int s = 0; s < PS_STAGES; ++s) mbar_init(&bar[s], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_mbar_init();
   }
   __syncwarp();
 
@@ -170,7 +115,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
       const int s = q % PS_STAGES;
       mbar_expect_tx(&bar[s], tx_bytes);
       bulk_load(fbuf + (size_t)s * ND * W, (fwd ? tabf_l : tabb_l) + (size_t)b * ND * W, ND * W * 8, &bar[s]);
-      tensor_load(rbuf + (size_t)s * PS_PAIRS * BOX, fwd ? &a.tm_rho : &a.tm_v2, 2 * b * ND, l, p0, &bar[s]);
+      tensor_load_3d(rbuf + (size_t)s * PS_PAIRS * BOX, fwd ? &a.tm_rho : &a.tm_v2, 2 * b * ND, l, p0, &bar[s]);
     }
   };
   // store ybuf half h to the rows of block b (rows past Nr and pairs past
@@ -179,7 +124,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
     fence_async_smem();
     __syncwarp();
     if (lane == 0) {
-      tensor_store(&a.tm_v2, 2 * b * ND, l, p0, ybuf + (size_t)h * PS_PAIRS * BOX);
+      tensor_store_3d(&a.tm_v2, 2 * b * ND, l, p0, ybuf + (size_t)h * PS_PAIRS * BOX);
       bulk_commit();
     }
   };
@@ -317,35 +262,14 @@ static int launch_nd(const PoissonArgs& a, cudaStream_t st) {
 // 3-d views [npair][L2][2 Nr] of rho2 and v2sph with a box of one block of
 // nd complex rows x one l x up to 16 pairs
 int poisson_encode_maps(PoissonArgs& a) {
-  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  if (!encode) {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn) {
-      fprintf(stderr, "td1c_b200: cuTensorMapEncodeTiled is not available\n");
-      return (int)cudaErrorNotSupported;
-    }
-    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  }
   if (a.npair <= 0) { a.boxp = 0; return 0; }
   a.boxp = std::min(PS_PAIRS, a.npair);
   const cuuint64_t dims[3] = {(cuuint64_t)2 * a.Nr, (cuuint64_t)a.L2, (cuuint64_t)a.npair};
   const cuuint64_t strides[2] = {(cuuint64_t)a.Nr * 16, (cuuint64_t)a.L2 * a.Nr * 16};
   const cuuint32_t box[3] = {(cuuint32_t)(2 * a.nd), 1u, (cuuint32_t)a.boxp};
-  const cuuint32_t estr[3] = {1u, 1u, 1u};
-  CUtensorMap* maps[2] = {&a.tm_rho, &a.tm_v2};
-  const void* bases[2] = {a.rho2, a.v2sph};
-  for (int i = 0; i < 2; ++i) {
-    CUresult r = encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(bases[i]), dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-      fprintf(stderr, "td1c_b200: cuTensorMapEncodeTiled (Poisson %s) failed: %d\n", i ? "v2sph" : "rho2", (int)r);
-      return (int)cudaErrorInvalidValue;
-    }
-  }
-  return 0;
+  int rc = encode_f64_map(&a.tm_rho, a.rho2, 3, dims, strides, box, "Poisson rho2");
+  if (!rc) rc = encode_f64_map(&a.tm_v2, a.v2sph, 3, dims, strides, box, "Poisson v2sph");
+  return rc;
 }
 
 int launch_poisson_tables(const PoissonArgs& a, double* tabf, double* tabb, cudaStream_t st) {

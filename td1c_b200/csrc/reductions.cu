@@ -191,11 +191,15 @@ __global__ void __launch_bounds__(I2_NT) int2e_block_kernel(Int2eArgs a) {
   }
 }
 
+// one warp per entry: lane l adds splits l, l + 32, ... in order, then a
+// fixed xor tree combines the lanes (deterministic)
 __global__ void int2e_sum_kernel(Int2eArgs a, int nsplit) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (t >= a.nblkent) return;
   cplx s = mkc(0, 0);
-  for (int c = 0; c < nsplit; ++c) s = cadd(s, a.partial[(size_t)c * a.nblkent + t]);
+  for (int c = lane; c < nsplit; c += 32) s = cadd(s, a.partial[(size_t)c * a.nblkent + t]);
+  for (int o = 16; o > 0; o >>= 1) { s.x += __shfl_xor_sync(0xffffffffu, s.x, o); s.y += __shfl_xor_sync(0xffffffffu, s.y, o); }
+  if (lane) return;
   int4 d = a.ent_dst[t];  // (i, j, k, l) active indices
   const int n = a.nact;
   a.int2e[d.x + n * (d.y + n * (d.z + n * d.w))] = s;
@@ -207,6 +211,14 @@ __global__ void int2e_fill_kernel(Int2eArgs a) {
   if (t >= n * n * n * n) return;
   int i = t % n, j = (t / n) % n, k = (t / (n * n)) % n, l = t / (n * n * n);
   if (i < j) a.int2e[t] = cconj(a.int2e[j + n * (i + n * (l + n * k))]);
+}
+
+// fixed-order sum of nsplit partial blocks into int2e, then the i < j half
+int launch_int2e_sum_fill(const Int2eArgs& a, int nsplit, cudaStream_t st) {
+  const int n = a.nact, n4 = n * n * n * n;
+  if (a.nblkent > 0) int2e_sum_kernel<<<(a.nblkent + 7) / 8, 256, 0, st>>>(a, nsplit);
+  int2e_fill_kernel<<<(n4 + 127) / 128, 128, 0, st>>>(a);
+  return (int)cudaGetLastError();
 }
 
 int launch_int2e(const Int2eArgs& a, int nsplit, cudaStream_t st) {
@@ -222,7 +234,7 @@ int launch_int2e(const Int2eArgs& a, int nsplit, cudaStream_t st) {
       fprintf(stderr, "td1c_b200: int2e block kernel (grid %d x %d): %s\n", nsplit, a.nblocks, cudaGetErrorString(e));
       return (int)e;
     }
-    int2e_sum_kernel<<<(a.nblkent + 127) / 128, 128, 0, st>>>(a, nsplit);
+    int2e_sum_kernel<<<(a.nblkent + 7) / 8, 256, 0, st>>>(a, nsplit);
     e = cudaGetLastError();
     if (e != cudaSuccess) { fprintf(stderr, "td1c_b200: int2e sum: %s\n", cudaGetErrorString(e)); return (int)e; }
   }

@@ -28,4 +28,29 @@ struct Int2eArgs {
 };
 int launch_int2e(const Int2eArgs& a, int nsplit, cudaStream_t st);
 
+// int2e on the FP64 tensor cores (DMMA m8n8k4), split over K.  Every
+// Delta-m block is padded to m-tiles of 8 row pairs (rho2) and n-tiles of 8
+// columns (v2sph); a group is one m-tile x up to I2D_NTMAX n-tiles, and the
+// host assigns at most I2D_MAXG groups to each warp (-1: none).
+constexpr int I2D_NW = 16, I2D_MAXG = 1, I2D_NTMAX = 3;
+struct I2dGroup { int arow0, brow0, nnt, pad; };  // 8 A rows x nnt n-tiles (8 B rows each)
+struct I2dArgs {
+  int nra, nrb, ngroups, nblkent;
+  size_t K;
+  const int* a_pair;     // [nra] stored pair of the padded A row (-1: padding)
+  const int* a_ent;      // [nra] first entry of the row (ent0 + r ncol), -1 for padding
+  const int2* b_pair;    // [nrb] (stored pair, conj) of the padded B row ((-1, 0): padding)
+  const int* b_col;      // [nrb] column index inside its block, -1 for padding
+  const I2dGroup* groups;
+  const int* warp_group;  // [nsets][I2D_NW][I2D_MAXG] group of each warp slot, -1: none
+  int nsets;
+  const cplx* rho2;
+  const cplx* v2sph;
+  double* partial;       // [nsplit][nblkent][2]
+};
+int launch_int2e_sum_fill(const Int2eArgs& a, int nsplit, cudaStream_t st);
+size_t int2e_dmma_smem(const I2dArgs& a);
+bool int2e_dmma_fits(const I2dArgs& a);
+int launch_int2e_dmma(const I2dArgs& d, const Int2eArgs& sum, int nsplit, cudaStream_t st);
+
 }  // namespace td1c
