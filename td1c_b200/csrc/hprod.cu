@@ -915,6 +915,70 @@ int build_reductions(Ctx& c) {
     c.a2_nblk = (int)blks.size(); c.a2_nrow = (int)rws.size(); c.a2_ncol = (int)cls.size(); c.a2_ncoef = coff;
     c.a2_blk = dupload(blks); c.a2_rows = dupload(rws); c.a2_cols = dupload(cls); c.a2_map = dupload(map);
     c.a2_coef = dalloc<cplx>(std::max(1, coff));
+    // the tensor-core form: per Delta one block (rows not chunked) over the
+    // same rows list; coefficients C[row][kl] at coff + row pa + kl with pa
+    // = 4 mod 8 (double2) and zero padding; padded columns read the zero W row
+    std::vector<MfdBlock> dblk;
+    std::vector<int2> dcol;
+    std::vector<Act2Coef> dmap;
+    int dcoff = 0;
+    for (size_t b0 = 0; b0 < blks.size();) {
+      size_t b1 = b0;  // the row chunks of one Delta share col0
+      int nr = 0;
+      while (b1 < blks.size() && blks[b1].col0 == blks[b0].col0) nr += blks[b1++].nrow;
+      const Act2Block& B = blks[b0];
+      MfdBlock db{};
+      db.kpad = (B.ncol + 3) / 4 * 4;
+      db.pa = db.kpad % 8 == 0 ? db.kpad + 4 : db.kpad;
+      db.mt = (nr + 7) / 8; db.col0 = (int)dcol.size(); db.drow0 = B.row0; db.nr = nr; db.coff = dcoff;
+      for (int y = 0; y < db.kpad; ++y) dcol.push_back(y < B.ncol ? cls[B.col0 + y] : make_int2(c.npair, 0));
+      for (size_t bb = b0; bb < b1; ++bb)
+        for (int y = 0; y < blks[bb].ncol; ++y)
+          for (int x = 0; x < blks[bb].nrow; ++x) {
+            // the chunk's map entry (y, x) sits at coff + y nrow + x, like its slot
+            Act2Coef m{};
+            m.d2idx = map[blks[bb].coff + y * blks[bb].nrow + x].d2idx;
+            m.dst = dcoff + (blks[bb].row0 + x - B.row0) * db.pa + y;
+            dmap.push_back(m);
+          }
+      dcoff += db.mt * 8 * db.pa;
+      dblk.push_back(db);
+      b0 = b1;
+    }
+    // per target x the D2V rows in row order: (row, other orbital), conj flag in bit 16
+    std::vector<int2> elist;
+    std::vector<int> eoff(n + 1, 0);
+    for (int x = 0; x < n; ++x) {
+      eoff[x] = (int)elist.size();
+      for (size_t r = 0; r < rws.size(); ++r) {
+        if (rws[r].x == x) elist.push_back(make_int2((int)r, rws[r].y));
+        else if (rws[r].y == x && rws[r].x > rws[r].y) elist.push_back(make_int2((int)r, rws[r].x | (1 << 16)));
+      }
+    }
+    eoff[n] = (int)elist.size();
+    // (block, m-tile) items over the 4 warps of a CTA, longest first to the
+    // least loaded warp; at most 8 per warp
+    std::vector<std::pair<int, int2>> items;
+    for (size_t b = 0; b < dblk.size(); ++b)
+      for (int mt = 0; mt < dblk[b].mt; ++mt) items.push_back({dblk[b].kpad / 4, make_int2((int)b, mt)});
+    std::stable_sort(items.begin(), items.end(), [](const std::pair<int, int2>& x, const std::pair<int, int2>& y) { return x.first > y.first; });
+    int wload[4] = {0, 0, 0, 0}, wcount[4] = {0, 0, 0, 0};
+    bool items_fit = items.size() <= 32;
+    for (int w = 0; w < 4; ++w)
+      for (int k = 0; k < 8; ++k) c.mf.witem[w][k] = make_int2(-1, -1);
+    for (size_t k = 0; k < items.size() && items_fit; ++k) {
+      int best = -1;
+      for (int w = 0; w < 4; ++w)
+        if (wcount[w] < 8 && (best < 0 || wload[w] < wload[best])) best = w;
+      c.mf.witem[best][wcount[best]++] = items[k].second;
+      wload[best] += items[k].first;
+    }
+    c.mf.dmma = n > 0 && !dblk.empty() && items_fit;
+    c.mf.nblk_d = (int)dblk.size(); c.mf.ndcol = (int)dcol.size(); c.mf.ncoef_d = dcoff; c.mf.nelist = (int)elist.size();
+    c.mf.dblk = dupload(dblk); c.mf.dcol = dupload(dcol); c.mf.dmap = dupload(dmap); c.mf.elist = dupload(elist);
+    c.mf.eoff = dupload(eoff);
+    c.mf.dcoef = dalloc<cplx>(std::max(1, dcoff));
+    cudaMemset(c.mf.dcoef, 0, sizeof(cplx) * std::max(1, dcoff));
   }
   // mean-field action arguments (fixed buffers; the tensor maps bind W and orbg)
   MfprodArgs& mf = c.mf;

@@ -6,7 +6,8 @@
 // m_i - m_j the rows ij and the columns kl form a dense complex product
 // C = A B^T, computed with four real products per complex depth step:
 //   Re C += Re A Re B + Im A (-Im B),   Im C += Re A Im B + Im A Re B
-// on mma.sync.m8n8k4.f64 tiles of 8 rows x 8 columns x 4 complex depths.
+// on mma.sync.m8n8k4.f64 tiles of 8 rows x 8 columns x 4 complex depths,
+// each of the four products in its own accumulator (independent chains).
 // Lane (g, t) of a fragment handles depth x = 4 s + t, so one 128-bit
 // shared-memory load gives it both parts of its A (row g) or B (column g)
 // element; a conjugated column flips the sign of Im B in the same lane.
@@ -104,7 +105,9 @@ __global__ void __launch_bounds__(I2D_NW * 32, 1) int2e_dmma_kernel(I2dArgs a) {
   // this warp's groups with the lane's fragment offsets (in double2 units)
   int nnt[I2D_MAXG], aoff[I2D_MAXG], boff[I2D_MAXG][I2D_NTMAX];
   unsigned bcj[I2D_MAXG];  // bit t: n-tile t of the lane's column is conjugated
-  double acc[I2D_MAXG][I2D_NTMAX][2][2];  // [g][t][re|im][c0|c1]
+  // [g][t][chain][c0|c1]: Re A Re B, Im A (-Im B), Re A Im B, Im A Re B as
+  // four independent accumulator chains, added at the end
+  double acc[I2D_MAXG][I2D_NTMAX][4][2];
   const int* wg = a.warp_group + ((size_t)blockIdx.y * I2D_NW + warp) * I2D_MAXG;
 #pragma unroll
   for (int g = 0; g < I2D_MAXG; ++g) {
@@ -118,7 +121,8 @@ __global__ void __launch_bounds__(I2D_NW * 32, 1) int2e_dmma_kernel(I2dArgs a) {
       const int brow = G.brow0 + 8 * t + gid;
       boff[g][t] = (a.nra + brow) * (I2D_PITCH / 2) + tig;
       if (t < G.nnt && a.b_pair[brow].y) bcj[g] |= 1u << t;
-      acc[g][t][0][0] = acc[g][t][0][1] = acc[g][t][1][0] = acc[g][t][1][1] = 0.0;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) acc[g][t][h][0] = acc[g][t][h][1] = 0.0;
     }
   }
 
@@ -142,9 +146,9 @@ __global__ void __launch_bounds__(I2D_NW * 32, 1) int2e_dmma_kernel(I2dArgs a) {
             const double2 bv = sm[boff[g][t] + 4 * s];
             const double bi = ((bcj[g] >> t) & 1) ? -bv.y : bv.y;
             dmma_8x8x4(acc[g][t][0][0], acc[g][t][0][1], av.x, bv.x);
-            dmma_8x8x4(acc[g][t][0][0], acc[g][t][0][1], av.y, -bi);
-            dmma_8x8x4(acc[g][t][1][0], acc[g][t][1][1], av.x, bi);
-            dmma_8x8x4(acc[g][t][1][0], acc[g][t][1][1], av.y, bv.x);
+            dmma_8x8x4(acc[g][t][1][0], acc[g][t][1][1], av.y, -bi);
+            dmma_8x8x4(acc[g][t][2][0], acc[g][t][2][1], av.x, bi);
+            dmma_8x8x4(acc[g][t][3][0], acc[g][t][3][1], av.y, bv.x);
           }
         }
       }
@@ -164,7 +168,8 @@ __global__ void __launch_bounds__(I2D_NW * 32, 1) int2e_dmma_kernel(I2dArgs a) {
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int bc = a.b_col[G.brow0 + 8 * t + 2 * tig + i];
-        if (ae >= 0 && bc >= 0) out[ae + bc] = make_double2(acc[g][t][0][i], acc[g][t][1][i]);
+        if (ae >= 0 && bc >= 0)
+          out[ae + bc] = make_double2(acc[g][t][0][i] + acc[g][t][1][i], acc[g][t][2][i] + acc[g][t][3][i]);
       }
     }
   }

@@ -77,6 +77,12 @@ struct Act2Block {     // one dense (ij) x (kl) block of the 2-RDM contraction
   int coff, pad0, pad1, pad2;  // coefficient offset, coef[coff + kl * nrow + ij]
 };
 struct Act2Coef { int d2idx, dst; };  // den2 element -> coefficient slot
+// one Delta-m block of the act2 contraction on the FP64 tensor cores:
+// coefficients C[row][kl] padded to mt m-tiles of 8 rows x kpad (multiple of
+// 4) columns, row pitch pa (double2, 4 mod 8) from coff; columns
+// dcol[col0 .. col0+kpad) (padding: the zero W row npair); D2V rows
+// drow0 .. drow0+nr
+struct MfdBlock { int coff, pa, mt, kpad, col0, drow0, nr, pad; };
 struct MfprodArgs {
   size_t ngrid;
   int nfun, npair;
@@ -99,6 +105,16 @@ struct MfprodArgs {
   const int2* cols;
   const Act2Coef* coef_map;
   cplx* coef;
+  // tensor-core form of act2 (used when dmma != 0): its own padded
+  // coefficient layout and map, per-target epilogue lists
+  int dmma, nblk_d, ndcol, ncoef_d, nelist;
+  const MfdBlock* dblk;
+  const int2* dcol;       // (pair, conj) of every padded column
+  const Act2Coef* dmap;   // den2 element -> padded coefficient slot
+  cplx* dcoef;            // [ncoef_d]
+  const int2* elist;      // per active target x: (D2V row, other orbital | conj << 16), in row order
+  const int* eoff;        // [nact + 1] offsets into elist
+  int2 witem[4][8];       // per warp: (block, m-tile) items, -1 ends the list
 };
 int launch_mfprod(const MfprodArgs& a, cudaStream_t st);
 

@@ -18,10 +18,14 @@
 // reads every W(k,l) once; the coefficients (den2, thresholded) are broadcast
 // from shared memory; twfn and the orbitals of the CTA's points live in
 // shared memory.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace td1c {
+
+static int launch_mfprod_scalar(const MfprodArgs& a, cudaStream_t st);
 
 constexpr int MF_MAXF = 16;
 constexpr int MF_NIJ = 24;   // rows of one act2 block chunk
@@ -161,7 +165,236 @@ __global__ void __launch_bounds__(MF_TQ) mfprod_kernel(MfprodArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// act2 on the FP64 tensor cores.  Persistent CTAs of 4 warps (2 per SM)
+// load the padded coefficients and the plan tables once, then loop over
+// tiles of MFD_TQ grid points:
+//   1. cp.async stages the tile's slice of every stored pair's W (rows of
+//      MFD_TQ points, pitch MFD_WP) and the orbitals in shared memory; row
+//      npair of the W slice is zero.
+//   2. core terms (fcx1, dcj, dcx into gorbg; actj, actx into v2orbg of the
+//      dynamic cores) over (point, orbital) items.
+//   3. D2V[ij][pt] = sum_kl C[ij][kl] W(kl)[pt] per block as
+//      mma.sync.m8n8k4.f64 tiles (rows ij, columns points, depth kl) with
+//      four real products per complex step, stored to shared memory.
+//   4. twfn_x[pt] from the target's D2V rows (in row order, as the
+//      reference's loop), then v2orbg_k = sum_x rden(x, k) twfn_x.
+// ---------------------------------------------------------------------------
+constexpr int MFD_TQ = 32;              // points per CTA (4 n-tiles)
+constexpr int MFD_WP = MFD_TQ + 2;      // double2 pitch of a W row: rows 8 banks apart
+constexpr int MFD_NT = 128;             // threads
+constexpr int MFD_MAXB = 16, MFD_MAXCOL = 256, MFD_MAXROW = 128, MFD_MAXE = 512;
+
+__device__ __forceinline__ void mfd_dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+__device__ __forceinline__ void mfd_cp16(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src),
+               "r"(bytes)
+               : "memory");
+}
+
+static size_t mfd_smem_bytes(const MfprodArgs& a) {
+  return sizeof(cplx) * ((size_t)(a.npair + 1) * MFD_WP + (size_t)a.ncoef_d + (size_t)a.nfun * MFD_TQ +
+                         (size_t)a.nrow * MFD_TQ + (size_t)a.nact * MFD_TQ);
+}
+static bool mfd_fits(const MfprodArgs& a) {
+  return a.dmma && a.nfun <= MF_MAXF && a.nblk_d <= MFD_MAXB && a.ndcol <= MFD_MAXCOL && a.nrow <= MFD_MAXROW &&
+         a.nelist <= MFD_MAXE && mfd_smem_bytes(a) <= 200 * 1024;
+}
+
+__global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
+  extern __shared__ __align__(16) cplx mfd_smem[];
+  const int nact = a.nact, ncore = a.ncore, nfcore = a.nfcore, nfun = a.nfun, npair = a.npair;
+  cplx* sW = mfd_smem;                                   // [npair + 1][WP]
+  cplx* sC = sW + (size_t)(npair + 1) * MFD_WP;          // [ncoef_d]
+  cplx* sPhi = sC + a.ncoef_d;                           // [nfun][TQ]
+  cplx* sD = sPhi + (size_t)nfun * MFD_TQ;               // [nrow][TQ]
+  cplx* sTw = sD + (size_t)a.nrow * MFD_TQ;              // [nact][TQ]
+  __shared__ MfdBlock sblk[MFD_MAXB];
+  __shared__ int2 scol[MFD_MAXCOL];
+  __shared__ int2 sel[MFD_MAXE];
+  __shared__ int seoff[MF_MAXF + 1];
+  __shared__ cplx srden[MF_MAXF * MF_MAXF], sden1[MF_MAXF * MF_MAXF];
+  __shared__ int spo[MF_MAXF * MF_MAXF], spc[MF_MAXF * MF_MAXF], smv[MF_MAXF];
+  const int tid = threadIdx.x;
+  const size_t ng = a.ngrid;
+  const bool do_act2 = a.nelact >= 2 && nact > 0 && a.nblk_d > 0;
+  const int ntile = (int)((ng + MFD_TQ - 1) / MFD_TQ);
+
+  // ---- once per CTA: coefficients and tables
+  if (do_act2)
+    for (int e = tid; e < a.ncoef_d; e += MFD_NT) mfd_cp16(sC + e, a.dcoef + e, 16u);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (int e = tid; e < MFD_WP; e += MFD_NT) sW[(size_t)npair * MFD_WP + e] = mkc(0, 0);
+  for (int e = tid; e < a.nblk_d; e += MFD_NT) sblk[e] = a.dblk[e];
+  for (int e = tid; e < a.ndcol; e += MFD_NT) scol[e] = a.dcol[e];
+  for (int e = tid; e < a.nelist; e += MFD_NT) sel[e] = a.elist[e];
+  for (int e = tid; e <= nact; e += MFD_NT) seoff[e] = a.eoff[e];
+  for (int e = tid; e < nact * nact; e += MFD_NT) { srden[e] = a.rden[e]; sden1[e] = a.den1[e]; }
+  for (int e = tid; e < nfun * nfun; e += MFD_NT) { spo[e] = a.pair_of[e]; spc[e] = a.pair_cj[e]; }
+  for (int e = tid; e < nfun; e += MFD_NT) smv[e] = a.mval[e];
+
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+  const size_t q0 = (size_t)tile * MFD_TQ;
+  __syncthreads();  // the previous tile's reads of sW, sPhi, sD, sTw are done
+  // ---- 1. this tile's W rows and orbitals
+  for (int e = tid; e < npair * MFD_TQ; e += MFD_NT) {
+    const int p = e / MFD_TQ, t = e % MFD_TQ;
+    const bool in = q0 + t < ng;
+    mfd_cp16(sW + (size_t)p * MFD_WP + t, a.W + (size_t)p * ng + (in ? q0 + t : 0), in ? 16u : 0u);
+  }
+  for (int e = tid; e < nfun * MFD_TQ; e += MFD_NT) {
+    const int f = e / MFD_TQ, t = e % MFD_TQ;
+    const bool in = q0 + t < ng;
+    mfd_cp16(sPhi + e, a.orbg + (size_t)f * ng + (in ? q0 + t : 0), in ? 16u : 0u);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+
+  auto PHI = [&](int f, int t) { return sPhi[(size_t)f * MFD_TQ + t]; };
+  auto WXY = [&](int x, int y, int t) {  // W(x, y) at point t from the stored pair
+    const int e = x * nfun + y;
+    const cplx w = sW[(size_t)spo[e] * MFD_WP + t];
+    return spc[e] ? cconj(w) : w;
+  };
+  const int ndcore = ncore - nfcore;
+  // ---- 2. core terms (same sums and order as mfprod_kernel)
+  for (int e = tid; e < (nfun - nfcore) * MFD_TQ; e += MFD_NT) {
+    const int i = nfcore + e / MFD_TQ, t = e % MFD_TQ;
+    if (q0 + t >= ng) continue;
+    cplx g = mkc(0, 0);
+    for (int j = 0; j < nfcore; ++j) g = csub(g, cmul(WXY(j, i, t), PHI(j, t)));  // fcx1
+    if (ndcore > 0) {
+      cplx dcsum = mkc(0.0, 0.0);
+      for (int j = nfcore; j < ncore; ++j) { cplx w = WXY(j, j, t); dcsum.x += w.x * 2.0; dcsum.y += w.y * 2.0; }
+      g = cadd(g, cmul(dcsum, PHI(i, t)));                                        // dcj
+      for (int j = nfcore; j < ncore; ++j) g = csub(g, cmul(WXY(j, i, t), PHI(j, t)));  // dcx
+    }
+    a.gorbg[(size_t)i * ng + q0 + t] = g;
+  }
+  for (int e = tid; e < ndcore * MFD_TQ; e += MFD_NT) {
+    const int i = nfcore + e / MFD_TQ, t = e % MFD_TQ;
+    if (q0 + t >= ng) continue;
+    cplx v = mkc(0, 0);
+    if (nact > 0) {
+      cplx d2v = mkc(0.0, 0.0);
+      for (int ja = 0; ja < nact; ++ja)
+        for (int ka = 0; ka < nact; ++ka) cfma(d2v, WXY(ncore + ja, ncore + ka, t), sden1[ka + nact * ja]);
+      v = cadd(v, cmul(d2v, PHI(i, t)));
+      for (int ja = 0; ja < nact; ++ja) {
+        const int jf = ncore + ja;
+        cplx wd1 = mkc(0.0, 0.0);
+        for (int ka = 0; ka < nact; ++ka) {
+          const int kf = ncore + ka;
+          if (smv[jf] != smv[kf]) continue;
+          wd1 = cadd(wd1, cmul(PHI(kf, t), cscale(sden1[ka + nact * ja], -0.5)));
+        }
+        v = cadd(v, cmul(wd1, WXY(jf, i, t)));
+      }
+    }
+    a.v2orbg[(size_t)i * ng + q0 + t] = v;
+  }
+  if (!do_act2) {
+    for (int e = tid; e < nact * MFD_TQ; e += MFD_NT) {
+      const int t = e % MFD_TQ;
+      if (q0 + t < ng) a.v2orbg[(size_t)(ncore + e / MFD_TQ) * ng + q0 + t] = mkc(0, 0);
+    }
+    continue;
+  }
+  // ---- 3. D2V tiles on the tensor cores: each warp runs its (block,
+  //      m-tile) items over all MFD_TQ / 8 n-tiles at once, the four real
+  //      products of each tile in separate accumulators
+  const int lane = tid & 31, warp = tid >> 5, gid = lane >> 2, tig = lane & 3;
+  constexpr int NT = MFD_TQ / 8;
+  for (int it = 0; it < 8; ++it) {
+    const int2 wi = a.witem[warp][it];
+    if (wi.x < 0) break;
+    const MfdBlock B = sblk[wi.x];
+    const int mt = wi.y;
+    double acc[NT][4][2];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) acc[t][h][0] = acc[t][h][1] = 0.0;
+    const cplx* arow = sC + B.coff + (size_t)(mt * 8 + gid) * B.pa + tig;
+    for (int ks = 0; ks < B.kpad / 4; ++ks) {
+      const cplx av = arow[4 * ks];
+      const int2 pc = scol[B.col0 + 4 * ks + tig];
+      const cplx* wrow = sW + (size_t)pc.x * MFD_WP + gid;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const cplx bv = wrow[8 * t];
+        const double bi = pc.y ? -bv.y : bv.y;
+        mfd_dmma(acc[t][0][0], acc[t][0][1], av.x, bv.x);
+        mfd_dmma(acc[t][1][0], acc[t][1][1], av.y, -bi);
+        mfd_dmma(acc[t][2][0], acc[t][2][1], av.x, bi);
+        mfd_dmma(acc[t][3][0], acc[t][3][1], av.y, bv.x);
+      }
+    }
+    const int r = mt * 8 + gid;
+    if (r < B.nr) {
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        cplx* drow = sD + (size_t)(B.drow0 + r) * MFD_TQ + t * 8 + 2 * tig;
+        drow[0] = mkc(acc[t][0][0] + acc[t][1][0], acc[t][2][0] + acc[t][3][0]);
+        drow[1] = mkc(acc[t][0][1] + acc[t][1][1], acc[t][2][1] + acc[t][3][1]);
+      }
+    }
+  }
+  __syncthreads();
+  // ---- 4. twfn, then v2orbg of the active orbitals
+  for (int e = tid; e < nact * MFD_TQ; e += MFD_NT) {
+    const int x = e / MFD_TQ, t = e % MFD_TQ;
+    cplx tw = mkc(0, 0);
+    for (int k = seoff[x]; k < seoff[x + 1]; ++k) {
+      const int2 en = sel[k];
+      const cplx d = sD[(size_t)en.x * MFD_TQ + t];
+      const cplx o = PHI(ncore + (en.y & 0xffff), t);
+      tw = cadd(tw, cmul(o, (en.y >> 16) ? cconj(d) : d));
+    }
+    sTw[(size_t)x * MFD_TQ + t] = tw;
+  }
+  __syncthreads();
+  for (int e = tid; e < nact * MFD_TQ; e += MFD_NT) {
+    const int ka = e / MFD_TQ, t = e % MFD_TQ;
+    if (q0 + t >= ng) continue;
+    const int kf = ncore + ka;
+    cplx v = mkc(0, 0);
+    for (int x = 0; x < nact; ++x)
+      if (smv[ncore + x] == smv[kf]) v = cadd(v, cmul(srden[x + nact * ka], sTw[(size_t)x * MFD_TQ + t]));
+    a.v2orbg[(size_t)kf * ng + q0 + t] = v;
+  }
+  }  // tile loop
+}
+
 int launch_mfprod(const MfprodArgs& a, cudaStream_t st) {
+  if (mfd_fits(a)) {
+    const bool do_act2 = a.nelact >= 2 && a.nact > 0 && a.nblk_d > 0;
+    if (do_act2) act2_fill_kernel<<<(a.ncoef + 127) / 128, 128, 0, st>>>(a.ncoef, a.dmap, a.den2, a.dcoef);
+    const size_t smem = mfd_smem_bytes(a);
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(mfprod_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr = true;
+    }
+    static int nsm = 0;
+    if (!nsm) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int ntile = (int)((a.ngrid + MFD_TQ - 1) / MFD_TQ);
+    mfprod_dmma_kernel<<<(unsigned)std::min(ntile, 2 * nsm), MFD_NT, smem, st>>>(a);  // persistent: 2 CTAs per SM
+    return (int)cudaGetLastError();
+  }
+  return launch_mfprod_scalar(a, st);
+}
+
+static int launch_mfprod_scalar(const MfprodArgs& a, cudaStream_t st) {
   if (a.nfun > MF_MAXF || a.nblk > 32 || a.nrow > 256 || a.ncol > 512) return (int)cudaErrorInvalidValue;
   const bool do_act2 = a.nelact >= 2 && a.nact > 0 && a.nblk > 0;
   if (do_act2) act2_fill_kernel<<<(a.ncoef + 127) / 128, 128, 0, st>>>(a.ncoef, a.coef_map, a.den2, a.coef);
