@@ -61,7 +61,7 @@ struct PoissonArgs {
   const double* tabb;    // [L2][Np][W] backward row tables
   int* status;           // device status word (ST_TIMEOUT on a stalled copy)
   int boxp;              // pairs per TMA box (min(16, npair)), set by poisson_encode_maps
-  CUtensorMap tm_rho;    // rho2 viewed as [npair][L2][2 Nr] float64, box (2 nd, 1, boxp)
+  CUtensorMap tm_rho;    // rho2 viewed as (re|im, pair, row, l) float64, box (2, boxp, nd, 1)
   CUtensorMap tm_v2;     // v2sph, same view
 };
 // doubles per row of the Poisson row tables: nd band values + 3, even

@@ -19,8 +19,10 @@
 // for the backward one), so a row costs a handful of 128-bit broadcast loads
 // from shared memory.  Blocks of nd rows move between HBM and shared memory
 // by the TMA: per block one bulk copy of the table rows and one tensor copy
-// of the 16 pairs' nd complex values (a 3-d box over [pair][l][2 Nr], rows
-// past Nr zero-filled) land in a 4-stage ring tracked by mbarriers, and the
+// of the 16 pairs' nd complex values (a 4-d box over (re|im, pair, row, l)
+// that lands as [row][pair][re|im], so every lane reads one contiguous line
+// per row; rows past Nr zero-filled) land in a 4-stage ring tracked by
+// mbarriers, and the
 // forward result y and the final v2sph leave through one tensor store per
 // block (clipped at Nr).  y is parked in the v2sph buffer between the
 // sweeps.  Every mbarrier wait is bounded; a wait that runs out sets
@@ -100,6 +102,11 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
   const double* tabb_l = a.tabb + (size_t)l * Np * W;
   // box bytes: rows past Nr and pairs past npair arrive zero-filled and count
   const unsigned tx_bytes = (unsigned)(ND * W * 8) + (unsigned)(BOX * a.boxp * 8);
+  // a staged block is [row][pair][re|im] (boxp pairs), so lane 2P+c reads
+  // row u at u * rstride + lane: one contiguous line per row
+  const int rstride = 2 * a.boxp;
+  const bool owner = P < a.boxp;  // lanes past the box must not write: their slots belong to the next row
+  if (!owner) active = false;
 
   if (lane == 0) {
     for (int s = 0; s < PS_STAGES; ++s) mbar_init(&bar[s], 1);
@@ -115,7 +122,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
       const int s = q % PS_STAGES;
       mbar_expect_tx(&bar[s], tx_bytes);
       bulk_load(fbuf + (size_t)s * ND * W, (fwd ? tabf_l : tabb_l) + (size_t)b * ND * W, ND * W * 8, &bar[s]);
-      tensor_load_3d(rbuf + (size_t)s * PS_PAIRS * BOX, fwd ? &a.tm_rho : &a.tm_v2, 2 * b * ND, l, p0, &bar[s]);
+      tensor_load_4d(rbuf + (size_t)s * PS_PAIRS * BOX, fwd ? &a.tm_rho : &a.tm_v2, 0, p0, b * ND, l, &bar[s]);
     }
   };
   // store ybuf half h to the rows of block b (rows past Nr and pairs past
@@ -124,7 +131,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
     fence_async_smem();
     __syncwarp();
     if (lane == 0) {
-      tensor_store_3d(&a.tm_v2, 2 * b * ND, l, p0, ybuf + (size_t)h * PS_PAIRS * BOX);
+      tensor_store_4d(&a.tm_v2, 0, p0, b * ND, l, ybuf + (size_t)h * PS_PAIRS * BOX);
       bulk_commit();
     }
   };
@@ -149,13 +156,13 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
     __syncwarp();
     const int s = b % PS_STAGES, h = b & 1;
     const double* __restrict__ fb = fbuf + (size_t)s * ND * W;
-    const double* __restrict__ rb = rbuf + (size_t)(s * PS_PAIRS + P) * BOX + c;
-    double* __restrict__ yb = ybuf + (size_t)(h * PS_PAIRS + P) * BOX + c;
+    const double* __restrict__ rb = rbuf + (size_t)s * PS_PAIRS * BOX + lane;  // row u at rb[u * rstride]
+    double* __restrict__ yb = ybuf + (size_t)h * PS_PAIRS * BOX + lane;
     // the block's inputs first and its results after it, so no shared-memory
     // store sits between the rows and the loads of later rows can be hoisted
     double in[ND];
 #pragma unroll
-    for (int u = 0; u < ND; ++u) in[u] = active ? rb[2 * u] : 0.0;
+    for (int u = 0; u < ND; ++u) in[u] = active ? rb[u * rstride] : 0.0;
 #pragma unroll
     for (int u = 0; u < ND; ++u) {
       double fr[W];
@@ -178,7 +185,8 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
       win[u] = sacc * fr[ND];
     }
 #pragma unroll
-    for (int u = 0; u < ND; ++u) yb[2 * u] = win[u];
+    for (int u = 0; u < ND; ++u)
+      if (owner) yb[u * rstride] = win[u];
     store(h, b);
     if (issued < nb) issue(issued++);
   }
@@ -202,11 +210,11 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
       __syncwarp();
       const int s = q % PS_STAGES, h = q & 1;
       const double* __restrict__ fb = fbuf + (size_t)s * ND * W;
-      const double* __restrict__ rb = rbuf + (size_t)(s * PS_PAIRS + P) * BOX + c;
-      double* __restrict__ yb = ybuf + (size_t)(h * PS_PAIRS + P) * BOX + c;
+      const double* __restrict__ rb = rbuf + (size_t)s * PS_PAIRS * BOX + lane;
+      double* __restrict__ yb = ybuf + (size_t)h * PS_PAIRS * BOX + lane;
       double in[ND];
 #pragma unroll
-      for (int u = 0; u < ND; ++u) in[u] = active ? rb[2 * u] : 0.0;
+      for (int u = 0; u < ND; ++u) in[u] = active ? rb[u * rstride] : 0.0;
 #pragma unroll
       for (int u = ND - 1; u >= 0; --u) {
         double fr[W];
@@ -229,7 +237,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
       }
 #pragma unroll
       for (int u = 0; u < ND; ++u) {
-        yb[2 * u] = fma(t, fb[u * W + ND + 1], win[u]) * fb[u * W + ND + 2];
+        if (owner) yb[u * rstride] = fma(t, fb[u * W + ND + 1], win[u]) * fb[u * W + ND + 2];
       }
       store(h, b);
       if (issued < 2 * nb) issue(issued++);
@@ -264,11 +272,13 @@ static int launch_nd(const PoissonArgs& a, cudaStream_t st) {
 int poisson_encode_maps(PoissonArgs& a) {
   if (a.npair <= 0) { a.boxp = 0; return 0; }
   a.boxp = std::min(PS_PAIRS, a.npair);
-  const cuuint64_t dims[3] = {(cuuint64_t)2 * a.Nr, (cuuint64_t)a.L2, (cuuint64_t)a.npair};
-  const cuuint64_t strides[2] = {(cuuint64_t)a.Nr * 16, (cuuint64_t)a.L2 * a.Nr * 16};
-  const cuuint32_t box[3] = {(cuuint32_t)(2 * a.nd), 1u, (cuuint32_t)a.boxp};
-  int rc = encode_f64_map(&a.tm_rho, a.rho2, 3, dims, strides, box, "Poisson rho2");
-  if (!rc) rc = encode_f64_map(&a.tm_v2, a.v2sph, 3, dims, strides, box, "Poisson v2sph");
+  // 4-d view (re|im, pair, row, l) of [pair][l][row] complex: the box
+  // (2, boxp, nd, 1) lands in shared memory as [row][pair][re|im]
+  const cuuint64_t dims[4] = {2u, (cuuint64_t)a.npair, (cuuint64_t)a.Nr, (cuuint64_t)a.L2};
+  const cuuint64_t strides[3] = {(cuuint64_t)a.L2 * a.Nr * 16, 16u, (cuuint64_t)a.Nr * 16};
+  const cuuint32_t box[4] = {2u, (cuuint32_t)a.boxp, (cuuint32_t)a.nd, 1u};
+  int rc = encode_f64_map(&a.tm_rho, a.rho2, 4, dims, strides, box, "Poisson rho2");
+  if (!rc) rc = encode_f64_map(&a.tm_v2, a.v2sph, 4, dims, strides, box, "Poisson v2sph");
   return rc;
 }
 

@@ -67,6 +67,19 @@ __device__ __forceinline__ void tensor_load_3d(void* dst, const CUtensorMap* tm,
       "l"(tm), "r"(x), "r"(y), "r"(z), "r"(su32(bar))
       : "memory");
 }
+__device__ __forceinline__ void tensor_load_4d(void* dst, const CUtensorMap* tm, int x, int y, int z, int w,
+                                               unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+          su32(dst)),
+      "l"(tm), "r"(x), "r"(y), "r"(z), "r"(w), "r"(su32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tensor_store_4d(const CUtensorMap* tm, int x, int y, int z, int w, const void* src) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(tm), "r"(x),
+               "r"(y), "r"(z), "r"(w), "r"(su32(src))
+               : "memory");
+}
 __device__ __forceinline__ void tensor_store_3d(const CUtensorMap* tm, int x, int y, int z, const void* src) {
   asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tm), "r"(x),
                "r"(y), "r"(z), "r"(su32(src))
@@ -91,7 +104,7 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return encode;
 }
 
-// float64 tensor map of rank 2 or 3, no swizzle, out-of-bounds elements read as 0
+// float64 tensor map of rank 2 to 4, no swizzle, out-of-bounds elements read as 0
 inline int encode_f64_map(CUtensorMap* tm, const void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides_bytes,
                           const cuuint32_t* box, const char* what) {
   auto encode = tensor_map_encoder();
@@ -99,7 +112,7 @@ inline int encode_f64_map(CUtensorMap* tm, const void* base, int rank, const cuu
     fprintf(stderr, "td1c_b200: cuTensorMapEncodeTiled is not available (%s)\n", what);
     return (int)cudaErrorNotSupported;
   }
-  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
   CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void*>(base), dims, strides_bytes, box,
                       estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
