@@ -201,6 +201,18 @@ def run_reference(args):
     return 0
 
 
+def profiled_traffic(phase):
+    """DRAM bytes per launch of the phase's main kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_per_launch.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) == 3 and cells[0] == phase and cells[2].isdigit():
+            return int(cells[2])
+    return None
+
+
 def metric_name():
     try:
         return json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"]
@@ -324,10 +336,7 @@ def main():
     t_dom = phases[dom] / 1e3
     intensity = fl / max(by, 1)
     ridge = f64 * 1e12 / (hbm * 1e9)
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(dom)
+    traffic = profiled_traffic(dom)
     if intensity > ridge:
         roof = {"bound": "tensor", "achieved": fl / t_dom / 1e12, "peak": f64, "unit": "TFLOP/s",
                 "frac": fl / t_dom / 1e12 / f64, "traffic": traffic, "kernel": dom,
