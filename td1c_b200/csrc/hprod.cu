@@ -133,6 +133,8 @@ struct Ctx {
   // phase timing (off during graph capture)
   bool profile = false;
   cudaEvent_t ev[16] = {};
+  cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int nev = 0;
 };
 
@@ -1137,14 +1139,25 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   CiArgs ca{};
   ca.t = c.cit; ca.cic = cic_in; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
   ca.sigma = hcic; ca.int1e = c.int1e; ca.int2e = c.int2e; ca.ene_act = c.ene + 3; ca.dtime = dtime; ca.icomp = c.icomp;
-  if (c.nact > 0) {
-    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, st));
-    rc |= chk("ci rdm", launch_ci_rdm(ca, st));
+  // The RDM chain reads only the CI vector, and its first consumer is
+  // mfprod: it runs on the side stream, concurrently with the one-body
+  // stencil, the pair densities, the Poisson solve and the l->theta
+  // transform, and joins before mfprod (the fork and join are events, so
+  // the RK4 step's graph capture takes them in as graph edges).
+  const bool fork = c.nact > 0;
+  if (fork) {
+    cudaStream_t s2 = c.st2;
+    cudaEventRecord(c.ev_fork, st);
+    cudaStreamWaitEvent(s2, c.ev_fork, 0);
+    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, s2));
+    rc |= chk("ci rdm", launch_ci_rdm(ca, s2));
     int need_rr = (c.ncore > 0 && c.nact * 2 != c.nelact) ? 1 : 0;
-    invden_kernel<<<1, 64, 0, st>>>(c.nact, need_rr, c.den1, c.rden, c.rrden, c.d_status);
+    invden_kernel<<<1, 64, 0, s2>>>(c.nact, need_rr, c.den1, c.rden, c.rrden, c.d_status);
+    cudaEventRecord(c.ev_join, s2);
     c.launches += 6;
   }
-  mark();  // end ci_rdm
+  auto join = [&]() { if (fork) cudaStreamWaitEvent(st, c.ev_join, 0); };
+  mark();  // end ci_rdm (the chain itself overlaps the next phases)
   // one-body
   OneBodyArgs ob{};
   ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = c.igauge;
@@ -1162,11 +1175,13 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     mark();  // end poisson
     rc |= chk("W gemm", gemm(c, c.b_W, c.npair, c.nlat, c.L2, false));
     mark();  // end w_gemm
+    join();
     rc |= chk("mfprod", launch_mfprod(c.mf, st));
     c.launches += 2;
     mark();  // end mfprod
     rc |= chk("gorb gemm", gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false));
   } else {
+    join();
     mark(); mark(); mark(); mark();
   }
   mark();  // end gorb_gemm
@@ -1394,9 +1409,13 @@ void hprod_init_(void) {
   if (c.nfun > 16) { c.status |= ST_CONFIG; return; }
   // one library stream for the process lifetime: callers may hold it
   // (td1c_gpu_stream) beyond hprod_final_
-  static cudaStream_t lib_stream = nullptr;
+  static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr;
   if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
+  if (!lib_stream2) cudaStreamCreateWithFlags(&lib_stream2, cudaStreamNonBlocking);
   c.st = lib_stream;
+  c.st2 = lib_stream2;
+  cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming);
   int rc = build_tables(c);
   rc |= build_pairs(c);
   rc |= build_state(c);
@@ -1490,6 +1509,9 @@ void hprod_final_(void) {
   Ctx& c = *g;
   for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
   if (c.st) cudaStreamSynchronize(c.st);
+  if (c.st2) cudaStreamSynchronize(c.st2);
+  for (cudaEvent_t e : {c.ev_fork, c.ev_join}) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t& e : c.ev) if (e) { cudaEventDestroy(e); e = nullptr; }
   for (void* p : g_allocs) cudaFree(p);
   g_allocs.clear();
   g_rk = RkBufs();

@@ -74,13 +74,15 @@ __global__ void __launch_bounds__(256) orbdots_kernel(OrbdotsArgs a) {
   }
 }
 
-// fixed-order sum of the per-chunk partials
+// fixed-order sum of the per-chunk partials: one warp per entry, lane l adds
+// chunks l, l + 32, ... in order, then a fixed xor tree combines the lanes
 __global__ void sum_partials_kernel(const cplx* __restrict__ partial, int nchunk, int nent, cplx* __restrict__ out) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (t >= nent) return;
   cplx s = mkc(0, 0);
-  for (int c = 0; c < nchunk; ++c) s = cadd(s, partial[(size_t)c * nent + t]);
-  out[t] = s;
+  for (int c = lane; c < nchunk; c += 32) s = cadd(s, partial[(size_t)c * nent + t]);
+  for (int o = 16; o > 0; o >>= 1) { s.x += __shfl_xor_sync(0xffffffffu, s.x, o); s.y += __shfl_xor_sync(0xffffffffu, s.y, o); }
+  if (lane == 0) out[t] = s;
 }
 
 int launch_orbdots(const OrbdotsArgs& a, cudaStream_t st) {
@@ -92,7 +94,7 @@ int launch_orbdots(const OrbdotsArgs& a, cudaStream_t st) {
     attr = true;
   }
   orbdots_kernel<<<nchunk, 256, smem, st>>>(a);
-  sum_partials_kernel<<<(a.nent + 127) / 128, 128, 0, st>>>(a.partial, nchunk, a.nent, a.result);
+  sum_partials_kernel<<<(a.nent + 7) / 8, 256, 0, st>>>(a.partial, nchunk, a.nent, a.result);
   return (int)cudaGetLastError();
 }
 
