@@ -135,6 +135,8 @@ struct Ctx {
   cudaEvent_t ev[16] = {};
   cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t st3 = nullptr;  // side stream of the one-body stencil and of int2e
+  cudaEvent_t ev_ob_fork = nullptr, ev_ob_join = nullptr, ev_i2_fork = nullptr, ev_i2_join = nullptr;
   int nev = 0;
 };
 
@@ -1163,15 +1165,33 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = c.igauge;
   ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
   ob.mval = c.d_mval; ob.orb = c.orb; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = d_lf;
-  rc |= chk("onebody", launch_onebody(ob, st));
+  // the one-body stencil reads only the orbitals and the field: it runs on
+  // the third stream, overlapping the mean-field chain, and joins before
+  // the orbital matrix elements
+  cudaEventRecord(c.ev_ob_fork, st);
+  cudaStreamWaitEvent(c.st3, c.ev_ob_fork, 0);
+  rc |= chk("onebody", launch_onebody(ob, c.st3));
+  cudaEventRecord(c.ev_ob_join, c.st3);
   c.launches++;
-  mark();  // end onebody
+  mark();  // end onebody (the stencil itself overlaps the next phases)
+  bool i2_forked = false;
   // mean field
   if (c.neltot >= 2 && c.npair > 0) {
     rc |= chk("rho gemm", gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true));
     mark();  // end rho_gemm
     rc |= chk("poisson", launch_poisson(c.ps_main, st));
     c.launches++;
+    // int2e needs only rho2 and v2sph: third stream, overlapping l->theta,
+    // mfprod and the theta->l transforms; joins before smallmat
+    if (c.nact > 0) {
+      cudaEventRecord(c.ev_i2_fork, st);
+      cudaStreamWaitEvent(c.st3, c.ev_i2_fork, 0);
+      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, c.st3));
+      else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, c.st3));
+      cudaEventRecord(c.ev_i2_join, c.st3);
+      c.launches += 3;
+      i2_forked = true;
+    }
     mark();  // end poisson
     rc |= chk("W gemm", gemm(c, c.b_W, c.npair, c.nlat, c.L2, false));
     mark();  // end w_gemm
@@ -1186,15 +1206,18 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   }
   mark();  // end gorb_gemm
   // integrals
+  cudaStreamWaitEvent(st, c.ev_ob_join, 0);
   rc |= chk("orbdots", launch_orbdots(c.od, st));
   c.launches += 2;
   mark();  // end orbdots
-  if (c.nact > 0) {
+  if (i2_forked) {
+    cudaStreamWaitEvent(st, c.ev_i2_join, 0);
+  } else if (c.nact > 0) {
     if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
     else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
     c.launches += 3;
   }
-  mark();  // end int2e
+  mark();  // end int2e (its wait for the third stream)
   SmallArgs sa{};
   sa.nfun = c.nfun; sa.nfcore = c.nfcore; sa.ndcore = c.ndcore; sa.nact = c.nact; sa.ncore = c.ncore; sa.nelact = c.nelact;
   sa.icomp = c.icomp; sa.dtime = dtime; sa.ene_fcore = c.ene_fcore; sa.mval = c.d_mval; sa.ent_index = c.ent_index;
@@ -1409,13 +1432,15 @@ void hprod_init_(void) {
   if (c.nfun > 16) { c.status |= ST_CONFIG; return; }
   // one library stream for the process lifetime: callers may hold it
   // (td1c_gpu_stream) beyond hprod_final_
-  static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr;
+  static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr, lib_stream3 = nullptr;
   if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
   if (!lib_stream2) cudaStreamCreateWithFlags(&lib_stream2, cudaStreamNonBlocking);
+  if (!lib_stream3) cudaStreamCreateWithFlags(&lib_stream3, cudaStreamNonBlocking);
   c.st = lib_stream;
   c.st2 = lib_stream2;
-  cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming);
+  c.st3 = lib_stream3;
+  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_join, &c.ev_ob_fork, &c.ev_ob_join, &c.ev_i2_fork, &c.ev_i2_join})
+    cudaEventCreateWithFlags(e, cudaEventDisableTiming);
   int rc = build_tables(c);
   rc |= build_pairs(c);
   rc |= build_state(c);
@@ -1510,7 +1535,9 @@ void hprod_final_(void) {
   for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
   if (c.st) cudaStreamSynchronize(c.st);
   if (c.st2) cudaStreamSynchronize(c.st2);
-  for (cudaEvent_t e : {c.ev_fork, c.ev_join}) if (e) cudaEventDestroy(e);
+  if (c.st3) cudaStreamSynchronize(c.st3);
+  for (cudaEvent_t e : {c.ev_fork, c.ev_join, c.ev_ob_fork, c.ev_ob_join, c.ev_i2_fork, c.ev_i2_join})
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t& e : c.ev) if (e) { cudaEventDestroy(e); e = nullptr; }
   for (void* p : g_allocs) cudaFree(p);
   g_allocs.clear();
