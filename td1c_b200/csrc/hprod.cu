@@ -555,8 +555,21 @@ int build_tables(Ctx& c) {
   c.radk0 = dupload(c.h_radk0);
   c.radp = dupload(c.h_radp);
   c.cost = dupload(c.h_cost);
-  c.legf1 = dupload(c.h_legf1); c.legb1 = dupload(c.h_legb1);
-  c.legf2 = dupload(c.h_legf2); c.legb2 = dupload(c.h_legb2);
+  // Legendre tables with rows padded to legendre_lda(K) (16-byte aligned, zeros
+  // past K) for the tensor-core GEMM: legf (l, theta) -> [theta][l]-major
+  // as the reference stores them, i.e. table(m) is [rows][K] with K contiguous
+  auto pad_tables = [&](const std::vector<double>& h, int nm, int rows, int K) {
+    const int lda = legendre_lda(K);
+    std::vector<double> p((size_t)nm * rows * lda, 0.0);
+    for (int m = 0; m < nm; ++m)
+      for (int r = 0; r < rows; ++r)
+        for (int k = 0; k < K; ++k) p[((size_t)m * rows + r) * lda + k] = h[((size_t)m * rows + r) * K + k];
+    return dupload(p);
+  };
+  c.legf1 = pad_tables(c.h_legf1, 2 * c.mmax1 + 1, c.nlat, c.L1);
+  c.legb1 = pad_tables(c.h_legb1, 2 * c.mmax1 + 1, c.L1, c.nlat);
+  c.legf2 = pad_tables(c.h_legf2, 2 * c.mmax2 + 1, c.nlat, c.L2);
+  c.legb2 = pad_tables(c.h_legb2, 2 * c.mmax2 + 1, c.L2, c.nlat);
   (void)bw;
   // alph_lm (bas_gen_alph.F90:2-26)
   std::vector<double> alph((size_t)c.L1 * (2 * c.mmax1 + 1), 0.0);
@@ -656,41 +669,42 @@ void batch_upload(LegGemmBatch*& dst, const std::vector<LegGemmBatch>& v) { dst 
 
 int build_batches(Ctx& c) {
   const int N = 2 * c.Nr;
-  auto lf1 = [&](int m) { return c.legf1 + (size_t)(m + c.mmax1) * c.nlat * c.L1; };
-  auto lb1 = [&](int m) { return c.legb1 + (size_t)(m + c.mmax1) * c.L1 * c.nlat; };
-  auto lf2 = [&](int m) { return c.legf2 + (size_t)(m + c.mmax2) * c.nlat * c.L2; };
-  auto lb2 = [&](int m) { return c.legb2 + (size_t)(m + c.mmax2) * c.L2 * c.nlat; };
+  const int ld1 = legendre_lda(c.L1), ldn = legendre_lda(c.nlat), ld2 = legendre_lda(c.L2);
+  auto lf1 = [&](int m) { return c.legf1 + (size_t)(m + c.mmax1) * c.nlat * ld1; };
+  auto lb1 = [&](int m) { return c.legb1 + (size_t)(m + c.mmax1) * c.L1 * ldn; };
+  auto lf2 = [&](int m) { return c.legf2 + (size_t)(m + c.mmax2) * c.nlat * ld2; };
+  auto lb2 = [&](int m) { return c.legb2 + (size_t)(m + c.mmax2) * c.L2 * ldn; };
   std::vector<LegGemmBatch> v;
   // sph2ang1 of dynamic orbitals: orbg[f] = legf1[m] (nlat x L1) * orb[f] (L1 x 2Nr)
   for (int f = c.nfcore; f < c.nfun; ++f)
-    v.push_back({lf1(c.mval[f]), (const double*)(c.orb + f * c.nbas), nullptr, (double*)(c.orbg + f * c.ngrid), N, N});
+    v.push_back({lf1(c.mval[f]), (const double*)(c.orb + f * c.nbas), nullptr, (double*)(c.orbg + f * c.ngrid), N, N, ld1, 0});
   c.n_orbg = (int)v.size(); batch_upload(c.b_orbg, v); v.clear();
   // sph2ang1 of the stored frozen core (set-up): orbg0[f] = legf1 * orb0[f]
   for (int f = 0; f < c.nfcore; ++f)
-    v.push_back({lf1(c.mval[f]), (const double*)(c.orb0 + f * c.nbas), nullptr, (double*)(c.orbg0 + f * c.ngrid), N, N});
+    v.push_back({lf1(c.mval[f]), (const double*)(c.orb0 + f * c.nbas), nullptr, (double*)(c.orbg0 + f * c.ngrid), N, N, ld1, 0});
   batch_upload(c.b_orbg0, v); v.clear();
   // ang2sph1 of the gauge-transformed frozen core: orb[f] = legb1 (L1 x nlat) * orbg[f]
   for (int f = 0; f < c.nfcore; ++f)
-    v.push_back({lb1(c.mval[f]), (const double*)(c.orbg + f * c.ngrid), nullptr, (double*)(c.orb + f * c.nbas), N, N});
+    v.push_back({lb1(c.mval[f]), (const double*)(c.orbg + f * c.ngrid), nullptr, (double*)(c.orb + f * c.nbas), N, N, ldn, 0});
   c.n_orbfc = (int)v.size(); batch_upload(c.b_orbfc, v); v.clear();
   // pair density -> rho2 (M = L2, K = nlat)
   for (int p = 0; p < c.npair; ++p) {
     int a = c.pa[p], b = c.pb[p];
     v.push_back({lb2(c.mval[b] - c.mval[a]), (const double*)(c.orbg + a * c.ngrid), (const double*)(c.orbg + b * c.ngrid),
-                 (double*)(c.rho2 + (size_t)p * c.nbas2), N, N});
+                 (double*)(c.rho2 + (size_t)p * c.nbas2), N, N, ldn, 0});
   }
   batch_upload(c.b_rho, v); v.clear();
   for (int p = c.npair; p < c.npair_all; ++p) {
     int a = c.pa[p], b = c.pb[p];
     v.push_back({lb2(c.mval[b] - c.mval[a]), (const double*)(c.orbg + a * c.ngrid), (const double*)(c.orbg + b * c.ngrid),
-                 (double*)(c.rho2 + (size_t)p * c.nbas2), N, N});
+                 (double*)(c.rho2 + (size_t)p * c.nbas2), N, N, ldn, 0});
   }
   batch_upload(c.b_rho_fcfc, v); v.clear();
   // W = legf2 (nlat x L2) * v2sph
   for (int p = 0; p < c.npair_all; ++p) {
     int a = c.pa[p], b = c.pb[p];
     v.push_back({lf2(c.mval[b] - c.mval[a]), (const double*)(c.v2sph + (size_t)p * c.nbas2), nullptr,
-                 (double*)(c.W + (size_t)p * c.ngrid), N, N});
+                 (double*)(c.W + (size_t)p * c.ngrid), N, N, ld2, 0});
   }
   {
     std::vector<LegGemmBatch> v1(v.begin(), v.begin() + c.npair), v2(v.begin() + c.npair, v.end());
@@ -699,12 +713,12 @@ int build_batches(Ctx& c) {
   v.clear();
   // ang2sph1 of g and v2 for dynamic orbitals (M = L1, K = nlat)
   for (int f = c.nfcore; f < c.nfun; ++f)
-    v.push_back({lb1(c.mval[f]), (const double*)(c.gorbg + f * c.ngrid), nullptr, (double*)(c.gorb + f * c.nbas), N, N});
+    v.push_back({lb1(c.mval[f]), (const double*)(c.gorbg + f * c.ngrid), nullptr, (double*)(c.gorb + f * c.nbas), N, N, ldn, 0});
   for (int f = c.nfcore; f < c.nfun; ++f)
-    v.push_back({lb1(c.mval[f]), (const double*)(c.v2orbg + f * c.ngrid), nullptr, (double*)(c.v2orb + f * c.nbas), N, N});
+    v.push_back({lb1(c.mval[f]), (const double*)(c.v2orbg + f * c.ngrid), nullptr, (double*)(c.v2orb + f * c.nbas), N, N, ldn, 0});
   c.n_gorb = (int)v.size(); batch_upload(c.b_gorb, v); v.clear();
   for (int f = 0; f < c.nfcore; ++f)
-    v.push_back({lb1(c.mval[f]), (const double*)(c.gorbg + f * c.ngrid), nullptr, (double*)(c.gorb + f * c.nbas), N, N});
+    v.push_back({lb1(c.mval[f]), (const double*)(c.gorbg + f * c.ngrid), nullptr, (double*)(c.gorb + f * c.nbas), N, N, ldn, 0});
   batch_upload(c.b_gorbfc, v);
   return 0;
 }

@@ -18,12 +18,14 @@
 namespace td1c {
 
 struct LegGemmBatch {
-  const double* A;   // real table, M x K row-major (K contiguous)
+  const double* A;   // real table, M x K row-major, row pitch lda (16-byte aligned rows, zero past K up to lda)
   const double* B0;  // slab (K rows x ldb reals) or conj operand for pair mode
   const double* B1;  // second operand for pair mode
   double* C;         // output, M rows x ldc reals
-  int ldb, ldc;
+  int ldb, ldc, lda, pad;
 };
+// row pitch of the padded Legendre tables: depth rounded up to the GEMM's 32-deep chunks
+__host__ __device__ inline int legendre_lda(int k) { return (k + 31) / 32 * 32; }
 int launch_legendre_gemm(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair,
                          cudaStream_t st);
 
