@@ -137,6 +137,7 @@ struct Ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t st3 = nullptr;  // side stream of the one-body stencil and of int2e
   cudaEvent_t ev_ob_fork = nullptr, ev_ob_join = nullptr, ev_i2_fork = nullptr, ev_i2_join = nullptr;
+  cudaEvent_t ev_sig_fork = nullptr, ev_sig_join = nullptr;
   int nev = 0;
 };
 
@@ -1135,6 +1136,28 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   (void)sg;  // gorbg / v2orbg rows of dynamic orbitals are fully written by mfprod
   cudaMemsetAsync(c.gorb, 0, so * sizeof(cplx), st);
   cudaMemsetAsync(c.v2orb, 0, so * sizeof(cplx), st);
+  // RDMs (ormas_mkden1/2, hprod_invden)
+  CiArgs ca{};
+  ca.t = c.cit; ca.cic = cic_in; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
+  ca.sigma = hcic; ca.int1e = c.int1e; ca.int2e = c.int2e; ca.ene_act = c.ene + 3; ca.dtime = dtime; ca.icomp = c.icomp;
+  // The RDM chain reads only the CI vector, and its first consumer is
+  // mfprod: it runs on the side stream, concurrently with the orbital
+  // transform, the one-body stencil, the pair densities, the Poisson solve
+  // and the l->theta transform, and joins before mfprod (the fork and join are events, so
+  // the RK4 step's graph capture takes them in as graph edges).
+  const bool fork = c.nact > 0;
+  if (fork) {
+    cudaStream_t s2 = c.st2;
+    cudaEventRecord(c.ev_fork, st);
+    cudaStreamWaitEvent(s2, c.ev_fork, 0);
+    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, s2));
+    rc |= chk("ci rdm", launch_ci_rdm(ca, s2));
+    int need_rr = (c.ncore > 0 && c.nact * 2 != c.nelact) ? 1 : 0;
+    invden_kernel<<<1, 64, 0, s2>>>(c.nact, need_rr, c.den1, c.rden, c.rrden, c.d_status);
+    cudaEventRecord(c.ev_join, s2);
+    c.launches += 6;
+  }
+  auto join = [&]() { if (fork) cudaStreamWaitEvent(st, c.ev_join, 0); };
   // orbitals (hprod_orbin.F90)
   cudaMemcpyAsync(c.orb + c.nfcore * c.nbas, wfn + c.nfcore * c.nbas, (so - c.nfcore * c.nbas) * sizeof(cplx),
                   cudaMemcpyDeviceToDevice, st);
@@ -1151,29 +1174,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     }
   }
   mark();  // end orbin
-  // RDMs (ormas_mkden1/2, hprod_invden)
-  CiArgs ca{};
-  ca.t = c.cit; ca.cic = cic_in; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
-  ca.sigma = hcic; ca.int1e = c.int1e; ca.int2e = c.int2e; ca.ene_act = c.ene + 3; ca.dtime = dtime; ca.icomp = c.icomp;
-  // The RDM chain reads only the CI vector, and its first consumer is
-  // mfprod: it runs on the side stream, concurrently with the one-body
-  // stencil, the pair densities, the Poisson solve and the l->theta
-  // transform, and joins before mfprod (the fork and join are events, so
-  // the RK4 step's graph capture takes them in as graph edges).
-  const bool fork = c.nact > 0;
-  if (fork) {
-    cudaStream_t s2 = c.st2;
-    cudaEventRecord(c.ev_fork, st);
-    cudaStreamWaitEvent(s2, c.ev_fork, 0);
-    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, s2));
-    rc |= chk("ci rdm", launch_ci_rdm(ca, s2));
-    int need_rr = (c.ncore > 0 && c.nact * 2 != c.nelact) ? 1 : 0;
-    invden_kernel<<<1, 64, 0, s2>>>(c.nact, need_rr, c.den1, c.rden, c.rrden, c.d_status);
-    cudaEventRecord(c.ev_join, s2);
-    c.launches += 6;
-  }
-  auto join = [&]() { if (fork) cudaStreamWaitEvent(st, c.ev_join, 0); };
-  mark();  // end ci_rdm (the chain itself overlaps the next phases)
+  mark();  // end ci_rdm (the chain itself runs on the side stream, forked before orbin)
   // one-body
   OneBodyArgs ob{};
   ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = c.igauge;
@@ -1240,15 +1241,23 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   smallmat_kernel<<<1, 256, 0, st>>>(sa);
   c.launches++;
   mark();  // end smallmat
-  // CI sigma (ormas_xact2 -> ormas_hcic)
-  if (c.nact > 0) { rc |= chk("ci sigma", launch_ci_sigma(ca, c.maxsec, st)); c.launches += 2; }
-  else cudaMemsetAsync(hcic, 0, sizeof(cplx), st);
-  mark();  // end ci_sigma
+  // CI sigma (ormas_xact2 -> ormas_hcic) on the side stream, concurrently with dtorb
+  if (c.nact > 0) {
+    cudaEventRecord(c.ev_sig_fork, st);
+    cudaStreamWaitEvent(c.st2, c.ev_sig_fork, 0);
+    rc |= chk("ci sigma", launch_ci_sigma(ca, c.maxsec, c.st2));
+    cudaEventRecord(c.ev_sig_join, c.st2);
+    c.launches += 2;
+  } else {
+    cudaMemsetAsync(hcic, 0, sizeof(cplx), st);
+  }
+  mark();  // end ci_sigma (the sigma itself overlaps dtorb)
   // dtorb
   dtorb_kernel<<<(unsigned)((so + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, c.icomp, dtime, c.d_mval, c.orb,
                                                              c.h0orb, c.h1orb, c.gorb, c.v2orb, c.xmat, hwfn);
   c.launches++;
-  mark();  // end dtorb
+  if (c.nact > 0) cudaStreamWaitEvent(st, c.ev_sig_join, 0);
+  mark();  // end dtorb (and sigma)
   c.nev = iev;
   rc |= chk("rhs tail", (int)cudaGetLastError());
   return rc;
@@ -1453,7 +1462,8 @@ void hprod_init_(void) {
   c.st = lib_stream;
   c.st2 = lib_stream2;
   c.st3 = lib_stream3;
-  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_join, &c.ev_ob_fork, &c.ev_ob_join, &c.ev_i2_fork, &c.ev_i2_join})
+  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_join, &c.ev_ob_fork, &c.ev_ob_join, &c.ev_i2_fork, &c.ev_i2_join,
+                         &c.ev_sig_fork, &c.ev_sig_join})
     cudaEventCreateWithFlags(e, cudaEventDisableTiming);
   int rc = build_tables(c);
   rc |= build_pairs(c);
@@ -1550,7 +1560,8 @@ void hprod_final_(void) {
   if (c.st) cudaStreamSynchronize(c.st);
   if (c.st2) cudaStreamSynchronize(c.st2);
   if (c.st3) cudaStreamSynchronize(c.st3);
-  for (cudaEvent_t e : {c.ev_fork, c.ev_join, c.ev_ob_fork, c.ev_ob_join, c.ev_i2_fork, c.ev_i2_join})
+  for (cudaEvent_t e : {c.ev_fork, c.ev_join, c.ev_ob_fork, c.ev_ob_join, c.ev_i2_fork, c.ev_i2_join, c.ev_sig_fork,
+                        c.ev_sig_join})
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t& e : c.ev) if (e) { cudaEventDestroy(e); e = nullptr; }
   for (void* p : g_allocs) cudaFree(p);
