@@ -93,6 +93,13 @@ int td1c_gpu_htot_dev(double dtime, const double* lfield, const void* d_wfn, con
  * (complex arrays as interleaved doubles); returns doubles copied or -1. */
 long td1c_gpu_debug_get(const char* name, double* out, long capacity);
 
+/* Length-form dipole <z> of a device-resident state, written to *out (host):
+ * dip(1) of hprod_dipole (src/hprod/hprod_dipole.F90:2-70), i.e.
+ * Re[2 sum_core <phi|z phi> + sum_{ij} <phi_i|z phi_j> den1(j,i)] with z
+ * applied as the unit-field length-gauge coupling.  Uses the library stream
+ * and its 1-RDM buffers; returns when the value is on the host. */
+int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out);
+
 /* Device-resident RK4 propagation (clcrk::prop with the standard tableau,
  * src/prop/clcrk.cpp:55-87,221-235, plus wfn_mask after every step).
  * d_wfn / d_cic are device buffers updated in place.  The sin^2 pulse is

@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtd1c_b200.so")
 SOURCES = ["hprod.cu", "legendre_gemm.cu", "onebody.cu", "poisson.cu", "mfprod.cu", "reductions.cu", "ci.cu",
-           "int2e_static.cu", "int2e_dmma.cu"]
+           "int2e_static.cu", "int2e_dmma.cu", "observables.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -74,6 +74,8 @@ def load():
     lib.td1c_gpu_rk4_reset.argtypes = [vp, vp]
     lib.td1c_gpu_profile.restype = c_int
     lib.td1c_gpu_profile.argtypes = [c_int, c_double, dp, vp, vp, vp, vp, dp, ctypes.c_char_p, c_int]
+    lib.td1c_gpu_dipole.restype = c_int
+    lib.td1c_gpu_dipole.argtypes = [vp, vp, dp]
     lib.td1c_gpu_int2e_static.restype = c_int
     lib.td1c_gpu_int2e_static.argtypes = [c_int, ip, c_long, vp, vp, vp, vp]
     _lib = lib
@@ -85,5 +87,5 @@ EXPORTED = [
     "hprod_bind_", "hprod_init_", "hprod_set_wfn0_", "hprod_htot_", "hprod_final_",
     "td1c_gpu_last_status", "td1c_gpu_dims", "td1c_gpu_ci_tables", "td1c_gpu_energies",
     "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
-    "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset", "td1c_gpu_int2e_static",
+    "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset", "td1c_gpu_int2e_static", "td1c_gpu_dipole",
 ]

@@ -130,6 +130,7 @@ struct Ctx {
   int status = 0;
   int* d_status = nullptr;  // device status word (ST_* bits)
   double* d_scalar = nullptr;
+  int2* dip_ent = nullptr; int dip_nent = 0; cplx* dip_partial = nullptr;  // dipole entries and chunk sums
   // phase timing (off during graph capture)
   bool profile = false;
   cudaEvent_t ev[16] = {};
@@ -1604,6 +1605,39 @@ int td1c_gpu_htot_dev(double dtime, const double* lfield, const void* d_wfn, con
   cudaMemcpyAsync(c.lfield, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, c.st);
   int rc = run_htot(c, c.lfield, (const cplx*)d_wfn, (const cplx*)d_cic, (cplx*)d_hwfn, (cplx*)d_hcic, dtime);
   return rc ? ST_CUDA : 0;
+}
+
+// length-form dipole <z> of a device-resident state (hprod_dipole.F90, dip(1));
+// uses the context's 1-RDM buffers and its stream, synchronous
+int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  if (!c.dip_ent) {
+    std::vector<int2> ent;
+    for (int f = 0; f < c.ncore; ++f) ent.push_back(make_int2(f, f));
+    for (int ia = 0; ia < c.nact; ++ia)
+      for (int ja = 0; ja < c.nact; ++ja)
+        if (c.mval[c.ncore + ia] == c.mval[c.ncore + ja]) ent.push_back(make_int2(c.ncore + ia, c.ncore + ja));
+    c.dip_nent = (int)ent.size();
+    c.dip_ent = dupload(ent);
+    c.dip_partial = dalloc<cplx>((size_t)std::max(1, dipole_partial_size(c.Nr, c.dip_nent)));
+  }
+  int rc = 0;
+  if (c.nact > 0) {
+    CiArgs ca{};
+    ca.t = c.cit; ca.cic = (const cplx*)d_cic; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
+    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, st));
+    rc |= chk("ci rdm", launch_ci_rdm(ca, st));
+  }
+  DipoleArgs da{};
+  da.Nr = c.Nr; da.L1 = c.L1; da.mmax1 = c.mmax1; da.ncore = c.ncore; da.nact = c.nact; da.nent = c.dip_nent;
+  da.xrad = c.xrad; da.alph = c.alph; da.mval = c.d_mval; da.ent = c.dip_ent; da.wfn = (const cplx*)d_wfn;
+  da.den1 = c.den1; da.partial = c.dip_partial; da.out = c.d_scalar + 2;
+  rc |= chk("dipole", launch_dipole(da, st));
+  cudaMemcpyAsync(out, c.d_scalar + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  return (rc || e != cudaSuccess) ? ST_CUDA : 0;
 }
 
 int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,

@@ -120,6 +120,21 @@ struct MfprodArgs {
 };
 int launch_mfprod(const MfprodArgs& a, cudaStream_t st);
 
+// ---- observables: length-form dipole (hprod_dipole.F90)
+struct DipoleArgs {
+  int Nr, L1, mmax1, ncore, nact, nent;
+  const double* xrad;    // [Nr + 2] radial points (index r + 1)
+  const double* alph;    // [2 mmax1 + 1][L1]
+  const int* mval;       // [nfun]
+  const int2* ent;       // [nent] (i, j): core (f, f) first, then active pairs of equal m
+  const cplx* wfn;       // [nfun][L1][Nr]
+  const cplx* den1;      // [nact][nact]
+  cplx* partial;         // [nchunk][nent]
+  double* out;           // device scalar
+};
+int launch_dipole(const DipoleArgs& a, cudaStream_t st);
+int dipole_partial_size(int Nr, int nent);
+
 
 // ---- CI (ormas_*), full string-product formulation
 struct CiTables {

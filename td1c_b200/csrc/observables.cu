@@ -1,0 +1,78 @@
+// observables.cu -- length-form dipole <z> of the state (hprod_dipole.F90:2-70,
+// dip(1) = Re hprod_trace1(den1, orb, z orb); dip(2) = 0 for the length form).
+//
+//   (z phi_j)(r, l) = x_r [alpha(l-1, m) phi_j(r, l-1) + alpha(l, m) phi_j(r, l+1)]
+//                     (hprod_zprod with unit field, hprod_zprod.F90:108-135)
+//   <z> = Re [ 2 sum_{core f} <phi_f|z phi_f> + sum_{ia, ja, m_i = m_j} <phi_i|z phi_j> den1(ja, ia) ]
+//                     (hprod_trace1.F90:2-88)
+// The matrix elements are accumulated per radial chunk (fixed order) and
+// combined with the 1-RDM in one finishing thread block, so the value does
+// not depend on scheduling.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace td1c {
+
+constexpr int DIP_CHUNK = 64;  // radial points per CTA
+
+// partial[chunk][e] = sum over the chunk's r and all l of conj(phi_i) (z phi_j)
+__global__ void __launch_bounds__(256) dipole_partial_kernel(DipoleArgs a) {
+  const int r0 = blockIdx.x * DIP_CHUNK;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int e = warp; e < a.nent; e += nw) {
+    const int2 ij = a.ent[e];
+    const int i = ij.x, j = ij.y, m = a.mval[j];
+    const int am = m < 0 ? -m : m;
+    const double* al = a.alph + (size_t)(m + a.mmax1) * a.L1;
+    const cplx* pi = a.wfn + (size_t)i * a.L1 * a.Nr;
+    const cplx* pj = a.wfn + (size_t)j * a.L1 * a.Nr;
+    cplx s = mkc(0, 0);
+    for (int q = lane; q < DIP_CHUNK * a.L1; q += 32) {
+      const int l = q / DIP_CHUNK, r = r0 + q % DIP_CHUNK;
+      if (r >= a.Nr || l < am) continue;
+      const double x = a.xrad[r + 1];
+      cplx zp = mkc(0, 0);
+      if (l - 1 >= am) { const cplx w = pj[(size_t)(l - 1) * a.Nr + r]; const double t = x * al[l - 1]; zp.x = fma(w.x, t, zp.x); zp.y = fma(w.y, t, zp.y); }
+      if (l + 1 < a.L1) { const cplx w = pj[(size_t)(l + 1) * a.Nr + r]; const double t = x * al[l]; zp.x = fma(w.x, t, zp.x); zp.y = fma(w.y, t, zp.y); }
+      s = cadd(s, cmulc(pi[(size_t)l * a.Nr + r], zp));
+    }
+    for (int o = 16; o > 0; o >>= 1) { s.x += __shfl_xor_sync(0xffffffffu, s.x, o); s.y += __shfl_xor_sync(0xffffffffu, s.y, o); }
+    if (lane == 0) a.partial[(size_t)blockIdx.x * a.nent + e] = s;
+  }
+}
+
+// sum the chunks of every entry in order, weight them and add
+__global__ void dipole_finish_kernel(DipoleArgs a, int nchunk) {
+  __shared__ double red[256];
+  double part = 0.0;
+  for (int e = threadIdx.x; e < a.nent; e += blockDim.x) {
+    cplx s = mkc(0, 0);
+    for (int c = 0; c < nchunk; ++c) s = cadd(s, a.partial[(size_t)c * a.nent + e]);
+    const int2 ij = a.ent[e];
+    if (ij.x < a.ncore) {
+      part += 2.0 * s.x;  // core orbital, doubly occupied (i == j)
+    } else {
+      const int ia = ij.x - a.ncore, ja = ij.y - a.ncore;
+      part += cmul(s, a.den1[ja + a.nact * ia]).x;  // den1(ja, ia)
+    }
+  }
+  red[threadIdx.x] = part;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.out[0] = red[0];
+}
+
+int launch_dipole(const DipoleArgs& a, cudaStream_t st) {
+  const int nchunk = (a.Nr + DIP_CHUNK - 1) / DIP_CHUNK;
+  if (a.nent <= 0) return (int)cudaMemsetAsync(a.out, 0, sizeof(double), st);
+  dipole_partial_kernel<<<nchunk, 256, 0, st>>>(a);
+  dipole_finish_kernel<<<1, 256, 0, st>>>(a, nchunk);
+  return (int)cudaGetLastError();
+}
+
+int dipole_partial_size(int Nr, int nent) { return ((Nr + DIP_CHUNK - 1) / DIP_CHUNK) * nent; }
+
+}  // namespace td1c

@@ -140,6 +140,12 @@ class HProd:
                                           int(nstep), float(wl["fint"]), float(wl["wlen"]), float(wl["numcyc"]),
                                           float(wl.get("cep", 0.0)), 1 if use_graph else 0))
 
+    def dipole_dev(self, d_wfn, d_cic):
+        """Length-form dipole <z> of a device-resident state (hprod_dipole.F90, dip(1))."""
+        out = np.zeros(1)
+        self._check(self.lib.td1c_gpu_dipole(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(out)))
+        return float(out[0])
+
     def rk4_reset(self, d_wfn0, d_cic0):
         self._check(self.lib.td1c_gpu_rk4_reset(ctypes.c_void_p(d_wfn0) if d_wfn0 else None,
                                                 ctypes.c_void_p(d_cic0) if d_cic0 else None))
