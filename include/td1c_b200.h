@@ -100,6 +100,18 @@ long td1c_gpu_debug_get(const char* name, double* out, long capacity);
  * and its 1-RDM buffers; returns when the value is on the host. */
 int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out);
 
+/* wfn_orth_cic + wfn_orth_orb (src/wfn/wfn_orth.F90:2-110): normalise the CI
+ * vector and Gram-Schmidt the non-frozen orbitals against all earlier
+ * orbitals of equal m, in place on device buffers (library stream). */
+int td1c_gpu_orth(void* d_wfn, void* d_cic);
+/* Imaginary-time relaxation in the form of init_prop12 (src/main/init.cpp:250-319):
+ * per cycle ene[s] (host, ncyc values) = total energy of the current state,
+ * one zero-field RK4 step of dt (with the absorbing mask) and td1c_gpu_orth.
+ * Needs a context bound with icomp = 0 (returns 16 otherwise).  The full-H
+ * RK4 step is explicit: dt must respect its stability limit on the grid's
+ * largest one-body eigenvalue. */
+int td1c_gpu_relax(void* d_wfn, void* d_cic, double dt, int ncyc, double* ene);
+
 /* Device-resident RK4 propagation (clcrk::prop with the standard tableau,
  * src/prop/clcrk.cpp:55-87,221-235, plus wfn_mask after every step).
  * d_wfn / d_cic are device buffers updated in place.  The sin^2 pulse is

@@ -40,6 +40,8 @@ def _load():
     lib.orc_energies.argtypes = [vp, dp]
     lib.orc_field.argtypes = [ctypes.POINTER(OrcPulse), ctypes.c_double, dp]
     lib.orc_rk4.argtypes = [vp, ctypes.POINTER(OrcPulse), ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp]
+    lib.orc_orth.argtypes = [vp, dp, dp]
+    lib.orc_relax.argtypes = [vp, ctypes.c_double, ctypes.c_int, dp, dp, dp]
     lib.orc_dipole.restype = ctypes.c_double
     lib.orc_dipole.argtypes = [vp, dp, dp]
     lib.orc_num_threads.restype = ctypes.c_int
@@ -149,6 +151,21 @@ class Oracle:
         self.lib.orc_rk4(self.h, ctypes.byref(p), float(t0), float(dt), int(nstep), _dp(wfn.view(np.float64)),
                          _dp(cic.view(np.float64)), _dp(dip))
         return wfn, cic, dip
+
+    def orth(self, wfn, cic):
+        """Gram-Schmidt of the orbitals within each m and CI normalisation (returns copies)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        cic = np.ascontiguousarray(cic, dtype=np.complex128).copy()
+        self.lib.orc_orth(self.h, _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)))
+        return wfn, cic
+
+    def relax(self, wfn, cic, dt, ncyc):
+        """Imaginary-time relaxation (icomp = 0); returns (wfn, cic, energy per cycle)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        cic = np.ascontiguousarray(cic, dtype=np.complex128).copy()
+        ene = np.zeros(ncyc)
+        self.lib.orc_relax(self.h, float(dt), int(ncyc), _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)), _dp(ene))
+        return wfn, cic, ene
 
     def dipole(self, wfn, cic):
         wfn = np.ascontiguousarray(wfn, dtype=np.complex128)

@@ -1175,6 +1175,35 @@ struct Oracle {
   }
 
   // length-form dipole <z> = sum_ij <phi_i|z|phi_j> den1_full(j,i)
+  // wfn_orth_cic (wfn_orth.F90:2-29): normalise the CI vector;
+  // wfn_orth_orb (wfn_orth.F90:31-110, fedvr_normalized, ecs_flag = 0):
+  // modified Gram-Schmidt of every non-frozen orbital against all earlier
+  // orbitals of equal m, each overlap taken with the current (already
+  // projected) orbital, then normalisation; sums over l >= |m|, r ascending.
+  void orth(cd* wfn, cd* cic) {
+    double cn = 0.0;
+    for (int d = 0; d < lcic; ++d) cn += std::norm(cic[d]);
+    cn = 1.0 / std::sqrt(cn);
+    for (int d = 0; d < lcic; ++d) cic[d] *= cn;
+    for (int i = nfcore; i < nfun; ++i) {
+      const int mi = mval[i], l0 = std::abs(mi);
+      for (int j = 0; j < i; ++j) {
+        if (mval[j] != mi) continue;
+        cd ov = 0.0;
+        for (int l = l0; l <= lmax1; ++l)
+          for (int ir = 0; ir < Nr; ++ir) ov += std::conj(wfn[io(ir, l, j)]) * wfn[io(ir, l, i)];
+        for (int l = l0; l <= lmax1; ++l)
+          for (int ir = 0; ir < Nr; ++ir) wfn[io(ir, l, i)] -= wfn[io(ir, l, j)] * ov;
+      }
+      double nr = 0.0;
+      for (int l = l0; l <= lmax1; ++l)
+        for (int ir = 0; ir < Nr; ++ir) nr += std::norm(wfn[io(ir, l, i)]);
+      nr = 1.0 / std::sqrt(nr);
+      for (int l = l0; l <= lmax1; ++l)
+        for (int ir = 0; ir < Nr; ++ir) wfn[io(ir, l, i)] *= nr;
+    }
+  }
+
   double dipole(const cd* wfn, const cd* cic) {
     std::vector<cd> zo((size_t)nbas * nfun, 0.0), w(wfn, wfn + (size_t)nbas * nfun);
     zprod(1.0, w, zo, 0, nfun);
@@ -1348,6 +1377,25 @@ void orc_rk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, doubl
         for (int ir = min_ir; ir <= o->Nr; ++ir) Y[o->io(ir - 1, l, f)] *= o->mask[ir];
     t += dt;
     if (dip) dip[s] = o->dipole(Y, C);
+  }
+}
+void orc_orth(void* h, double* wfn, double* cic) {
+  static_cast<Oracle*>(h)->orth(reinterpret_cast<cd*>(wfn), reinterpret_cast<cd*>(cic));
+}
+// imaginary-time relaxation in the form of init_prop12 (init.cpp:250-319):
+// per cycle the energy of the current state, one RK4 step at zero field
+// (wfn_mask included, as in orc_rk4), then wfn_orth_cic + wfn_orth_orb
+void orc_relax(void* h, double dt, int ncyc, double* wfn, double* cic, double* ene) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t no = (size_t)o->nbas * o->nfun, nc = o->lcic;
+  std::vector<cd> hw(no), hc(nc);
+  orc_pulse zero{0.0, 800.0, 1.0, 0.0, o->cfg.igauge};
+  const double lf0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < ncyc; ++s) {
+    o->htot(1.0, lf0, reinterpret_cast<cd*>(wfn), reinterpret_cast<cd*>(cic), hw.data(), hc.data());
+    if (ene) ene[s] = o->ene_tot;
+    orc_rk4(h, &zero, 0.0, dt, 1, wfn, cic, nullptr);
+    o->orth(reinterpret_cast<cd*>(wfn), reinterpret_cast<cd*>(cic));
   }
 }
 double orc_dipole(void* h, const double* wfn, const double* cic) {

@@ -75,6 +75,12 @@ typedef struct {
 void  orc_field(const orc_pulse* p, double t, double* lfield9);
 void  orc_rk4(void* h, const orc_pulse* p, double t0, double dt, int nstep,
               double* wfn, double* cic, double* dip);
+/* wfn_orth_cic + wfn_orth_orb (Gram-Schmidt within each m), in place        */
+void  orc_orth(void* h, double* wfn, double* cic);
+/* Imaginary-time relaxation (init_prop12 form; needs icomp = 0): per cycle
+ * ene[s] = total energy of the current state, one zero-field RK4 step of dt,
+ * then orc_orth.  wfn/cic are updated in place.                              */
+void  orc_relax(void* h, double dt, int ncyc, double* wfn, double* cic, double* ene);
 /* Observable: length-form dipole <z> of the full state (orbitals + CI)      */
 double orc_dipole(void* h, const double* wfn, const double* cic);
 int   orc_num_threads(void);

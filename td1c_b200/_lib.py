@@ -74,6 +74,10 @@ def load():
     lib.td1c_gpu_rk4_reset.argtypes = [vp, vp]
     lib.td1c_gpu_profile.restype = c_int
     lib.td1c_gpu_profile.argtypes = [c_int, c_double, dp, vp, vp, vp, vp, dp, ctypes.c_char_p, c_int]
+    lib.td1c_gpu_orth.restype = c_int
+    lib.td1c_gpu_orth.argtypes = [vp, vp]
+    lib.td1c_gpu_relax.restype = c_int
+    lib.td1c_gpu_relax.argtypes = [vp, vp, c_double, c_int, dp]
     lib.td1c_gpu_dipole.restype = c_int
     lib.td1c_gpu_dipole.argtypes = [vp, vp, dp]
     lib.td1c_gpu_int2e_static.restype = c_int
@@ -88,4 +92,5 @@ EXPORTED = [
     "td1c_gpu_last_status", "td1c_gpu_dims", "td1c_gpu_ci_tables", "td1c_gpu_energies",
     "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
     "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset", "td1c_gpu_int2e_static", "td1c_gpu_dipole",
+    "td1c_gpu_orth", "td1c_gpu_relax",
 ]

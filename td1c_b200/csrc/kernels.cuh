@@ -134,6 +134,8 @@ struct DipoleArgs {
 };
 int launch_dipole(const DipoleArgs& a, cudaStream_t st);
 int dipole_partial_size(int Nr, int nent);
+// wfn_orth_cic + wfn_orth_orb on device-resident orbitals and CI
+int launch_orth(int Nr, int L1, int nfun, int nfcore, int lcic, const int* mval, cplx* wfn, cplx* cic, cudaStream_t st);
 
 
 // ---- CI (ormas_*), full string-product formulation

@@ -1,4 +1,7 @@
-// observables.cu -- length-form dipole <z> of the state (hprod_dipole.F90:2-70,
+// observables.cu -- state-level operations outside the RHS: the length-form
+// dipole and the orthonormalisation used by imaginary-time relaxation.
+//
+// Dipole <z> of the state (hprod_dipole.F90:2-70,
 // dip(1) = Re hprod_trace1(den1, orb, z orb); dip(2) = 0 for the length form).
 //
 //   (z phi_j)(r, l) = x_r [alpha(l-1, m) phi_j(r, l-1) + alpha(l, m) phi_j(r, l+1)]
@@ -74,5 +77,61 @@ int launch_dipole(const DipoleArgs& a, cudaStream_t st) {
 }
 
 int dipole_partial_size(int Nr, int nent) { return ((Nr + DIP_CHUNK - 1) / DIP_CHUNK) * nent; }
+
+// ---------------------------------------------------------------------------
+// wfn_orth_cic + wfn_orth_orb (wfn_orth.F90:2-29, 31-110; fedvr_normalized,
+// ecs_flag = 0): normalise the CI vector; then modified Gram-Schmidt of every
+// non-frozen orbital against all earlier orbitals of equal m (each overlap
+// with the already projected orbital), then normalisation, over l >= |m|.
+// One CTA; every sum is a fixed-order block reduction.
+// ---------------------------------------------------------------------------
+constexpr int ORTH_NT = 1024;
+
+__device__ cplx orth_block_sum(cplx v, cplx* red) {
+  const int tid = threadIdx.x;
+  red[tid] = v;
+  __syncthreads();
+  for (int st = ORTH_NT / 2; st > 0; st >>= 1) {
+    if (tid < st) red[tid] = cadd(red[tid], red[tid + st]);
+    __syncthreads();
+  }
+  const cplx r = red[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(ORTH_NT) orth_kernel(int Nr, int L1, int nfun, int nfcore, int lcic,
+                                                       const int* __restrict__ mval, cplx* wfn, cplx* cic) {
+  __shared__ cplx red[ORTH_NT];
+  const int tid = threadIdx.x;
+  cplx s = mkc(0, 0);
+  for (int d = tid; d < lcic; d += ORTH_NT) s.x += cabs2(cic[d]);
+  const double cn = 1.0 / sqrt(orth_block_sum(s, red).x);
+  for (int d = tid; d < lcic; d += ORTH_NT) cic[d] = cscale(cic[d], cn);
+  for (int i = nfcore; i < nfun; ++i) {
+    const int mi = mval[i], l0 = mi < 0 ? -mi : mi;
+    cplx* pi = wfn + (size_t)i * L1 * Nr;
+    const int n = (L1 - l0) * Nr;  // the l >= |m| rows are contiguous
+    for (int j = 0; j < i; ++j) {
+      if (mval[j] != mi) continue;
+      const cplx* pj = wfn + (size_t)j * L1 * Nr;
+      cplx ov = mkc(0, 0);
+      for (int e = tid; e < n; e += ORTH_NT) ov = cadd(ov, cmulc(pj[(size_t)l0 * Nr + e], pi[(size_t)l0 * Nr + e]));
+      ov = orth_block_sum(ov, red);
+      for (int e = tid; e < n; e += ORTH_NT) pi[(size_t)l0 * Nr + e] = csub(pi[(size_t)l0 * Nr + e], cmul(pj[(size_t)l0 * Nr + e], ov));
+      __syncthreads();
+    }
+    cplx nr = mkc(0, 0);
+    for (int e = tid; e < n; e += ORTH_NT) nr.x += cabs2(pi[(size_t)l0 * Nr + e]);
+    const double inv = 1.0 / sqrt(orth_block_sum(nr, red).x);
+    for (int e = tid; e < n; e += ORTH_NT) pi[(size_t)l0 * Nr + e] = cscale(pi[(size_t)l0 * Nr + e], inv);
+    __syncthreads();
+  }
+}
+
+int launch_orth(int Nr, int L1, int nfun, int nfcore, int lcic, const int* mval, cplx* wfn, cplx* cic, cudaStream_t st) {
+  orth_kernel<<<1, ORTH_NT, 0, st>>>(Nr, L1, nfun, nfcore, lcic, mval, wfn, cic);
+  return (int)cudaGetLastError();
+}
 
 }  // namespace td1c

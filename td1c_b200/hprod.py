@@ -146,6 +146,16 @@ class HProd:
         self._check(self.lib.td1c_gpu_dipole(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(out)))
         return float(out[0])
 
+    def orth_dev(self, d_wfn, d_cic):
+        """wfn_orth_cic + wfn_orth_orb in place on device buffers."""
+        self._check(self.lib.td1c_gpu_orth(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic)))
+
+    def relax_dev(self, d_wfn, d_cic, dt, ncyc):
+        """Imaginary-time relaxation in place (context bound with icomp = 0); returns the energy per cycle."""
+        ene = np.zeros(max(1, int(ncyc)))
+        self._check(self.lib.td1c_gpu_relax(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(dt), int(ncyc), _dp(ene)))
+        return ene[: int(ncyc)]
+
     def rk4_reset(self, d_wfn0, d_cic0):
         self._check(self.lib.td1c_gpu_rk4_reset(ctypes.c_void_p(d_wfn0) if d_wfn0 else None,
                                                 ctypes.c_void_p(d_cic0) if d_cic0 else None))

@@ -87,3 +87,31 @@ def test_full_size_rhs(cuda_ok, wl):
             assert abs(np.vdot(cic, hc).real) < 1e-12 * max(1.0, np.linalg.norm(hc))
     finally:
         h.final()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.NE_SMALL, W.MIXED_SMALL, W.HE_SMALL], ids=lambda w: w["name"])
+def test_relaxation_trace(cuda_ok, base):
+    """Imaginary-time relaxation (icomp = 0): the device orth matches the oracle's on a
+    non-orthonormal state, and 20 relaxation cycles match its energy trace and final state."""
+    import torch
+    wl = dict(base, icomp=0)
+    o, h, orb, cic = _setup(wl)
+    try:
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        h.orth_dev(d_orb.data_ptr(), d_cic.data_ptr())
+        h.sync()
+        wo, co = o.orth(orb, cic)
+        assert rel_err(d_orb.cpu().numpy(), wo) < TOL
+        assert rel_err(d_cic.cpu().numpy(), co) < TOL
+        ncyc = 20
+        wr, cr, eo = o.relax(wo, co, 2e-4, ncyc)
+        h.rk4_reset(None, None)
+        eg = h.relax_dev(d_orb.data_ptr(), d_cic.data_ptr(), 2e-4, ncyc)
+        assert np.all(np.diff(eg) < 0), eg
+        assert np.abs(eg - eo).max() < TOL * np.abs(eo).max(), (eg, eo)
+        assert rel_err(d_orb.cpu().numpy(), wr) < TOL
+        assert rel_err(d_cic.cpu().numpy(), cr) < TOL
+    finally:
+        h.final()

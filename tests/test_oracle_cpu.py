@@ -163,3 +163,23 @@ def test_field_sin2_velocity():
         lf = o.field(t)
         assert abs(lf[2] - A) < 1e-14 and abs(lf[8] - A) < 1e-14
         assert abs(lf[5] + dA) < 1e-8 * famp
+
+
+@pytest.mark.parametrize("base", [W.HE_SMALL, W.MIXED_SMALL], ids=lambda w: w["name"])
+def test_imaginary_time_relaxation(base):
+    """init_prop12 form: the energy falls monotonically, and orth leaves an orthonormal set and a unit CI vector."""
+    wl = dict(base, icomp=0)
+    o = Oracle(wl)
+    orb, cic = oracle_state(o)
+    orb, cic = o.orth(orb, cic)
+    nf = len(wl["orbitals"])
+    mval = [x[2] for x in wl["orbitals"]]
+    w2 = orb.reshape(nf, -1)
+    for i in range(nf):
+        for j in range(nf):
+            if mval[i] == mval[j] and i >= o.dims["nfcore"]:
+                assert abs(np.vdot(w2[j], w2[i]) - (1.0 if i == j else 0.0)) < 1e-12
+    assert abs(np.linalg.norm(cic) - 1.0) < 1e-14
+    w, c, e = o.relax(orb, cic, 2e-4, 25)
+    assert np.all(np.diff(e) < 0), e
+    assert abs(np.linalg.norm(c) - 1.0) < 1e-14
