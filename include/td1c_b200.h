@@ -64,6 +64,11 @@ int td1c_gpu_bind_bas(double znuc, int smul, int mtot, int nfun, const int* otyp
 /* control_bind_ (src/control/control_bind.F90:2-61): icomp 1 real time,
  * 0 imaginary time; igauge 0 length, 1 velocity. */
 int td1c_gpu_bind_control(int icomp, int igauge);
+/* split_type of control_bind_ (isplit; src/control/clcontrol.cpp:98): 0 the
+ * orbital RHS holds h0 + h1 + g + v2, 2 it leaves out h0, 1 it leaves out h0
+ * and the laser coupling h1 (src/hprod/hprod_htot_dtorb.F90:58-84), which the
+ * one-body propagators below then apply.  Default 0. */
+int td1c_gpu_bind_split(int split_type);
 
 /* ---- drop-in hprod entry points -------------------------------------- */
 void hprod_bind_(double* ene_fcore, double* ene_dcore, double* ene_core, double* ene_act,
@@ -74,6 +79,32 @@ void hprod_set_wfn0_(const double* wfn, const double* cic, const char* v2xfc_typ
 void hprod_htot_(const double* dtime, const double* lfield, const double* wfn, const double* cic,
                  double* hwfn, double* hcic);
 void hprod_final_(void);
+
+/* ---- drop-in one-body propagators (src/prop) --------------------------
+ * The reference factors 1 + c T_l (c = i dtime/2, or i dtime/alpha) per l
+ * with ZGBTRF into the caller's band array and solves with ZGBTRS.  Here the
+ * factor calls build the factors on the device and write a handle into the
+ * caller's pivot array (at least 2 ints); the band array is not touched and
+ * may be any buffer.  The product calls take host orbitals
+ * orb(1:nrad-1, 0:lmax1, 1:nfun) and replace the non-frozen ones.  The flags
+ * passed must equal the bound ones (icomp, igauge, split_type) and iprojfc
+ * must be 0; violations, a missing handle or a singular factor are recorded
+ * in td1c_gpu_last_status().
+ *   h1itr_gen_cninv_  include/wrapper.hpp:668 (src/prop/h1itr_gen_cninv.F90:2-63)
+ *   h1itr_prop_       include/wrapper.hpp:670 (src/prop/h1itr_prop.F90:2-175):
+ *       (1 + i dtime/2 H1)^-1 (1 - i dtime/2 H1), H1 = T + V (split_type 1,
+ *       V by correction cycles until their rms norm < thresh, at most maxcyc)
+ *   dpade_gen_        include/wrapper.hpp:650 (src/prop/dpade_gen.F90:2-63)
+ *   dpade_prod_       include/wrapper.hpp:653 (src/prop/dpade_prod.F90:2-124):
+ *       (1 + i dtime/alpha (T + V))^-1, alpha complex (2 doubles) */
+void h1itr_gen_cninv_(const int* icomp, const double* dtime, int* cnpiv, double* cninv);
+void h1itr_prop_(const int* icomp, const int* isplit, const int* igauge, const int* iprojfc, const double* lfield,
+                 const double* dtime, const int* maxcyc, const double* thresh, const int* cnpiv, const double* cninv,
+                 double* wfn);
+void dpade_gen_(const int* icomp, const double* dtime, const double* alpha, double* tinv, int* tpiv);
+void dpade_prod_(const int* isplit, const int* igauge, const int* icomp, const int* iprojfc, const double* lfield,
+                 const double* dtime, const double* alpha, const int* maxcyc, const double* thresh, const int* tpiv,
+                 const double* tinv, double* wfn);
 
 /* ---- extensions ------------------------------------------------------- */
 int td1c_gpu_last_status(void);
@@ -120,6 +151,28 @@ int td1c_gpu_relax(void* d_wfn, void* d_cic, double dt, int ncyc, double* ene);
  * per step when use_graph != 0. */
 int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep,
                  double fint, double wlen, double numcyc, double cep, int use_graph);
+/* The one-body propagators on a device-resident state, in place (library
+ * stream, synchronous); *cycles (may be NULL) = correction cycles added.
+ * lfield is a host array of 9 doubles. */
+int td1c_gpu_h1itr(void* d_wfn, const double* lfield, double dtime, int maxcyc, double thresh, int* cycles);
+int td1c_gpu_dpade(void* d_wfn, const double* lfield, double dtime, double alpha_re, double alpha_im, int maxcyc,
+                   double thresh, int* cycles);
+/* Device-resident split-operator propagation, tdse_split2 with clh1itr +
+ * clcrk (src/main/tdse.cpp:225-266, src/prop/clh1itr.cpp:61-94): per step
+ * the one-body Crank-Nicolson over dt/2 (field at t + dt/4), RK4 over dt on
+ * the RHS of the bound split_type, one-body over dt/2 (field at t + 3dt/4),
+ * wfn_mask.  The one-body steps are skipped for split_type 0 (then this is
+ * td1c_gpu_rk4).  One CUDA graph per step when use_graph != 0. */
+int td1c_gpu_split2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                    double cep, int maxcyc, double thresh, int use_graph);
+/* ETD-RK2 with the Pade one-body inverse (cletdrk2::prop + cldpade with
+ * alpha = 2, src/prop/cletdrk2.cpp:36-61; tdse_prop12 mask per step). */
+int td1c_gpu_etdrk2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                    double cep, int maxcyc, double thresh, int use_graph);
+/* init_prop12 with cletdrk2 (src/main/init.cpp:250-319): per cycle ene[s] =
+ * total energy, one zero-field ETD-RK2 step of dt (no mask), td1c_gpu_orth;
+ * needs icomp = 0. */
+int td1c_gpu_relax_etdrk2(void* d_wfn, void* d_cic, double dt, int ncyc, int maxcyc, double thresh, double* ene);
 /* Make every following td1c_gpu_rk4 step start from the given device state
  * (NULL, NULL to switch off): each step then performs the complete update on
  * the same input, for throughput measurement of a fixed synthetic state. */

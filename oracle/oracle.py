@@ -42,6 +42,16 @@ def _load():
     lib.orc_rk4.argtypes = [vp, ctypes.POINTER(OrcPulse), ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp]
     lib.orc_orth.argtypes = [vp, dp, dp]
     lib.orc_relax.argtypes = [vp, ctypes.c_double, ctypes.c_int, dp, dp, dp]
+    lib.orc_set_split.argtypes = [vp, ctypes.c_int]
+    lib.orc_h1itr_prop.restype = ctypes.c_int
+    lib.orc_h1itr_prop.argtypes = [vp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
+    lib.orc_dpade_prod.restype = ctypes.c_int
+    lib.orc_dpade_prod.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_double, dp]
+    for name in ("orc_split2", "orc_etdrk2"):
+        getattr(lib, name).argtypes = [vp, ctypes.POINTER(OrcPulse), ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_double, dp, dp, dp]
+    lib.orc_relax_etdrk2.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
     lib.orc_dipole.restype = ctypes.c_double
     lib.orc_dipole.argtypes = [vp, dp, dp]
     lib.orc_num_threads.restype = ctypes.c_int
@@ -165,6 +175,52 @@ class Oracle:
         cic = np.ascontiguousarray(cic, dtype=np.complex128).copy()
         ene = np.zeros(ncyc)
         self.lib.orc_relax(self.h, float(dt), int(ncyc), _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)), _dp(ene))
+        return wfn, cic, ene
+
+    def set_split(self, isplit):
+        """split_type: 0 full H in the RHS, 1 two-body part only, 2 h0 left out."""
+        self.lib.orc_set_split(self.h, int(isplit))
+
+    def h1itr_prop(self, lfield, dtime, wfn, maxcyc=20, thresh=1e-10):
+        """One h1itr Crank-Nicolson step over dtime; returns (wfn, cycles)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        n = self.lib.orc_h1itr_prop(self.h, _dp(lf), float(dtime), int(maxcyc), float(thresh), _dp(wfn.view(np.float64)))
+        return wfn, n
+
+    def dpade_prod(self, lfield, dtime, wfn, alpha=2.0, maxcyc=20, thresh=1e-10):
+        """(1 + i dtime/alpha (T + V))^-1 on the non-frozen orbitals; returns (wfn, cycles)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        a = complex(alpha)
+        n = self.lib.orc_dpade_prod(self.h, _dp(lf), float(dtime), a.real, a.imag, int(maxcyc), float(thresh),
+                                    _dp(wfn.view(np.float64)))
+        return wfn, n
+
+    def _prop(self, name, wfn, cic, t0, dt, nstep, maxcyc, thresh):
+        wfn = np.array(wfn, dtype=np.complex128, copy=True)
+        cic = np.array(cic, dtype=np.complex128, copy=True)
+        dip = np.zeros(nstep)
+        p = self.pulse()
+        getattr(self.lib, name)(self.h, ctypes.byref(p), float(t0), float(dt), int(nstep), int(maxcyc), float(thresh),
+                                _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)), _dp(dip))
+        return wfn, cic, dip
+
+    def split2(self, wfn, cic, t0, dt, nstep, maxcyc=20, thresh=1e-10):
+        """tdse_split2 (h1itr + RK4 + h1itr, mask); returns (wfn, cic, dipole per step)."""
+        return self._prop("orc_split2", wfn, cic, t0, dt, nstep, maxcyc, thresh)
+
+    def etdrk2(self, wfn, cic, t0, dt, nstep, maxcyc=20, thresh=1e-10):
+        """ETD-RK2 with the Pade one-body inverse (mask per step); returns (wfn, cic, dipole per step)."""
+        return self._prop("orc_etdrk2", wfn, cic, t0, dt, nstep, maxcyc, thresh)
+
+    def relax_etdrk2(self, wfn, cic, dt, ncyc, maxcyc=20, thresh=1e-10):
+        """Imaginary-time relaxation with ETD-RK2 steps (icomp = 0); returns (wfn, cic, energy per cycle)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        cic = np.ascontiguousarray(cic, dtype=np.complex128).copy()
+        ene = np.zeros(ncyc)
+        self.lib.orc_relax_etdrk2(self.h, float(dt), int(ncyc), int(maxcyc), float(thresh), _dp(wfn.view(np.float64)),
+                                  _dp(cic.view(np.float64)), _dp(ene))
         return wfn, cic, ene
 
     def dipole(self, wfn, cic):

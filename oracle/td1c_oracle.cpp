@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 #ifdef _OPENMP
@@ -163,6 +164,71 @@ static void band_solve(int n, int kd, const double* ab, double* b) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Complex banded LU with partial pivoting and its solve: restatements of the
+// unblocked LAPACK ZGBTF2 / ZGBTRS('N') algorithms that dpade_gen.F90:43 and
+// h1itr_gen_cninv.F90:57 (zgbtrf) and dpade_h0inv / h1itr_cninv (zgbtrs)
+// call.  LAPACK band storage: kv = kl + ku, ab[(kv + i - j) + ldab * j] =
+// A(i, j), ldab = 2 kl + ku + 1; the top kl rows take the fill-in.  Pivots
+// are chosen by |re| + |im| (IZAMAX), first maximum on ties.
+// ---------------------------------------------------------------------------
+struct BandLU {
+  int n = 0, kl = 0, ku = 0;
+  std::vector<cd> ab;
+  std::vector<int> ipiv;
+  cd& A(int i, int j) { return ab[(size_t)(kl + ku + i - j) + (size_t)(2 * kl + ku + 1) * j]; }
+  const cd& A(int i, int j) const { return ab[(size_t)(kl + ku + i - j) + (size_t)(2 * kl + ku + 1) * j]; }
+};
+static double cabs1(cd z) { return std::fabs(z.real()) + std::fabs(z.imag()); }
+static int band_lu(BandLU& m) {
+  const int n = m.n, kl = m.kl, ku = m.ku;
+  m.ipiv.assign(n, 0);
+  int ju = 0, info = 0;
+  for (int j = 0; j < n; ++j) {
+    const int km = std::min(kl, n - 1 - j);
+    int jp = 0;
+    double best = -1.0;
+    for (int i = 0; i <= km; ++i) {
+      double v = cabs1(m.A(j + i, j));
+      if (v > best) { best = v; jp = i; }
+    }
+    m.ipiv[j] = j + jp;
+    if (m.A(j + jp, j) != cd(0.0)) {
+      ju = std::max(ju, std::min(j + ku + jp, n - 1));
+      if (jp != 0)
+        for (int c = j; c <= ju; ++c) std::swap(m.A(j + jp, c), m.A(j, c));
+      if (km > 0) {
+        const cd r = 1.0 / m.A(j, j);
+        for (int i = 1; i <= km; ++i) m.A(j + i, j) *= r;
+        for (int c = j + 1; c <= ju; ++c) {
+          const cd u = m.A(j, c);
+          if (u != cd(0.0))
+            for (int i = 1; i <= km; ++i) m.A(j + i, c) -= m.A(j + i, j) * u;
+        }
+      }
+    } else if (info == 0) {
+      info = j + 1;
+    }
+  }
+  return info;
+}
+static void band_lu_solve(const BandLU& m, cd* b) {
+  const int n = m.n, kl = m.kl, kv = m.kl + m.ku;
+  for (int j = 0; j + 1 < n; ++j) {  // L^-1 P
+    const int lm = std::min(kl, n - 1 - j);
+    const int p = m.ipiv[j];
+    if (p != j) std::swap(b[p], b[j]);
+    const cd t = b[j];
+    for (int i = 1; i <= lm; ++i) b[j + i] -= m.A(j + i, j) * t;
+  }
+  for (int j = n - 1; j >= 0; --j) {  // U^-1 (ZTBSV upper, no transpose, non-unit)
+    if (b[j] == cd(0.0)) continue;
+    b[j] /= m.A(j, j);
+    const cd t = b[j];
+    for (int i = j - 1; i >= std::max(0, j - kv); --i) b[i] -= t * m.A(i, j);
+  }
+}
+
 // Regularised inverse of a Hermitian matrix: U diag(d/(d^2+thr)) U^H
 // (hprod_invden.F90:62-107; zheev replaced by a cyclic complex Jacobi).
 static void herm_reg_inverse(int n, double thr, const cd* a, cd* inva) {
@@ -222,6 +288,7 @@ struct Oracle {
   int nfun = 0, nfcore = 0, ndcore = 0, nact = 0, ncore = 0;
   int nela = 0, nelb = 0, nelact_a = 0, nelact_b = 0, neltot = 0;
   int mmax1 = 0, mmax2 = 0;
+  int isplit = 0;  // split_type (clcontrol.cpp:98): which one-body terms the RHS leaves out
   // radial grid (clfedvr.cpp)
   int nfe = 0, nd = 0, nrad = 0, Nr = 0;
   std::vector<double> xrad, wrad, mask, radk, radk0, radp;  // radk: (2nd+1)*(nrad+1)
@@ -1110,7 +1177,13 @@ struct Oracle {
 #pragma omp parallel for
     for (int i = nfcore; i < nfun; ++i) {
       const size_t oi = (size_t)i * nbas;
-      for (int k = 0; k < nbas; ++k) hwfn[oi + k] = (v2orb[oi + k] + gorb[oi + k] + h1orb[oi + k] + h0orb[oi + k]) * tf2;
+      // isplit 0: h0 + h1 + g + v2; 2: h1 + g + v2; 1: g + v2 (hprod_htot_dtorb.F90:58-84)
+      for (int k = 0; k < nbas; ++k) {
+        cd h = v2orb[oi + k] + gorb[oi + k];
+        if (isplit != 1) h += h1orb[oi + k];
+        if (isplit == 0) h += h0orb[oi + k];
+        hwfn[oi + k] = h * tf2;
+      }
       for (int j = 0; j < nfun; ++j) {
         if (mval[i] != mval[j]) continue;
         cd x = X(j, i);
@@ -1123,6 +1196,7 @@ struct Oracle {
   // hprod_set_wfn0 / hprod_v2fc (hprod_set_wfn0.F90:2-130, 132-219, 790-865)
   void set_wfn0(const cd* wfn, const cd* cic) {
     (void)cic;
+    h1lu_cache.clear();  // tmat changes below
     std::copy(wfn, wfn + (size_t)nbas * nfun, orb0.begin());
     std::fill(v2jfc.begin(), v2jfc.end(), cd(0.0));
     ene_fcore = 0;
@@ -1217,6 +1291,118 @@ struct Oracle {
         s += dot_orb(w, ifn, zo, jfn) * D1(den1, ja, ia);
       }
     return s.real();
+  }
+
+  // =========================================================================
+  // One-body propagators of the split schemes
+  // =========================================================================
+  // LU factors of M_l = 1 + fac T_l, l = 0..lmax1, with T_l the kinetic +
+  // nuclear (+ frozen-core Hartree) band of tmat (dpade_gen.F90:2-63,
+  // h1itr_gen_cninv.F90:2-63, fedvr_normalized: unit diagonal; the stored
+  // A(jrad, irad) = delta + fac tmat(jb1, irad, l)).  Cached per fac.
+  std::map<std::pair<double, double>, std::vector<BandLU>> h1lu_cache;
+  const std::vector<BandLU>& h1lu(cd fac) {
+    const auto key = std::make_pair(fac.real(), fac.imag());
+    auto it = h1lu_cache.find(key);
+    if (it != h1lu_cache.end()) return it->second;
+    std::vector<BandLU> lus(L1);
+    const int bw = 2 * nd + 1;
+#pragma omp parallel for schedule(dynamic)
+    for (int l = 0; l <= lmax1; ++l) {
+      BandLU& m = lus[l];
+      m.n = Nr; m.kl = nd; m.ku = nd;
+      m.ab.assign((size_t)(3 * nd + 1) * Nr, 0.0);
+      const double* tm = &tmat[(size_t)l * Nr * bw];
+      for (int ir = 1; ir <= Nr; ++ir) {
+        m.A(ir - 1, ir - 1) = 1.0;
+        const int jll = std::max(1, ir - nd), jul = std::min(Nr, ir + nd);
+        for (int jr = jll; jr <= jul; ++jr) m.A(jr - 1, ir - 1) += tm[(size_t)(ir - 1) * bw + nd + jr - ir] * fac;
+      }
+      const int info = band_lu(m);
+      if (info != 0) { fprintf(stderr, "oracle: banded LU of 1 + c T failed, l=%d info=%d\n", l, info); abort(); }
+    }
+    return h1lu_cache.emplace(key, std::move(lus)).first->second;
+  }
+  // dpade_h0inv (dpade_prod.F90:126-155), h1itr_cninv (h1itr_cninv.F90:2-31):
+  // w(:, l, f) <- M_l^-1 w(:, l, f) for every orbital and l >= |m_f|
+  void h1inv(const std::vector<BandLU>& lus, std::vector<cd>& w) {
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int f = 0; f < nfun; ++f)
+      for (int l = 0; l <= lmax1; ++l)
+        if (l >= std::abs(mval[f])) band_lu_solve(lus[l], &w[io(0, l, f)]);
+  }
+  // sqrt(sum_{f0 <= f < nfun} <w_f|w_f> / nfun): the residual norm of the
+  // correction cycles (dpade_prod.F90:61-77 with f0 = nfcore;
+  // h1itr_prop.F90:105-129 with f0 = 0)
+  double rms_res(const std::vector<cd>& w, int f0) const {
+    double s = 0.0;
+    for (int f = f0; f < nfun; ++f) s += std::abs(dot_orb(w, f, w, f));
+    return std::sqrt(s / nfun);
+  }
+  // hprod_zprod_dyn / hprod_pzprod_dyn with factor zfac (adds into h)
+  void laser_dyn(cd zfac, const std::vector<cd>& w, std::vector<cd>& h) {
+    if (cfg.igauge == 0) zprod(zfac, w, h, nfcore, nfun);
+    else pzprod(zfac, w, h, nfcore, nfun);
+  }
+  // h1itr_prop (h1itr_prop.F90:2-175, iprojfc = 0, fedvr_normalized): one
+  // Crank-Nicolson step over dtime of the one-body Hamiltonian of the
+  // non-frozen orbitals, (1 + i dtime/2 H1)^-1 (1 - i dtime/2 H1), H1 = T + V
+  // for isplit 1 (V by the correction cycles), T alone otherwise.  Returns
+  // the number of corrections added.
+  int h1itr_prop(const double* lfield, double dtime, int maxcyc, double thresh, cd* wfn) {
+    const cd fac = cfg.icomp == 1 ? IU * dtime * 0.5 : cd(dtime * 0.5);
+    const auto& lus = h1lu(fac);
+    const size_t n = (size_t)nbas * nfun, nf = (size_t)nbas * nfcore;
+    const cd zfield = lfield[2];
+    const cd zfac1 = cfg.icomp == 1 ? -IU * dtime * 0.5 : cd(-dtime * 0.5);
+    const cd zfac2 = zfac1 * zfield;
+    std::vector<cd> o(wfn, wfn + n), h(n, 0.0), t;
+    tprod(o, h, nfcore, nfun);
+    if (isplit == 1) laser_dyn(zfield, o, h);
+    for (size_t k = nf; k < n; ++k) o[k] += zfac1 * h[k];
+    h1inv(lus, o);
+    t = o;
+    int ncorr = 0;
+    if (isplit == 1) {
+      for (int icyc = 1; icyc <= maxcyc; ++icyc) {
+        if (rms_res(o, 0) < thresh) break;
+        std::fill(h.begin(), h.end(), cd(0.0));
+        laser_dyn(zfac2, o, h);
+        o.swap(h);
+        h1inv(lus, o);
+        for (size_t k = 0; k < n; ++k) t[k] += o[k];
+        ++ncorr;
+      }
+    }
+    for (size_t k = nf; k < n; ++k) wfn[k] = t[k];
+    return ncorr;
+  }
+  // dpade_prod (dpade_prod.F90:2-124, iprojfc = 0): the non-frozen orbitals
+  // of w become (1 + c (T + V))^-1 w, c = i dtime / alpha (dtime / alpha in
+  // imaginary time), V by the correction cycles for isplit 1.  Returns the
+  // number of corrections added.
+  int dpade_prod(const double* lfield, double dtime, cd alpha, int maxcyc, double thresh, cd* wfn) {
+    const cd fac = cfg.icomp == 1 ? IU * dtime / alpha : cd(dtime) / alpha;
+    const auto& lus = h1lu(fac);
+    const size_t n = (size_t)nbas * nfun, nf = (size_t)nbas * nfcore;
+    const cd zfac = (cfg.icomp == 1 ? -IU * dtime / alpha : cd(-dtime) / alpha) * lfield[2];
+    std::vector<cd> o(wfn, wfn + n), h(n, 0.0), t;
+    h1inv(lus, o);
+    t = o;
+    int ncorr = 0;
+    if (isplit == 1) {
+      for (int icyc = 1; icyc <= maxcyc; ++icyc) {
+        if (rms_res(o, nfcore) < thresh) break;
+        std::fill(h.begin(), h.end(), cd(0.0));
+        laser_dyn(zfac, o, h);
+        o.swap(h);
+        h1inv(lus, o);
+        for (size_t k = 0; k < n; ++k) t[k] += o[k];
+        ++ncorr;
+      }
+    }
+    for (size_t k = nf; k < n; ++k) wfn[k] = t[k];
+    return ncorr;
   }
 };
 
@@ -1345,38 +1531,122 @@ void orc_field(const orc_pulse* p, double t, double* lf) {
     lf[2] = E; lf[5] = E; lf[8] = A;
   }
 }
-void orc_rk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, double* wfn, double* cic, double* dip) {
-  Oracle* o = static_cast<Oracle*>(h);
+// one clcrk::prop step (clcrk.cpp:55-87, set_coeff_04 221-235) from t over dt
+static void rk4_step(Oracle* o, const orc_pulse* p, double t, double dt, cd* Y, cd* C) {
   const size_t no = (size_t)o->nbas * o->nfun, nc = o->lcic, n = no + nc;
   std::vector<cd> y0(n), ty(n), k[4];
   for (auto& v : k) v.assign(n, 0.0);
-  cd* Y = reinterpret_cast<cd*>(wfn);
-  cd* C = reinterpret_cast<cd*>(cic);
   const double nodes[4] = {0, 0.5, 0.5, 1}, wg[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
   const double a[4][3] = {{0, 0, 0}, {0.5, 0, 0}, {0, 0.5, 0}, {0, 0, 1}};
+  for (size_t q = 0; q < no; ++q) y0[q] = Y[q];
+  for (size_t q = 0; q < nc; ++q) y0[no + q] = C[q];
+  for (int is = 0; is < 4; ++is) {
+    for (size_t q = 0; q < n; ++q) {
+      cd v = y0[q];
+      for (int js = 0; js < is; ++js) v += dt * a[is][js] * k[js][q];
+      ty[q] = v;
+    }
+    double lf[9]; orc_field(p, t + dt * nodes[is], lf);
+    o->htot(1.0, lf, ty.data(), ty.data() + no, k[is].data(), k[is].data() + no);
+    for (size_t q = 0; q < no; ++q) Y[q] += dt * wg[is] * k[is][q];
+    for (size_t q = 0; q < nc; ++q) C[q] += dt * wg[is] * k[is][no + q];
+  }
+}
+// wfn_mask (wfn_mask.F90:2-35)
+static void mask_orbitals(Oracle* o, cd* Y) {
+  int min_ir = 1;
+  for (int ir = 1; ir <= o->Nr; ++ir) if (o->xrad[ir] > o->cfg.rmask) { min_ir = ir; break; }
+  for (int f = o->nfcore; f < o->nfun; ++f)
+    for (int l = std::abs(o->mval[f]); l <= o->lmax1; ++l)
+      for (int ir = min_ir; ir <= o->Nr; ++ir) Y[o->io(ir - 1, l, f)] *= o->mask[ir];
+}
+void orc_rk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, double* wfn, double* cic, double* dip) {
+  Oracle* o = static_cast<Oracle*>(h);
+  cd* Y = reinterpret_cast<cd*>(wfn);
+  cd* C = reinterpret_cast<cd*>(cic);
   double t = t0;
   for (int s = 0; s < nstep; ++s) {
-    for (size_t q = 0; q < no; ++q) y0[q] = Y[q];
-    for (size_t q = 0; q < nc; ++q) y0[no + q] = C[q];
-    for (int is = 0; is < 4; ++is) {  // clcrk.cpp:55-87, set_coeff_04 221-235
-      for (size_t q = 0; q < n; ++q) {
-        cd v = y0[q];
-        for (int js = 0; js < is; ++js) v += dt * a[is][js] * k[js][q];
-        ty[q] = v;
-      }
-      double lf[9]; orc_field(p, t + dt * nodes[is], lf);
-      o->htot(1.0, lf, ty.data(), ty.data() + no, k[is].data(), k[is].data() + no);
-      for (size_t q = 0; q < no; ++q) Y[q] += dt * wg[is] * k[is][q];
-      for (size_t q = 0; q < nc; ++q) C[q] += dt * wg[is] * k[is][no + q];
-    }
-    // wfn_mask (wfn_mask.F90:2-35)
-    int min_ir = 1;
-    for (int ir = 1; ir <= o->Nr; ++ir) if (o->xrad[ir] > o->cfg.rmask) { min_ir = ir; break; }
-    for (int f = o->nfcore; f < o->nfun; ++f)
-      for (int l = std::abs(o->mval[f]); l <= o->lmax1; ++l)
-        for (int ir = min_ir; ir <= o->Nr; ++ir) Y[o->io(ir - 1, l, f)] *= o->mask[ir];
+    rk4_step(o, p, t, dt, Y, C);
+    mask_orbitals(o, Y);
     t += dt;
     if (dip) dip[s] = o->dipole(Y, C);
+  }
+}
+void orc_set_split(void* h, int isplit) { static_cast<Oracle*>(h)->isplit = isplit; }
+int orc_h1itr_prop(void* h, const double* lfield, double dtime, int maxcyc, double thresh, double* wfn) {
+  return static_cast<Oracle*>(h)->h1itr_prop(lfield, dtime, maxcyc, thresh, reinterpret_cast<cd*>(wfn));
+}
+int orc_dpade_prod(void* h, const double* lfield, double dtime, double alpha_re, double alpha_im, int maxcyc,
+                   double thresh, double* wfn) {
+  return static_cast<Oracle*>(h)->dpade_prod(lfield, dtime, cd(alpha_re, alpha_im), maxcyc, thresh,
+                                             reinterpret_cast<cd*>(wfn));
+}
+// tdse_split2 (tdse.cpp:225-266) with H1P = clh1itr (clh1itr.cpp:29-44,
+// 61-94: half step dt/2, field at the middle of each half step) and
+// H2P = clcrk: per step H1P(t), RK4 over dt, H1P(t + dt/2), wfn_mask
+void orc_split2(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh, double* wfn,
+                double* cic, double* dip) {
+  Oracle* o = static_cast<Oracle*>(h);
+  cd* Y = reinterpret_cast<cd*>(wfn);
+  cd* C = reinterpret_cast<cd*>(cic);
+  const bool doh1 = o->isplit != 0;
+  const bool doh2 = o->neltot > 1 || o->isplit != 1;  // ORMAS neltot[2]: all electrons
+  const double dt2 = 0.5 * dt;
+  double lf[9];
+  for (int s = 0; s < nstep; ++s) {
+    const double t = t0 + dt * s;
+    if (doh1) { orc_field(p, t + 0.5 * dt2, lf); o->h1itr_prop(lf, dt2, maxcyc, thresh, Y); }
+    if (doh2) rk4_step(o, p, t, dt, Y, C);
+    if (doh1) { orc_field(p, t + dt2 + 0.5 * dt2, lf); o->h1itr_prop(lf, dt2, maxcyc, thresh, Y); }
+    mask_orbitals(o, Y);
+    if (dip) dip[s] = o->dipole(Y, C);
+  }
+}
+// cletdrk2::prop (cletdrk2.cpp:36-61) with dPade1 = cldpade(alpha = 2)
+static void etdrk2_step(Oracle* o, const orc_pulse* p, double t, double dt, int maxcyc, double thresh, cd* Y, cd* C) {
+  const size_t no = (size_t)o->nbas * o->nfun, nc = o->lcic, n = no + nc;
+  std::vector<cd> w0(n), w1(n), h0(n), h1(n), tw(n);
+  for (size_t q = 0; q < no; ++q) w0[q] = Y[q];
+  for (size_t q = 0; q < nc; ++q) w0[no + q] = C[q];
+  double lf[9];
+  orc_field(p, t, lf);
+  o->htot(1.0, lf, w0.data(), w0.data() + no, h0.data(), h0.data() + no);
+  for (size_t q = 0; q < n; ++q) tw[q] = 2.0 * w0[q] + dt * h0[q];
+  if (o->isplit != 0) o->dpade_prod(lf, dt, cd(2.0), maxcyc, thresh, tw.data());
+  for (size_t q = 0; q < n; ++q) w1[q] = tw[q] - w0[q];
+  orc_field(p, t + dt, lf);
+  o->htot(1.0, lf, w1.data(), w1.data() + no, h1.data(), h1.data() + no);
+  for (size_t q = 0; q < n; ++q) tw[q] = (h1[q] - h0[q]) * (0.5 * dt);
+  if (o->isplit != 0) o->dpade_prod(lf, dt, cd(2.0), maxcyc, thresh, tw.data());
+  for (size_t q = 0; q < no; ++q) Y[q] = w1[q] + tw[q];
+  for (size_t q = 0; q < nc; ++q) C[q] = w1[no + q] + tw[no + q];
+}
+// tdse_prop12 (tdse.cpp:268-310) with H2P = cletdrk2: per step the ETD-RK2
+// update, then wfn_mask
+void orc_etdrk2(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh, double* wfn,
+                double* cic, double* dip) {
+  Oracle* o = static_cast<Oracle*>(h);
+  cd* Y = reinterpret_cast<cd*>(wfn);
+  cd* C = reinterpret_cast<cd*>(cic);
+  for (int s = 0; s < nstep; ++s) {
+    etdrk2_step(o, p, t0 + dt * s, dt, maxcyc, thresh, Y, C);
+    mask_orbitals(o, Y);
+    if (dip) dip[s] = o->dipole(Y, C);
+  }
+}
+// init_prop12 (init.cpp:250-319) with H2P = cletdrk2: per cycle the energy
+// of the current state, one zero-field ETD-RK2 step (no mask), wfn_orth
+void orc_relax_etdrk2(void* h, double dt, int ncyc, int maxcyc, double thresh, double* wfn, double* cic, double* ene) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t no = (size_t)o->nbas * o->nfun, nc = o->lcic;
+  std::vector<cd> hw(no), hc(nc);
+  orc_pulse zero{0.0, 800.0, 1.0, 0.0, o->cfg.igauge};
+  const double lf0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < ncyc; ++s) {
+    o->htot(1.0, lf0, reinterpret_cast<cd*>(wfn), reinterpret_cast<cd*>(cic), hw.data(), hc.data());
+    if (ene) ene[s] = o->ene_tot;
+    etdrk2_step(o, &zero, 0.0, dt, maxcyc, thresh, reinterpret_cast<cd*>(wfn), reinterpret_cast<cd*>(cic));
+    o->orth(reinterpret_cast<cd*>(wfn), reinterpret_cast<cd*>(cic));
   }
 }
 void orc_orth(void* h, double* wfn, double* cic) {

@@ -81,6 +81,28 @@ void  orc_orth(void* h, double* wfn, double* cic);
  * ene[s] = total energy of the current state, one zero-field RK4 step of dt,
  * then orc_orth.  wfn/cic are updated in place.                              */
 void  orc_relax(void* h, double dt, int ncyc, double* wfn, double* cic, double* ene);
+/* split_type (0 full H in the RHS, 1 two-body part only, 2 h0 left out);
+ * only hprod_htot_dtorb and the one-body propagators below read it.         */
+void  orc_set_split(void* h, int isplit);
+/* h1itr_prop: one Crank-Nicolson step over dtime of the one-body part of the
+ * non-frozen orbitals (laser coupling by correction cycles when isplit = 1,
+ * at most maxcyc, stopping below thresh); returns the corrections added.   */
+int   orc_h1itr_prop(void* h, const double* lfield9, double dtime, int maxcyc, double thresh, double* wfn);
+/* dpade_prod: non-frozen orbitals <- (1 + c (T + V))^-1 wfn, c = i dtime /
+ * alpha (dtime / alpha in imaginary time); returns the corrections added.  */
+int   orc_dpade_prod(void* h, const double* lfield9, double dtime, double alpha_re, double alpha_im,
+                     int maxcyc, double thresh, double* wfn);
+/* tdse_split2 with clh1itr + clcrk: per step h1itr over dt/2, RK4 over dt,
+ * h1itr over dt/2, wfn_mask; dip[nstep] as in orc_rk4.                      */
+void  orc_split2(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh,
+                 double* wfn, double* cic, double* dip);
+/* tdse_prop12 with cletdrk2 (+ cldpade, alpha = 2) and wfn_mask per step.   */
+void  orc_etdrk2(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh,
+                 double* wfn, double* cic, double* dip);
+/* init_prop12 with cletdrk2: per cycle ene[s], one zero-field ETD-RK2 step
+ * (no mask), orc_orth (needs icomp = 0).                                     */
+void  orc_relax_etdrk2(void* h, double dt, int ncyc, int maxcyc, double thresh, double* wfn, double* cic,
+                       double* ene);
 /* Observable: length-form dipole <z> of the full state (orbitals + CI)      */
 double orc_dipole(void* h, const double* wfn, const double* cic);
 int   orc_num_threads(void);

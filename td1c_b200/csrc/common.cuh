@@ -32,6 +32,7 @@ enum : int {
   ST_CUDA = 8,         // a CUDA API call failed on the host side
   ST_CONFIG = 16,      // unsupported configuration
   ST_TIMEOUT = 32,     // a bounded wait on an asynchronous copy ran out
+  ST_SINGULAR = 64,    // zero pivot in the one-body propagator factorisation
 };
 
 }  // namespace td1c

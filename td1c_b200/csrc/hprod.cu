@@ -48,7 +48,11 @@ T* dalloc(size_t n) {
     fprintf(stderr, "td1c_b200: cudaMalloc of %zu bytes failed\n", n * sizeof(T));
     return nullptr;
   }
+  // zero it on the legacy stream and wait: the library stream does not
+  // synchronise with the legacy stream, so work queued on it right after the
+  // allocation must not race the clearing
   cudaMemset(p, 0, n * sizeof(T));
+  cudaStreamSynchronize(cudaStreamLegacy);
   g_allocs.push_back(p);
   return p;
 }
@@ -70,6 +74,7 @@ struct Ctx {
   double znuc = 0; int smul = 1, mtot = 0, nfun = 0, nela = 0, nelb = 0;
   std::vector<int> otype, mval, lval;
   int icomp = 1, igauge = 0;
+  int isplit = 0;  // split_type (clcontrol.cpp:98): one-body terms left out of the orbital RHS
   int nfcore = 0, ndcore = 0, nact = 0, ncore = 0, nelact = 0, neltot = 0;
   // ---- hprod_bind_ outputs
   double *p_ene_fcore = nullptr, *p_ene_dcore = nullptr, *p_ene_core = nullptr, *p_ene_act = nullptr, *p_ene_tot = nullptr;
@@ -122,7 +127,7 @@ struct Ctx {
   int n_orbg = 0, n_orbfc = 0, n_gorb = 0;
   // ---- RK4
   cplx *y0 = nullptr, *yacc = nullptr, *ytmp = nullptr, *kbuf = nullptr;
-  double* field_tab = nullptr; int field_cap = 0;
+  double* field_tab = nullptr; long field_cap = 0;  // field table, capacity in doubles
   cudaGraphExec_t graph_exec[4] = {nullptr, nullptr, nullptr, nullptr};
   long launches = 0;
   // ---- misc
@@ -132,6 +137,15 @@ struct Ctx {
   double* d_scalar = nullptr;
   int2* dip_ent = nullptr; int dip_nent = 0; cplx* dip_partial = nullptr;  // dipole entries and chunk sums
   cplx *relax_hw = nullptr, *relax_hc = nullptr;  // RHS outputs of the energy evaluation in td1c_gpu_relax
+  // one-body propagators: condensed factors of 1 + c T per c, and scratch
+  struct H1Slot { double cre = 0, cim = 0; H1Fac f; };
+  H1Slot h1slot[4];
+  int n_h1 = 0;
+  cplx *h1_orb = nullptr, *h1_horb = nullptr;  // correction and laser product [nbas * nfun]
+  double* h1_partial = nullptr;
+  unsigned* h1_ticket = nullptr;
+  int* h1_flags = nullptr;  // [0] done, [1] cycles of the last application
+  int h1_cg = 0;
   // phase timing (off during graph capture)
   bool profile = false;
   cudaEvent_t ev[16] = {};
@@ -518,9 +532,9 @@ __global__ void __launch_bounds__(256) smallmat_kernel(SmallArgs a) {
   }
 }
 
-// hwfn_i = tf2 (v2 + g + h1 + h0)_i + sum_{j, m_j = m_i} orb_j X(j,i)
+// hwfn_i = tf2 (v2 + g [+ h1 [+ h0]])_i + sum_{j, m_j = m_i} orb_j X(j,i)
 // (hprod_htot_dtorb.F90:54-104); frozen-core rows are zero.
-__global__ void dtorb_kernel(int Nr, int L1, int nfun, int nfcore, int icomp, double dtime, const int* __restrict__ mval,
+__global__ void dtorb_kernel(int Nr, int L1, int nfun, int nfcore, int icomp, int isplit, double dtime, const int* __restrict__ mval,
                              const cplx* __restrict__ orb, const cplx* __restrict__ h0, const cplx* __restrict__ h1,
                              const cplx* __restrict__ gg, const cplx* __restrict__ v2, const cplx* __restrict__ xmat,
                              cplx* __restrict__ hwfn) {
@@ -531,7 +545,10 @@ __global__ void dtorb_kernel(int Nr, int L1, int nfun, int nfcore, int icomp, do
   const size_t k = t % nb;
   if (i < nfcore) { hwfn[t] = mkc(0, 0); return; }
   const cplx tf2 = icomp == 0 ? mkc(-dtime, 0) : mkc(0, -dtime);
-  cplx h = cadd(cadd(cadd(v2[t], gg[t]), h1[t]), h0[t]);
+  // isplit 0: v2 + g + h1 + h0; 2: without h0; 1: without h1 and h0 (hprod_htot_dtorb.F90:58-84)
+  cplx h = cadd(v2[t], gg[t]);
+  if (isplit != 1) h = cadd(h, h1[t]);
+  if (isplit == 0) h = cadd(h, h0[t]);
   cplx o = cmul(h, tf2);
   const int mi = mval[i];
   for (int j = 0; j < nfun; ++j) {
@@ -1261,7 +1278,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   }
   mark();  // end ci_sigma (the sigma itself overlaps dtorb)
   // dtorb
-  dtorb_kernel<<<(unsigned)((so + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, c.icomp, dtime, c.d_mval, c.orb,
+  dtorb_kernel<<<(unsigned)((so + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, c.icomp, c.isplit, dtime, c.d_mval, c.orb,
                                                              c.h0orb, c.h1orb, c.gorb, c.v2orb, c.xmat, hwfn);
   c.launches++;
   if (c.nact > 0) cudaStreamWaitEvent(st, c.ev_sig_join, 0);
@@ -1304,12 +1321,26 @@ __global__ void mask_kernel(int Nr, int L1, int nfun, int nfcore, int min_irad, 
   y[t] = cscale(y[t], mask[r + 1]);
 }
 
-// copy the four stage fields of the current step from the table and advance
-__global__ void field_select_kernel(const double* __restrict__ tab, int* __restrict__ counter, int unused,
+// copy the fields of the current step (per doubles) from the table
+__global__ void field_select_kernel(const double* __restrict__ tab, int* __restrict__ counter, int per,
                                     double* __restrict__ cur) {
   int s = counter[0];
   if (s >= counter[1]) s = counter[1] - 1;  // counter[1] = steps staged in the table
-  for (int e = threadIdx.x; e < 36; e += blockDim.x) cur[e] = tab[(size_t)s * 36 + e];
+  if (s < 0) s = 0;
+  for (int e = threadIdx.x; e < per; e += blockDim.x) cur[e] = tab[(size_t)s * per + e];
+}
+
+// z = a x + b y (mode 0) or z = (x - y) a (mode 1); the vector operations of
+// the propagators (clhprod_blas.cpp: axpbyz, xmyz, xpyz, scal)
+__global__ void lincomb_kernel(size_t n, cplx* __restrict__ z, const cplx* __restrict__ x, const cplx* __restrict__ y,
+                               double a, double b, int mode) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const cplx xv = x[t], yv = y[t];
+  cplx o;
+  if (mode == 0) { o.x = a * xv.x + b * yv.x; o.y = a * xv.y + b * yv.y; }
+  else { o.x = (xv.x - yv.x) * a; o.y = (xv.y - yv.y) * a; }
+  z[t] = o;
 }
 __global__ void counter_inc_kernel(int* counter) { if (threadIdx.x == 0) *counter += 1; }
 
@@ -1348,7 +1379,7 @@ void pulse_lfield(const Pulse& p, double t, double* lf) {
 }
 
 struct RkBufs {
-  cplx *y0 = nullptr, *yt = nullptr, *k = nullptr;  // orbitals then CI, contiguous
+  cplx *y0 = nullptr, *yt = nullptr, *k = nullptr, *k2 = nullptr;  // orbitals then CI, contiguous
   double* lf_cur = nullptr;
   int* counter = nullptr;
   size_t cap = 0;
@@ -1358,40 +1389,315 @@ struct RkBufs {
   const void* g_y = nullptr; const void* g_yc = nullptr; const void* g_tab = nullptr;
   const void* g_ro = nullptr; double g_dt = 0; long g_per = 0;
   int h_counter[2] = {0, 0};
+  // cached graphs of one split2 / ETD-RK2 step
+  const void* s_y[2] = {nullptr, nullptr}; const void* s_yc[2] = {nullptr, nullptr};
+  const void* s_tab[2] = {nullptr, nullptr}; double s_dt[2] = {0, 0}; int s_cyc[2] = {0, 0}; double s_thr[2] = {0, 0};
+  int s_split[2] = {-1, -1}; int s_mask[2] = {-1, -1}; long s_per[2] = {0, 0};
+  const void* s_ro[2] = {nullptr, nullptr};
 };
 RkBufs g_rk;
 
-int rk_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int nstep) {
+// ---------------------------------------------------------------------------
+// one-body propagators (h1prop.cu): factor cache and the application of
+// h1itr_prop / dpade_prod to the orbitals of a device state
+// ---------------------------------------------------------------------------
+int h1_factor(Ctx& c, cplx fac, H1Fac* out) {
+  for (int i = 0; i < c.n_h1; ++i)
+    if (c.h1slot[i].cre == fac.x && c.h1slot[i].cim == fac.y) { *out = c.h1slot[i].f; return 0; }
+  if (c.nd < 2 || c.nfe < 1 || (c.nfe * c.nd - 1) != c.Nr) return ST_CONFIG;
+  Ctx::H1Slot* sl = nullptr;
+  for (int i = 0; i < c.n_h1 && !sl; ++i)
+    if (std::isnan(c.h1slot[i].cre)) sl = &c.h1slot[i];  // invalidated by a change of T
+  if (sl) {
+  } else if (c.n_h1 < 4) {
+    sl = &c.h1slot[c.n_h1++];
+    H1Fac& f = sl->f;
+    f.nfe = c.nfe; f.nd = c.nd; f.ni = c.nd - 1; f.nb = c.nfe - 1; f.L1 = c.L1;
+    const size_t ne = (size_t)c.L1 * f.nfe * f.ni, nbt = (size_t)c.L1 * std::max(1, f.nb);
+    f.ainv = dalloc<cplx>(ne * f.ni);
+    f.gl = dalloc<cplx>(ne); f.gr = dalloc<cplx>(ne); f.vl = dalloc<cplx>(ne); f.vr = dalloc<cplx>(ne);
+    f.tdl = dalloc<cplx>(nbt); f.tdi = dalloc<cplx>(nbt); f.tdu = dalloc<cplx>(nbt); f.tdu2 = dalloc<cplx>(nbt);
+    f.tpiv = dalloc<int>(nbt);
+  } else {
+    // all slots taken: rebuild the oldest in place
+    for (int i = 0; i < 3; ++i) std::swap(c.h1slot[i], c.h1slot[i + 1]);
+    sl = &c.h1slot[3];
+  }
+  sl->cre = fac.x; sl->cim = fac.y;
+  H1FacSrc src{};
+  src.Nr = c.Nr; src.L1 = c.L1; src.nd = c.nd; src.nfe = c.nfe; src.c = fac;
+  src.radk = c.radk; src.radk0 = c.radk0; src.tdiag = c.tdiag; src.status = c.d_status;
+  int rc = launch_h1fac(src, sl->f, c.st);
+  *out = sl->f;
+  return rc ? ST_CUDA : 0;
+}
+
+int h1_bufs(Ctx& c) {
+  if (c.h1_orb) return 0;
+  const size_t so = c.nbas * c.nfun;
+  c.h1_orb = dalloc<cplx>(so);
+  c.h1_horb = dalloc<cplx>(so);
+  c.h1_cg = h1solve_pick_cg(c.Nr, c.nfe, c.nd - 1, c.nfe - 1);
+  if (c.h1_cg == 0 || h1op_smem(c.L1, c.nd) > 227 * 1024) return ST_CONFIG;
+  c.h1_partial = dalloc<double>((size_t)c.L1 * h1solve_groups(c.nfun, c.h1_cg));
+  c.h1_ticket = dalloc<unsigned>(1);  // zero (dalloc clears)
+  c.h1_flags = dalloc<int>(2);
+  return 0;
+}
+
+// pade = false: h1itr_prop (h1itr_prop.F90:2-175) over dtime, the
+// Crank-Nicolson factor 1 + (i dtime / 2) T; pade = true: dpade_prod
+// (dpade_prod.F90:2-124), (1 + (i dtime / alpha) (T + V))^-1.  Imaginary
+// time (icomp = 0) drops the i.  d_lf: device lfield of the call.  The
+// non-frozen orbitals of wfn are replaced; launches are fixed in number
+// (maxcyc correction cycles, skipped on the device once converged).
+int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cplx alpha, int maxcyc, double thresh) {
+  cudaStream_t st = c.st;
+  int rc = h1_bufs(c);
+  if (rc) return rc;
+  const bool rt = c.icomp == 1;
+  cplx fac, zf0;  // M = 1 + fac T; laser factor zf0 * lfield[2]
+  if (pade) {
+    const double den = alpha.x * alpha.x + alpha.y * alpha.y;
+    const cplx ia = mkc(alpha.x / den, -alpha.y / den);  // 1 / alpha
+    fac = rt ? cmul(mkc(0, dtime), ia) : cmul(mkc(dtime, 0), ia);
+    zf0 = rt ? cmul(mkc(0, -dtime), ia) : cmul(mkc(-dtime, 0), ia);
+  } else {
+    fac = rt ? mkc(0, dtime * 0.5) : mkc(dtime * 0.5, 0);
+    zf0 = rt ? mkc(0, -dtime * 0.5) : mkc(-dtime * 0.5, 0);
+  }
+  H1Fac F;
+  rc = h1_factor(c, fac, &F);
+  if (rc) return rc;
+  H1OpArgs op{};
+  op.Nr = c.Nr; op.L1 = c.L1; op.nd = c.nd; op.nfun = c.nfun; op.nfcore = c.nfcore; op.mmax1 = c.mmax1;
+  op.igauge = c.igauge; op.radk = c.radk; op.radk0 = c.radk0; op.radp = c.radp; op.tdiag = c.tdiag; op.xrad = c.xrad;
+  op.alph = c.alph; op.mval = c.d_mval; op.lfield = d_lf;
+  H1SolveArgs sv{};
+  sv.fac = F; sv.Nr = c.Nr; sv.L1 = c.L1; sv.nfun = c.nfun; sv.nfcore = c.nfcore; sv.mval = c.d_mval;
+  sv.thresh = thresh; sv.norm_div = (double)c.nfun; sv.partial = c.h1_partial; sv.ticket = c.h1_ticket;
+  sv.done = c.h1_flags; sv.ncyc = c.h1_flags + 1;
+  cudaMemsetAsync(c.h1_flags + 1, 0, sizeof(int), st);
+  if (!pade) {
+    // orb = wfn + zfac1 (T + [zfield V]) wfn on the non-frozen orbitals, then M^-1 on all
+    op.f0 = 0; op.a = mkc(1, 0); op.b = zf0; op.cz0 = c.isplit == 1 ? zf0 : mkc(0, 0); op.afc = mkc(1, 0);
+    op.in = wfn; op.out = c.h1_horb; op.skip = nullptr;
+    rc |= launch_h1op(op, st);
+    sv.fs0 = 0; sv.in = c.h1_horb;
+  } else {
+    sv.fs0 = c.nfcore; sv.in = wfn;
+  }
+  sv.out = c.h1_orb; sv.torb = wfn; sv.accumulate = 0; sv.check_skip = 0;
+  rc |= launch_h1solve(sv, c.h1_cg, st);
+  c.launches += pade ? 1 : 2;
+  if (c.isplit == 1) {
+    op.f0 = c.nfcore; op.a = mkc(0, 0); op.b = mkc(0, 0); op.cz0 = zf0; op.afc = mkc(0, 0);
+    op.in = c.h1_orb; op.out = c.h1_horb; op.skip = c.h1_flags;
+    sv.fs0 = c.nfcore; sv.in = c.h1_horb; sv.out = c.h1_orb; sv.accumulate = 1; sv.check_skip = 1;
+    for (int k = 0; k < maxcyc; ++k) {
+      rc |= launch_h1op(op, st);
+      rc |= launch_h1solve(sv, c.h1_cg, st);
+      c.launches += 2;
+    }
+  }
+  return rc ? ST_CUDA : 0;
+}
+
+// the four stages of clcrk::prop (clcrk.cpp:55-87, set_coeff_04 221-235)
+// from the state (y_orb, y_cic), stage fields lf[0..35] on the device
+int rk4_stages(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, const double* lf) {
   cudaStream_t st = c.st;
   const size_t no = c.nbas * c.nfun, nc = c.lcic;
   RkBufs& b = g_rk;
   const double wts[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
   const double anext[4] = {0.5, 0.5, 1.0, 0.0};
-  field_select_kernel<<<1, 64, 0, st>>>(c.field_tab, b.counter, nstep, b.lf_cur);
-  c.launches++;
-  if (b.reset_orb) {
-    cudaMemcpyAsync(y_orb, b.reset_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(y_cic, b.reset_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
-  }
   cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(b.y0 + no, y_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
   int rc = 0;
   for (int is = 0; is < 4; ++is) {
     const cplx* in = (is == 0) ? b.y0 : b.yt;
-    rc |= run_htot(c, b.lf_cur + 9 * is, in, in + no, b.k, b.k + no, 1.0);
+    rc |= run_htot(c, lf + 9 * is, in, in + no, b.k, b.k + no, 1.0);
     const int nxt = is < 3 ? 1 : 0;
     rk_combine_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(no, y_orb, b.y0, b.k, b.yt, dt * wts[is], dt * anext[is], nxt);
     rk_combine_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(nc, y_cic, b.y0 + no, b.k + no, b.yt + no, dt * wts[is],
                                                                   dt * anext[is], nxt);
     c.launches += 2;
   }
-  int min_irad = 1;
-  for (int ir = 1; ir <= c.Nr; ++ir) if (c.h_xrad[ir] > c.rmask) { min_irad = ir; break; }
-  mask_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, min_irad, c.d_mval, c.mask, y_orb);
-  counter_inc_kernel<<<1, 32, 0, st>>>(b.counter);
-  c.launches += 2;
-  rc |= (int)cudaGetLastError();
   return rc;
+}
+
+// step prologue (fields of the step, optional restart state) and epilogue
+// (wfn_mask, step counter)
+void step_begin(Ctx& c, cplx* y_orb, cplx* y_cic, int per) {
+  cudaStream_t st = c.st;
+  RkBufs& b = g_rk;
+  field_select_kernel<<<1, 64, 0, st>>>(c.field_tab, b.counter, per, b.lf_cur);
+  c.launches++;
+  if (b.reset_orb) {
+    cudaMemcpyAsync(y_orb, b.reset_orb, c.nbas * c.nfun * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(y_cic, b.reset_cic, c.lcic * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  }
+}
+int step_end(Ctx& c, cplx* y_orb, bool do_mask) {
+  cudaStream_t st = c.st;
+  const size_t no = c.nbas * c.nfun;
+  if (do_mask) {
+    int min_irad = 1;
+    for (int ir = 1; ir <= c.Nr; ++ir) if (c.h_xrad[ir] > c.rmask) { min_irad = ir; break; }
+    mask_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, min_irad, c.d_mval, c.mask, y_orb);
+    c.launches++;
+  }
+  counter_inc_kernel<<<1, 32, 0, st>>>(g_rk.counter);
+  c.launches++;
+  return (int)cudaGetLastError();
+}
+
+int rk_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt) {
+  step_begin(c, y_orb, y_cic, 36);
+  int rc = rk4_stages(c, y_orb, y_cic, dt, g_rk.lf_cur);
+  rc |= step_end(c, y_orb, true);
+  return rc;
+}
+
+// tdse_split2 (tdse.cpp:225-266) with H1P = clh1itr, H2P = clcrk: h1itr over
+// dt/2 with the field at t + dt/4, RK4 over dt, h1itr over dt/2 with the
+// field at t + 3 dt/4 (clh1itr.cpp:61-94), wfn_mask.  Step fields: the four
+// RK4 stages, then the two h1itr fields.
+int split2_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double thresh, bool do_mask) {
+  step_begin(c, y_orb, y_cic, 54);
+  const bool doh1 = c.isplit != 0, doh2 = c.neltot > 1 || c.isplit != 1;
+  const double* lf = g_rk.lf_cur;
+  int rc = 0;
+  if (doh1) rc |= h1_apply(c, false, lf + 36, y_orb, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
+  if (doh2) rc |= rk4_stages(c, y_orb, y_cic, dt, lf);
+  if (doh1) rc |= h1_apply(c, false, lf + 45, y_orb, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
+  rc |= step_end(c, y_orb, do_mask);
+  return rc;
+}
+
+// cletdrk2::prop (cletdrk2.cpp:36-61) with cldpade(alpha = 2) and wfn_mask
+// (tdse_prop12, tdse.cpp:268-310; init_prop12 does not mask).  Step fields:
+// t, t + dt.
+int etdrk2_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double thresh, bool do_mask) {
+  cudaStream_t st = c.st;
+  step_begin(c, y_orb, y_cic, 18);
+  RkBufs& b = g_rk;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic, n = no + nc;
+  const double* lf = b.lf_cur;
+  const unsigned gn = (unsigned)((n + 255) / 256), go = (unsigned)((no + 255) / 256), gc = (unsigned)((nc + 255) / 256);
+  cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(b.y0 + no, y_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  int rc = run_htot(c, lf, b.y0, b.y0 + no, b.k, b.k + no, 1.0);  // hWfn0
+  lincomb_kernel<<<gn, 256, 0, st>>>(n, b.yt, b.y0, b.k, 2.0, dt, 0);  // tWfn = 2 Wfn0 + dt hWfn0
+  c.launches++;
+  if (c.isplit != 0) rc |= h1_apply(c, true, lf, b.yt, dt, mkc(2, 0), maxcyc, thresh);
+  lincomb_kernel<<<go, 256, 0, st>>>(no, y_orb, b.yt, b.y0, 1.0, -1.0, 0);  // Wfn1 = tWfn - Wfn0
+  lincomb_kernel<<<gc, 256, 0, st>>>(nc, y_cic, b.yt + no, b.y0 + no, 1.0, -1.0, 0);
+  c.launches += 2;
+  rc |= run_htot(c, lf + 9, y_orb, y_cic, b.k2, b.k2 + no, 1.0);  // hWfn1
+  lincomb_kernel<<<gn, 256, 0, st>>>(n, b.yt, b.k2, b.k, 0.5 * dt, 0.0, 1);  // tWfn = (hWfn1 - hWfn0) dt/2
+  c.launches++;
+  if (c.isplit != 0) rc |= h1_apply(c, true, lf + 9, b.yt, dt, mkc(2, 0), maxcyc, thresh);
+  lincomb_kernel<<<go, 256, 0, st>>>(no, y_orb, y_orb, b.yt, 1.0, 1.0, 0);  // Wfn = Wfn1 + tWfn
+  lincomb_kernel<<<gc, 256, 0, st>>>(nc, y_cic, y_cic, b.yt + no, 1.0, 1.0, 0);
+  c.launches += 2;
+  rc |= step_end(c, y_orb, do_mask);
+  return rc;
+}
+
+// Propagation driver of td1c_gpu_rk4 / _split2 / _etdrk2 (kind 0 / 1 / 2):
+// stages the fields of every step, then runs the steps eagerly or as one
+// CUDA graph per step (captured after one eager step that does the first-call
+// set-up: factor tables, scratch, kernel attributes).
+int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+             double cep, int maxcyc, double thresh, int use_graph, bool do_mask = true) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  if (nstep <= 0) return 0;
+  if (kind != 0 && (maxcyc < 0 || !(thresh >= 0.0))) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic;
+  RkBufs& b = g_rk;
+  if (b.cap < no + nc) {
+    b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc); b.k2 = dalloc<cplx>(no + nc);
+    if (!b.lf_cur) { b.lf_cur = dalloc<double>(54); b.counter = dalloc<int>(2); }
+    b.cap = no + nc;
+  }
+  // fields of every step: RK4 stages t + dt c_s (clcrk.cpp:62-73); split2
+  // adds the two h1itr fields; ETD-RK2 uses t and t + dt
+  Pulse p;
+  p.famp = std::sqrt(fint / 3.50944506E+16); p.freq = 1239.84190 / (wlen * 27.2113845);
+  p.period = 2 * PI / p.freq; p.numcyc = numcyc; p.cep = cep / 180.0 * PI; p.igauge = c.igauge;
+  static const double nodes_rk[4] = {0.0, 0.5, 0.5, 1.0};
+  static const double nodes_s2[6] = {0.0, 0.5, 0.5, 1.0, 0.25, 0.75};
+  static const double nodes_etd[2] = {0.0, 1.0};
+  const double* nodes = kind == 0 ? nodes_rk : (kind == 1 ? nodes_s2 : nodes_etd);
+  const int nf = kind == 0 ? 4 : (kind == 1 ? 6 : 2), per = 9 * nf;
+  std::vector<double> tab((size_t)nstep * per);
+  for (int s = 0; s < nstep; ++s)
+    for (int is = 0; is < nf; ++is) pulse_lfield(p, t0 + dt * s + dt * nodes[is], &tab[(size_t)s * per + 9 * is]);
+  const size_t need = (size_t)nstep * per;
+  if ((size_t)c.field_cap < need) {
+    const size_t cap = std::max(need, (size_t)65536 * 54);  // keep the table address stable across calls
+    c.field_tab = dalloc<double>(cap);
+    c.field_cap = (long)cap;
+  }
+  cudaMemcpyAsync(c.field_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  b.h_counter[0] = 0; b.h_counter[1] = nstep;
+  cudaMemcpyAsync(b.counter, b.h_counter, 2 * sizeof(int), cudaMemcpyHostToDevice, st);
+  c.launches = 0;
+  cplx* y = (cplx*)d_wfn;
+  cplx* yc = (cplx*)d_cic;
+  auto step = [&]() -> int {
+    if (kind == 0) return rk_step(c, y, yc, dt);
+    if (kind == 1) return split2_step(c, y, yc, dt, maxcyc, thresh, do_mask);
+    return etdrk2_step(c, y, yc, dt, maxcyc, thresh, do_mask);
+  };
+  int rc = 0;
+  if (!use_graph) {
+    for (int s = 0; s < nstep; ++s) rc |= step();
+  } else {
+    int s0 = 0;
+    cudaGraphExec_t& ge = c.graph_exec[kind];
+    bool cached;
+    if (kind == 0) {
+      cached = ge && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt && b.g_ro == b.reset_orb;
+    } else {
+      const int q = kind - 1;
+      cached = ge && b.s_y[q] == y && b.s_yc[q] == yc && b.s_tab[q] == c.field_tab && b.s_dt[q] == dt &&
+               b.s_cyc[q] == maxcyc && b.s_thr[q] == thresh && b.s_split[q] == c.isplit &&
+               b.s_mask[q] == (int)do_mask && b.s_ro[q] == b.reset_orb;
+    }
+    if (!cached) {
+      rc |= step();
+      s0 = 1;
+      if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+      long l0 = c.launches;
+      cudaGraph_t graph;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
+      rc |= step();
+      if (cudaStreamEndCapture(st, &graph) != cudaSuccess) return ST_CUDA;
+      if (cudaGraphInstantiate(&ge, graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
+      cudaGraphDestroy(graph);
+      const long per_step = c.launches - l0;
+      c.launches = l0;
+      if (kind == 0) {
+        b.g_per = per_step; b.g_y = y; b.g_yc = yc; b.g_tab = c.field_tab; b.g_dt = dt; b.g_ro = b.reset_orb;
+      } else {
+        const int q = kind - 1;
+        b.s_per[q] = per_step; b.s_y[q] = y; b.s_yc[q] = yc; b.s_tab[q] = c.field_tab; b.s_dt[q] = dt;
+        b.s_cyc[q] = maxcyc; b.s_thr[q] = thresh; b.s_split[q] = c.isplit; b.s_mask[q] = (int)do_mask;
+        b.s_ro[q] = b.reset_orb;
+      }
+    }
+    const long per_step = kind == 0 ? b.g_per : b.s_per[kind - 1];
+    for (int s = s0; s < nstep; ++s) {
+      if (cudaGraphLaunch(ge, st) != cudaSuccess) return ST_CUDA;
+      c.launches += per_step;
+    }
+  }
+  rc |= (int)cudaGetLastError();
+  return rc ? ST_CUDA : 0;
 }
 
 }  // namespace
@@ -1447,6 +1753,12 @@ int td1c_gpu_bind_bas(double znuc, int smul, int mtot, int nfun, const int* otyp
 int td1c_gpu_bind_control(int icomp, int igauge) {
   Ctx& c = ctx();
   c.icomp = icomp; c.igauge = igauge;
+  return 0;
+}
+
+int td1c_gpu_bind_split(int split_type) {
+  if (split_type < 0 || split_type > 2) return ST_CONFIG;
+  ctx().isplit = split_type;
   return 0;
 }
 
@@ -1531,8 +1843,10 @@ void hprod_set_wfn0_(const double* wfn, const double* cic, const char* v2xfc_typ
   cudaStreamSynchronize(st);
   c.ene_fcore = 2.0 * es[0] + es[1];
   cudaMemsetAsync(c.gorbg, 0, c.nfcore * c.ngrid * sizeof(cplx), st);  // scratch of the energy only
-  // hprod_addfc_tmat: add v2jfc to the kinetic diagonal
+  // hprod_addfc_tmat: add v2jfc to the kinetic diagonal; the one-body
+  // propagator factors of the old T are stale
   tdiag_kernel<<<(c.Nr * c.L1 + 255) / 256, 256, 0, st>>>(c.Nr, c.L1, c.nd, c.znuc, c.xrad, c.radk, c.radk0, c.v2jfc, c.tdiag);
+  for (int i = 0; i < c.n_h1; ++i) c.h1slot[i].cre = c.h1slot[i].cim = std::nan("");
   cudaStreamSynchronize(st);
   if (cudaGetLastError() != cudaSuccess) c.status |= ST_CUDA;
 }
@@ -1601,6 +1915,7 @@ int td1c_gpu_ci_tables(unsigned* stra, unsigned* strb, int* detoff, int* afirst,
 
 int td1c_gpu_energies(double* e) {
   Ctx& c = ctx();
+  if (c.st) cudaStreamSynchronize(c.st);
   cudaMemcpy(c.h_ene, c.ene, 5 * sizeof(double), cudaMemcpyDeviceToHost);
   memcpy(e, c.h_ene, sizeof(c.h_ene));
   return 0;
@@ -1689,66 +2004,147 @@ int td1c_gpu_relax(void* d_wfn, void* d_cic, double dt, int ncyc, double* ene) {
 
 int td1c_gpu_rk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
                  double cep, int use_graph) {
+  return prop_run(0, d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, 0, 0.0, use_graph);
+}
+
+int td1c_gpu_split2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                    double cep, int maxcyc, double thresh, int use_graph) {
+  return prop_run(1, d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, maxcyc, thresh, use_graph);
+}
+
+int td1c_gpu_etdrk2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                    double cep, int maxcyc, double thresh, int use_graph) {
+  return prop_run(2, d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, maxcyc, thresh, use_graph);
+}
+
+// one h1itr_prop / dpade_prod on a device-resident state; cycles = correction
+// cycles applied
+static int h1_call(bool pade, void* d_wfn, const double* lfield, double dtime, cplx alpha, int maxcyc, double thresh,
+                   int* cycles) {
   Ctx& c = ctx();
-  if (!c.initialized) return ST_CONFIG;
-  if (nstep <= 0) return 0;
+  if (!c.initialized || !d_wfn || !lfield || maxcyc < 0 || !(thresh >= 0.0)) return ST_CONFIG;
   cudaStream_t st = c.st;
-  const size_t no = c.nbas * c.nfun, nc = c.lcic;
-  RkBufs& b = g_rk;
-  if (b.cap < no + nc) {
-    b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc);
-    if (!b.lf_cur) { b.lf_cur = dalloc<double>(36); b.counter = dalloc<int>(2); }
-    b.cap = no + nc;
-  }
-  // stage fields of every step (clcrk.cpp:62-73: t + dt * c_s)
-  Pulse p;
-  p.famp = std::sqrt(fint / 3.50944506E+16); p.freq = 1239.84190 / (wlen * 27.2113845);
-  p.period = 2 * PI / p.freq; p.numcyc = numcyc; p.cep = cep / 180.0 * PI; p.igauge = c.igauge;
-  std::vector<double> tab((size_t)nstep * 36);
-  const double nodes[4] = {0.0, 0.5, 0.5, 1.0};
-  for (int s = 0; s < nstep; ++s)
-    for (int is = 0; is < 4; ++is) pulse_lfield(p, t0 + dt * s + dt * nodes[is], &tab[(size_t)s * 36 + 9 * is]);
-  if (c.field_cap < nstep) {
-    const int cap = std::max(nstep, 65536);  // keep the table address stable across calls
-    c.field_tab = dalloc<double>((size_t)cap * 36);
-    c.field_cap = cap;
-  }
-  cudaMemcpyAsync(c.field_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st);
-  b.h_counter[0] = 0; b.h_counter[1] = nstep;
-  cudaMemcpyAsync(b.counter, b.h_counter, 2 * sizeof(int), cudaMemcpyHostToDevice, st);
-  c.launches = 0;
-  cplx* y = (cplx*)d_wfn;
-  cplx* yc = (cplx*)d_cic;
+  cudaMemcpyAsync(c.lfield, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+  int rc = h1_apply(c, pade, c.lfield, (cplx*)d_wfn, dtime, alpha, maxcyc, thresh);
+  if (rc) return rc;
+  int flags[2] = {0, 0}, dst = 0;
+  cudaMemcpyAsync(flags, c.h1_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return ST_CUDA;
+  if (cycles) *cycles = flags[1];
+  return dst;
+}
+
+int td1c_gpu_h1itr(void* d_wfn, const double* lfield, double dtime, int maxcyc, double thresh, int* cycles) {
+  return h1_call(false, d_wfn, lfield, dtime, mkc(0, 0), maxcyc, thresh, cycles);
+}
+
+int td1c_gpu_dpade(void* d_wfn, const double* lfield, double dtime, double alpha_re, double alpha_im, int maxcyc,
+                   double thresh, int* cycles) {
+  if (alpha_re == 0.0 && alpha_im == 0.0) return ST_CONFIG;
+  return h1_call(true, d_wfn, lfield, dtime, mkc(alpha_re, alpha_im), maxcyc, thresh, cycles);
+}
+
+// imaginary-time relaxation in the form of init_prop12 (init.cpp:250-319)
+// with H2P = cletdrk2: per cycle the total energy (ene[s], host), one
+// zero-field ETD-RK2 step of dt without mask, wfn_orth; icomp = 0
+int td1c_gpu_relax_etdrk2(void* d_wfn, void* d_cic, double dt, int ncyc, int maxcyc, double thresh, double* ene) {
+  Ctx& c = ctx();
+  if (!c.initialized || c.icomp != 0 || ncyc < 0) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  const size_t so = c.nbas * c.nfun;
+  if (!c.relax_hw) { c.relax_hw = dalloc<cplx>(so); c.relax_hc = dalloc<cplx>(std::max(1, c.lcic)); }
+  double* d_trace = nullptr;
+  if (cudaMalloc(&d_trace, sizeof(double) * std::max(1, ncyc)) != cudaSuccess) return ST_CUDA;
+  const double lf0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   int rc = 0;
-  if (!use_graph) {
-    for (int s = 0; s < nstep; ++s) rc |= rk_step(c, y, yc, dt, nstep);
-  } else {
-    int s0 = 0;
-    const bool cached = c.graph_exec[0] && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt &&
-                        b.g_ro == b.reset_orb;
-    if (!cached) {
-      // one eager step (kernel attributes, first-call set-up), then capture one step
-      rc |= rk_step(c, y, yc, dt, nstep);
-      s0 = 1;
-      if (c.graph_exec[0]) { cudaGraphExecDestroy(c.graph_exec[0]); c.graph_exec[0] = nullptr; }
-      long l0 = c.launches;
-      cudaGraph_t graph;
-      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
-      rc |= rk_step(c, y, yc, dt, nstep);
-      if (cudaStreamEndCapture(st, &graph) != cudaSuccess) return ST_CUDA;
-      if (cudaGraphInstantiate(&c.graph_exec[0], graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
-      cudaGraphDestroy(graph);
-      b.g_per = c.launches - l0;
-      c.launches = l0;
-      b.g_y = y; b.g_yc = yc; b.g_tab = c.field_tab; b.g_dt = dt; b.g_ro = b.reset_orb;
-    }
-    for (int s = s0; s < nstep; ++s) {
-      if (cudaGraphLaunch(c.graph_exec[0], st) != cudaSuccess) return ST_CUDA;
-      c.launches += b.g_per;
-    }
+  for (int s = 0; s < ncyc && !rc; ++s) {
+    cudaMemcpyAsync(c.lfield, lf0, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+    rc |= run_htot(c, c.lfield, (const cplx*)d_wfn, (const cplx*)d_cic, c.relax_hw, c.relax_hc, 1.0);
+    cudaMemcpyAsync(d_trace + s, c.ene + 4, sizeof(double), cudaMemcpyDeviceToDevice, st);
+    rc |= prop_run(2, d_wfn, d_cic, 0.0, dt, 1, 0.0, 800.0, 1.0, 0.0, maxcyc, thresh, 1, false);
+    rc |= launch_orth(c.Nr, c.L1, c.nfun, c.nfcore, c.lcic, c.d_mval, (cplx*)d_wfn, (cplx*)d_cic, st);
   }
-  rc |= (int)cudaGetLastError();
-  return rc ? ST_CUDA : 0;
+  if (ene && ncyc > 0) cudaMemcpyAsync(ene, d_trace, ncyc * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(d_trace);
+  int dst = 0;
+  cudaMemcpy(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  return (rc || e != cudaSuccess) ? ST_CUDA : dst;
+}
+
+// ---- drop-in one-body propagator entries (host buffers) -------------------
+// The factor calls build the condensed factors on the device and write a
+// handle into the caller's pivot array (the band array is not touched); the
+// product calls check the handle and the bound control flags.
+static const int kH1Magic = 0x7D1C0B1;
+
+static int h1_dropin_factor(int icomp, double dtime, cplx alpha, bool pade, int* piv) {
+  Ctx& c = ctx();
+  if (!c.initialized || icomp != c.icomp || !piv) return ST_CONFIG;
+  const bool rt = icomp == 1;
+  cplx fac;
+  if (pade) {
+    const double den = alpha.x * alpha.x + alpha.y * alpha.y;
+    if (den == 0.0) return ST_CONFIG;
+    const cplx ia = mkc(alpha.x / den, -alpha.y / den);
+    fac = rt ? cmul(mkc(0, dtime), ia) : cmul(mkc(dtime, 0), ia);
+  } else {
+    fac = rt ? mkc(0, dtime * 0.5) : mkc(dtime * 0.5, 0);
+  }
+  H1Fac F;
+  int rc = h1_bufs(c);
+  rc |= h1_factor(c, fac, &F);
+  if (cudaStreamSynchronize(c.st) != cudaSuccess) rc |= ST_CUDA;
+  int dst = 0;
+  cudaMemcpy(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  piv[0] = kH1Magic;
+  piv[1] = pade ? 1 : 0;
+  return rc | dst;
+}
+
+static int h1_dropin_prod(bool pade, int isplit, int igauge, int icomp, int iprojfc, const double* lfield, double dtime,
+                          cplx alpha, int maxcyc, double thresh, const int* piv, double* wfn) {
+  Ctx& c = ctx();
+  if (!c.initialized || !piv || piv[0] != kH1Magic || piv[1] != (pade ? 1 : 0)) return ST_CONFIG;
+  if (isplit != c.isplit || igauge != c.igauge || icomp != c.icomp || iprojfc != 0) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  const size_t so = c.nbas * c.nfun;
+  cudaMemcpyAsync(c.wfn_io, wfn, so * sizeof(cplx), cudaMemcpyHostToDevice, st);
+  int rc = h1_call(pade, c.wfn_io, lfield, dtime, alpha, maxcyc, thresh, nullptr);
+  cudaMemcpyAsync(wfn, c.wfn_io, so * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc |= ST_CUDA;
+  return rc;
+}
+
+void h1itr_gen_cninv_(const int* icomp, const double* dtime, int* cnpiv, double* cninv) {
+  (void)cninv;
+  Ctx& c = ctx();
+  c.status |= h1_dropin_factor(*icomp, *dtime, mkc(0, 0), false, cnpiv);
+}
+
+void h1itr_prop_(const int* icomp, const int* isplit, const int* igauge, const int* iprojfc, const double* lfield,
+                 const double* dtime, const int* maxcyc, const double* thresh, const int* cnpiv, const double* cninv,
+                 double* wfn) {
+  (void)cninv;
+  Ctx& c = ctx();
+  c.status |= h1_dropin_prod(false, *isplit, *igauge, *icomp, *iprojfc, lfield, *dtime, mkc(0, 0), *maxcyc, *thresh,
+                             cnpiv, wfn);
+}
+
+void dpade_gen_(const int* icomp, const double* dtime, const double* alpha, double* tinv, int* tpiv) {
+  (void)tinv;
+  Ctx& c = ctx();
+  c.status |= h1_dropin_factor(*icomp, *dtime, mkc(alpha[0], alpha[1]), true, tpiv);
+}
+
+void dpade_prod_(const int* isplit, const int* igauge, const int* icomp, const int* iprojfc, const double* lfield,
+                 const double* dtime, const double* alpha, const int* maxcyc, const double* thresh, const int* tpiv,
+                 const double* tinv, double* wfn) {
+  (void)tinv;
+  Ctx& c = ctx();
+  c.status |= h1_dropin_prod(true, *isplit, *igauge, *icomp, *iprojfc, lfield, *dtime, mkc(alpha[0], alpha[1]), *maxcyc,
+                             *thresh, tpiv, wfn);
 }
 
 long td1c_gpu_launch_count(void) { return g ? g->launches : 0; }

@@ -183,4 +183,73 @@ int launch_ci_dvec(const CiArgs& a, int maxsec, cudaStream_t st);
 int launch_ci_rdm(const CiArgs& a, cudaStream_t st);
 int launch_ci_sigma(const CiArgs& a, int maxsec, cudaStream_t st);
 
+// ---- one-body propagators of the split schemes (h1prop.cu) ----------------
+// Condensed inverse of M_l = 1 + c T_l, l = 0..L1-1: per finite element the
+// inverse of the interior block and its couplings to the two bridge points,
+// per l the pivoted tridiagonal LU of the bridge Schur complement.
+struct H1Fac {
+  int nfe = 0, nd = 0, ni = 0, nb = 0, L1 = 0;  // ni = nd - 1 interior points, nb = nfe - 1 bridges
+  cplx* ainv = nullptr;  // [L1][nfe][ni][ni]: ainv[..][j][k] = (A_e^-1)(k, j)
+  cplx* gl = nullptr;    // [L1][nfe][ni]: A_e^-1 M(I_e, left bridge)
+  cplx* gr = nullptr;    // [L1][nfe][ni]: A_e^-1 M(I_e, right bridge)
+  cplx* vl = nullptr;    // [L1][nfe][ni]: M(left bridge, I_e)
+  cplx* vr = nullptr;    // [L1][nfe][ni]: M(right bridge, I_e)
+  cplx* tdl = nullptr;   // [L1][nb] tridiagonal factors: multipliers,
+  cplx* tdi = nullptr;   //   reciprocal pivots,
+  cplx* tdu = nullptr;   //   first and
+  cplx* tdu2 = nullptr;  //   second superdiagonal of U
+  int* tpiv = nullptr;   // [L1][nb] row interchanges
+};
+struct H1FacSrc {
+  int Nr, L1, nd, nfe;
+  cplx c;                // M = 1 + c T
+  const double* radk;    // (2nd+1) x (nrad+1) bands (l = 0 / l >= 1)
+  const double* radk0;
+  const double* tdiag;   // [L1][Nr] diagonal of T
+  int* status;           // ST_SINGULAR on a zero pivot
+};
+int launch_h1fac(const H1FacSrc& s, H1Fac& f, cudaStream_t st);
+
+// out = a in + b T in + (cz0 lfield[2]) V1 in for orbitals >= nfcore, afc in
+// below (orbitals f0 .. nfun-1); V1 the unit-field laser coupling of igauge
+struct H1OpArgs {
+  int Nr, L1, nd, nfun, nfcore, mmax1, igauge, f0;
+  const double* radk;
+  const double* radk0;
+  const double* radp;
+  const double* tdiag;
+  const double* xrad;
+  const double* alph;
+  const int* mval;
+  const double* lfield;  // device lfield(1:3,1:3) (may be null: no laser term)
+  cplx a, b, cz0, afc;
+  const cplx* in;
+  cplx* out;
+  const int* skip;       // when non-null and *skip != 0 the launch does nothing
+};
+int launch_h1op(const H1OpArgs& a, cudaStream_t st);
+size_t h1op_smem(int L1, int nd);
+
+// x = M_l^-1 in on the orbital columns fs0 .. nfun-1 (channels l < |m| pass
+// through); out = x and torb = x or += x on orbitals >= nfcore; the last CTA
+// sets *done = sqrt(sum |x|^2 / norm_div) < thresh
+struct H1SolveArgs {
+  H1Fac fac;
+  int Nr, L1, nfun, nfcore, fs0;
+  const int* mval;
+  const cplx* in;
+  cplx* out;             // may be null
+  cplx* torb;
+  int accumulate;
+  double thresh, norm_div;
+  double* partial;       // [L1 * column groups]
+  unsigned* ticket;      // zero between launches
+  int* done;
+  int* ncyc;             // cycles run (incremented by launches with check_skip)
+  int check_skip;        // the launch does nothing when *done != 0
+};
+int launch_h1solve(const H1SolveArgs& a, int CG, cudaStream_t st);
+int h1solve_pick_cg(int Nr, int nfe, int ni, int nb);
+int h1solve_groups(int ncol, int CG);
+
 }  // namespace td1c

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(32, 1) poisson_kernel(const __grid_constant__ 
   const int nb = (Nr + ND - 1) / ND, Np = nb * ND;
   const int p0 = blockIdx.y * PS_PAIRS;
   const int np = min(PS_PAIRS, a.npair - p0);
-  const int P = lane >> 1, c = lane & 1;
+  const int P = lane >> 1;
   bool active = P < np;
   if (active) {
     const int m = a.pair_m[p0 + P];

@@ -59,6 +59,7 @@ class HProd:
         self._check(lib.td1c_gpu_bind_bas(float(wl["znuc"]), int(wl.get("smul", 1)), int(wl.get("mtot", 0)),
                                           self.nfun, _ip(ot), _ip(mv), _ip(lv), int(wl["nela"]), int(wl["nelb"])))
         self._check(lib.td1c_gpu_bind_control(int(wl.get("icomp", 1)), int(wl["igauge"])))
+        self._check(lib.td1c_gpu_bind_split(int(wl.get("split_type", 0))))
         self.ene = np.zeros(8)
         projhigh = ctypes.c_bool(False)
         cutoff = ctypes.c_double(0.0)
@@ -155,6 +156,86 @@ class HProd:
         ene = np.zeros(max(1, int(ncyc)))
         self._check(self.lib.td1c_gpu_relax(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(dt), int(ncyc), _dp(ene)))
         return ene[: int(ncyc)]
+
+    # ---- one-body propagators of the split schemes (src/prop: clh1itr, cldpade)
+    def set_split(self, split_type):
+        """split_type of control_bind_: 0 full H in the RHS, 1 two-body part only, 2 h0 left out."""
+        self._check(self.lib.td1c_gpu_bind_split(int(split_type)))
+
+    def h1itr_dev(self, d_wfn, lfield, dtime, maxcyc=20, thresh=1e-10):
+        """h1itr_prop on a device state in place; returns the corrections added."""
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        n = ctypes.c_int(0)
+        self._check(self.lib.td1c_gpu_h1itr(ctypes.c_void_p(d_wfn), _dp(lf), float(dtime), int(maxcyc), float(thresh),
+                                            ctypes.byref(n)))
+        return n.value
+
+    def dpade_dev(self, d_wfn, lfield, dtime, alpha=2.0, maxcyc=20, thresh=1e-10):
+        """dpade_prod on a device state in place; returns the corrections added."""
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        a = complex(alpha)
+        n = ctypes.c_int(0)
+        self._check(self.lib.td1c_gpu_dpade(ctypes.c_void_p(d_wfn), _dp(lf), float(dtime), a.real, a.imag, int(maxcyc),
+                                            float(thresh), ctypes.byref(n)))
+        return n.value
+
+    def _prop_dev(self, fn, d_wfn, d_cic, t0, dt, nstep, maxcyc, thresh, use_graph):
+        wl = self.wl
+        self._check(fn(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(t0), float(dt), int(nstep), float(wl["fint"]),
+                       float(wl["wlen"]), float(wl["numcyc"]), float(wl.get("cep", 0.0)), int(maxcyc), float(thresh),
+                       1 if use_graph else 0))
+
+    def split2_dev(self, d_wfn, d_cic, t0, dt, nstep, maxcyc=20, thresh=1e-10, use_graph=True):
+        """tdse_split2 steps (h1itr over dt/2, RK4 over dt, h1itr over dt/2, mask) in place."""
+        self._prop_dev(self.lib.td1c_gpu_split2, d_wfn, d_cic, t0, dt, nstep, maxcyc, thresh, use_graph)
+
+    def etdrk2_dev(self, d_wfn, d_cic, t0, dt, nstep, maxcyc=20, thresh=1e-10, use_graph=True):
+        """ETD-RK2 steps with the Pade one-body inverse (cletdrk2 + cldpade, mask) in place."""
+        self._prop_dev(self.lib.td1c_gpu_etdrk2, d_wfn, d_cic, t0, dt, nstep, maxcyc, thresh, use_graph)
+
+    def relax_etdrk2_dev(self, d_wfn, d_cic, dt, ncyc, maxcyc=20, thresh=1e-10):
+        """Imaginary-time relaxation with ETD-RK2 steps (icomp = 0); returns the energy per cycle."""
+        ene = np.zeros(max(1, int(ncyc)))
+        self._check(self.lib.td1c_gpu_relax_etdrk2(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(dt), int(ncyc),
+                                                   int(maxcyc), float(thresh), _dp(ene)))
+        return ene[: int(ncyc)]
+
+    def h1itr_host(self, lfield, dtime, wfn, maxcyc=20, thresh=1e-10, split_type=1):
+        """clh1itr's Fortran calls through the drop-in symbols: h1itr_gen_cninv_ then
+        h1itr_prop_ on a host copy of wfn (returned)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        icomp, isplit, igauge, iprojfc = (ctypes.c_int(v) for v in (self.wl.get("icomp", 1), split_type,
+                                                                     self.wl["igauge"], 0))
+        dt, thr, mc = ctypes.c_double(dtime), ctypes.c_double(thresh), ctypes.c_int(maxcyc)
+        piv = np.zeros(4, dtype=np.int32)
+        band = np.zeros(2)
+        self.lib.h1itr_gen_cninv_(ctypes.byref(icomp), ctypes.byref(dt), _ip(piv), _dp(band))
+        self._status()
+        self.lib.h1itr_prop_(ctypes.byref(icomp), ctypes.byref(isplit), ctypes.byref(igauge), ctypes.byref(iprojfc),
+                             _dp(lf), ctypes.byref(dt), ctypes.byref(mc), ctypes.byref(thr), _ip(piv), _dp(band),
+                             _dp(wfn.view(np.float64)))
+        self._status()
+        return wfn
+
+    def dpade_host(self, lfield, dtime, wfn, alpha=2.0, maxcyc=20, thresh=1e-10, split_type=1):
+        """cldpade's Fortran calls through the drop-in symbols: dpade_gen_ then dpade_prod_
+        on a host copy of wfn (returned)."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128).copy()
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        icomp, isplit, igauge, iprojfc = (ctypes.c_int(v) for v in (self.wl.get("icomp", 1), split_type,
+                                                                     self.wl["igauge"], 0))
+        dt, thr, mc = ctypes.c_double(dtime), ctypes.c_double(thresh), ctypes.c_int(maxcyc)
+        al = np.array([complex(alpha).real, complex(alpha).imag])
+        piv = np.zeros(4, dtype=np.int32)
+        band = np.zeros(2)
+        self.lib.dpade_gen_(ctypes.byref(icomp), ctypes.byref(dt), _dp(al), _dp(band), _ip(piv))
+        self._status()
+        self.lib.dpade_prod_(ctypes.byref(isplit), ctypes.byref(igauge), ctypes.byref(icomp), ctypes.byref(iprojfc),
+                             _dp(lf), ctypes.byref(dt), _dp(al), ctypes.byref(mc), ctypes.byref(thr), _ip(piv), _dp(band),
+                             _dp(wfn.view(np.float64)))
+        self._status()
+        return wfn
 
     def rk4_reset(self, d_wfn0, d_cic0):
         self._check(self.lib.td1c_gpu_rk4_reset(ctypes.c_void_p(d_wfn0) if d_wfn0 else None,

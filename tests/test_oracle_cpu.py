@@ -13,7 +13,7 @@ import scipy.linalg as sl
 from oracle.oracle import Oracle
 from td1c_b200 import workloads as W
 
-from .helpers import oracle_state
+from .helpers import oracle_state, rel_err
 
 
 def band_to_dense(band, Nr, nd):
@@ -183,3 +183,85 @@ def test_imaginary_time_relaxation(base):
     w, c, e = o.relax(orb, cic, 2e-4, 25)
     assert np.all(np.diff(e) < 0), e
     assert abs(np.linalg.norm(c) - 1.0) < 1e-14
+
+
+def _dense_T(o, l):
+    d = o.dims
+    Nr, nd, L1 = d["nrad"] - 1, d["ndvr"], d["lmax1"] + 1
+    tm = o.get("tmat").reshape(L1, Nr, 2 * nd + 1)
+    return band_to_dense(tm[l], Nr, nd)
+
+
+@pytest.mark.parametrize("wl", [W.MIXED_SMALL, W.NE_SMALL], ids=lambda w: w["name"])
+def test_one_body_inverse_against_lapack(wl):
+    """dpade_prod with split_type 2 (no laser cycles) is (1 + i dt/2 T_l)^-1 per channel:
+    the oracle's ZGBTF2/ZGBTRS restatement against LAPACK ?gbsv through scipy."""
+    o = Oracle(dict(wl, split_type=2))
+    o.set_split(2)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    d = o.dims
+    Nr, nd, L1, nfc = d["nrad"] - 1, d["ndvr"], d["lmax1"] + 1, d["nfcore"]
+    mval = [x[2] for x in wl["orbitals"]]
+    nf = len(mval)
+    dt = 0.05
+    w2, ncorr = o.dpade_prod(np.zeros(9), dt, orb, alpha=2.0)
+    assert ncorr == 0
+    W0, W2 = orb.reshape(nf, L1, Nr), w2.reshape(nf, L1, Nr)
+    assert np.array_equal(W2[:nfc], W0[:nfc])
+    for l in range(L1):
+        M = np.eye(Nr) + 1j * dt / 2 * _dense_T(o, l).T
+        ab = np.zeros((2 * nd + 1, Nr), complex)
+        for i in range(Nr):
+            for j in range(max(0, i - nd), min(Nr, i + nd + 1)):
+                ab[nd + i - j, j] = M[i, j]
+        for f in range(nfc, nf):
+            if l < abs(mval[f]):
+                assert np.array_equal(W2[f, l], W0[f, l])
+                continue
+            x = sl.solve_banded((nd, nd), ab, W0[f, l])
+            assert np.abs(x - W2[f, l]).max() <= 1e-13 * np.abs(x).max()
+
+
+@pytest.mark.parametrize("wl", [W.MIXED_SMALL, W.LENGTH_SMALL], ids=lambda w: w["name"])
+def test_crank_nicolson_one_body_step(wl):
+    """h1itr_prop: without the laser the step is the Cayley form of exp(-i dt T), exactly
+    unitary; with the laser the correction cycles converge to the Cayley form of T + V
+    (unitary to the threshold) and stop once the correction norm is below it."""
+    o = Oracle(dict(wl, split_type=2))
+    o.set_split(2)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    nf = len(wl["orbitals"])
+    n0 = np.linalg.norm(orb.reshape(nf, -1), axis=1)
+    w, ncorr = o.h1itr_prop(np.zeros(9), 0.05, orb)
+    assert ncorr == 0
+    assert np.abs(np.linalg.norm(w.reshape(nf, -1), axis=1) - n0).max() < 1e-13
+    # backward step returns the state: (1 + i dt/2 T)(1 - i dt/2 T)^-1 inverts the Cayley map
+    wb, _ = o.h1itr_prop(np.zeros(9), -0.05, w)
+    assert rel_err(wb, orb) < 1e-13
+    o.set_split(1)
+    lf = np.zeros(9)
+    lf[2] = lf[8] = 1.5 if wl["igauge"] == 1 else 0.3
+    w1, n1 = o.h1itr_prop(lf, 0.05, orb, 30, 1e-12)
+    assert 3 <= n1 < 30
+    assert np.abs(np.linalg.norm(w1.reshape(nf, -1), axis=1) - n0).max() < 1e-10
+    wb, _ = o.h1itr_prop(lf, -0.05, w1, 30, 1e-12)
+    assert rel_err(wb, orb) < 1e-10
+
+
+def test_split_propagators_beyond_rk4_limit():
+    """split2 and ETD-RK2 stay bounded at dt = 0.05 on a grid where full-H RK4 needs dt < 1e-3."""
+    wl = dict(W.MIXED_SMALL, split_type=1)
+    o = Oracle(wl)
+    o.set_split(1)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    nf = len(wl["orbitals"])
+    for prop in (o.split2, o.etdrk2):
+        w, c, dip = prop(orb, cic, 10.0, 0.05, 20)
+        assert np.all(np.isfinite(w)) and np.all(np.isfinite(dip))
+        assert np.abs(np.linalg.norm(w.reshape(nf, -1), axis=1) - 1).max() < 0.3
+    o.set_split(0)
+    w, c, dip = o.rk4(orb, cic, 10.0, 0.05, 3)
+    assert not np.all(np.abs(w) < 10)  # full-H RK4 blows up at this step
