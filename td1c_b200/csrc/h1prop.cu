@@ -204,127 +204,369 @@ int launch_h1fac(const H1FacSrc& s, H1Fac& f, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// out = a in + b T in + (cz0 lfield[2]) V1 in for the orbitals f >= nfcore,
-// out = afc in below; V1 the unit-field laser coupling (hprod_zprod /
-// hprod_pzprod of the 'dyn' orbitals).  Same tiling as the one-body kernel:
-// one CTA per (orbital, 32-point radial tile), all l channels and a +-nd halo
-// in shared memory.
+// Application of M^-1 with the correction cycles, element by element.
+//
+// One pass of the element kernel, per (finite element e, chunk of LC l):
+//   1. x on the element's points (both bridges included) for l in the chunk
+//      and its l +- 1 halo: the input vector (first pass), or the previous
+//      correction finished from its interior part z and bridge values xb,
+//      x(I_e) = z_e - GL_e xb(left) - GR_e xb(right);
+//   2. finished corrections go to torb (= or +=) and into the residual norm;
+//      each point counted once: interior points and the element's left bridge;
+//   3. the next right-hand side  r = a x + b T x + cz V1 x  (V1 the unit-field
+//      laser coupling l <-> l +- 1, T the kinetic + nuclear band) on the
+//      element's points.  T and the radial derivative in V1 couple only the
+//      points of one element, so a bridge point gets each element's share
+//      from that element's CTA; its diagonal and point-local terms come from
+//      the element to its right (the bridge's owner);
+//   4. z_e = A_e^-1 r(I_e) and the bridge shares r(bridge) - v.z_e.
+// The bridge kernel, per l, adds the two shares of every bridge point and
+// solves the tridiagonal bridge system for xb.  Channels l < |m| pass
+// through (z = r, xb = r), as the reference skips their solve.  z is read
+// and written by the same pass (halo rows of the neighbouring chunks), so
+// consecutive passes alternate between two z buffers.
 // ---------------------------------------------------------------------------
-constexpr int H1O_TILE = 32;
+constexpr int H1E_NT = 256;
+constexpr int H1E_LC = 4;   // l channels per CTA
+constexpr int H1E_FG = 3;   // orbital groups of the interior solve
 
-__global__ void __launch_bounds__(256) h1op_kernel(H1OpArgs a) {
-  if (a.skip && *a.skip) return;
-  extern __shared__ double smem_d[];
-  const int Nr = a.Nr, L1 = a.L1, nd = a.nd, bw = 2 * nd + 1;
-  const int W = H1O_TILE + 2 * nd;
-  cplx* so = reinterpret_cast<cplx*>(smem_d);  // [L1][W]
-  cplx* sdw = so + (size_t)L1 * W;             // [L1][TILE] radial derivative
-  cplx* sh = sdw + (size_t)L1 * H1O_TILE;      // [L1][TILE] T in
-  double* sb = reinterpret_cast<double*>(sh + (size_t)L1 * H1O_TILE);  // [3][bw][TILE]
-  const int f = a.f0 + blockIdx.y;
-  const int r0 = blockIdx.x * H1O_TILE;
-  const cplx* __restrict__ in = a.in + (size_t)f * L1 * Nr;
-  cplx* __restrict__ out = a.out + (size_t)f * L1 * Nr;
-  if (f < a.nfcore) {
-    for (int e = threadIdx.x; e < L1 * H1O_TILE; e += blockDim.x) {
-      const int l = e / H1O_TILE, r = r0 + e % H1O_TILE;
-      if (r < Nr) out[(size_t)l * Nr + r] = cmul(a.afc, in[(size_t)l * Nr + r]);
+struct H1ElemSmem {
+  int np, nf, lh;  // points per element (nd + 1), orbitals, halo rows (LC + 2)
+  __host__ __device__ int ni() const { return np - 2; }
+  __host__ __device__ size_t x_off() const { return 0; }
+  __host__ __device__ size_t r_off() const { return x_off() + (size_t)nf * lh * np; }
+  __host__ __device__ size_t z_off() const { return r_off() + (size_t)nf * H1E_LC * np; }
+  __host__ __device__ size_t xb_off() const { return z_off() + (size_t)nf * H1E_LC * ni(); }
+  __host__ __device__ size_t g_off() const { return xb_off() + (size_t)nf * lh * 2; }
+  __host__ __device__ size_t v_off() const { return g_off() + (size_t)2 * lh * ni(); }
+  __host__ __device__ size_t ai_off() const { return v_off() + (size_t)2 * H1E_LC * ni(); }
+  __host__ __device__ size_t cplx_count() const { return ai_off() + (size_t)H1E_LC * ni() * ni(); }
+  __host__ __device__ size_t dbl_count() const { return (size_t)3 * np * np + 2 * np + (size_t)H1E_LC * np + (size_t)nf * lh; }
+  __host__ __device__ size_t bytes() const { return sizeof(cplx) * cplx_count() + sizeof(double) * dbl_count() + sizeof(int) * nf; }
+};
+
+// band value at (irad ip, irad iq), |ip - iq| <= nd, of a (2nd+1) x (nrad+1) table
+__device__ __forceinline__ double band_at(const double* band, int nd, int ip, int iq) {
+  return band[(size_t)(2 * nd + 1) * ip + nd + iq - ip];
+}
+
+template <int NDT>
+__global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
+  if (a.check_skip && *a.done) return;
+  extern __shared__ cplx sm[];
+  const H1Fac& F = a.fac;
+  const int nd = NDT > 0 ? NDT : F.nd;
+  const int np = nd + 1, ni = nd - 1, nfe = F.nfe, nb = F.nb, L1 = a.L1, Nr = a.Nr, nfun = a.nfun;
+  const int e = blockIdx.x, l0 = blockIdx.y * H1E_LC, lh = H1E_LC + 2;
+  const int tid = threadIdx.x;
+  const H1ElemSmem lay{np, nfun, lh};
+  cplx* X = sm + lay.x_off();     // [f][lh][np]  rows l0-1 .. l0+LC
+  cplx* R = sm + lay.r_off();     // [f][LC][np]
+  cplx* Z = sm + lay.z_off();     // [f][LC][ni]
+  cplx* XB = sm + lay.xb_off();   // [f][lh][2] bridge values left / right of the element
+  cplx* GLs = sm + lay.g_off();   // [lh][ni]
+  cplx* GRs = GLs + lh * ni;      // [lh][ni]
+  cplx* VLs = sm + lay.v_off();   // [LC][ni]
+  cplx* VRs = VLs + H1E_LC * ni;  // [LC][ni]
+  cplx* AI = sm + lay.ai_off();   // [LC][ni][ni], AI[lc][j][k] = (A_e^-1)(k, j)
+  double* Pb = reinterpret_cast<double*>(sm + lay.cplx_count());  // [np][np] derivative, off-diagonal
+  double* Tb0 = Pb + np * np;     // [np][np] kinetic off-diagonal, l = 0 (radk)
+  double* Tb1 = Tb0 + np * np;    // l >= 1 (radk0)
+  double* Pd = Tb1 + np * np;     // [np] derivative diagonal of owned points
+  double* Xr = Pd + np;           // [np] radial coordinate
+  double* TD = Xr + np;           // [LC][np] kinetic diagonal
+  double* AL = TD + H1E_LC * np;  // [f][lh] alpha_lm of l0-1 .. l0+LC
+  int* MV = reinterpret_cast<int*>(AL + (size_t)nfun * lh);  // [f] m
+  __shared__ double red[H1E_NT / 32];
+  __shared__ bool last;
+  const int ir0 = nd * e;  // irad of local point 0
+  const int f_lo = a.finalize ? min(a.f_fin, a.f_rhs) : a.f_rhs;
+  const size_t eb = (size_t)e * ni;
+  // 0. tables of the element and the chunk, loaded together
+  for (int q2 = tid; q2 < np * np; q2 += H1E_NT) {
+    const int p = q2 / np, q = q2 % np;
+    const int ip = ir0 + p, iq = ir0 + q;
+    double pv = 0.0, t0 = 0.0, t1 = 0.0;
+    if (p != q && ip >= 1 && ip <= Nr && iq >= 1 && iq <= Nr) {
+      pv = band_at(a.radp, nd, ip, iq);
+      t0 = band_at(a.radk, nd, ip, iq);
+      t1 = band_at(a.radk0, nd, ip, iq);
     }
-    return;
+    Pb[q2] = pv; Tb0[q2] = t0; Tb1[q2] = t1;
   }
-  for (int e = threadIdx.x; e < H1O_TILE * bw; e += blockDim.x) {
-    const int q = e / bw, jb = e % bw;
-    const int ir = r0 + q + 1;
-    double k0 = 0.0, k1 = 0.0, pp = 0.0;
-    if (ir <= Nr) {
-      const size_t o = (size_t)bw * ir + jb;
-      k0 = a.radk[o]; k1 = a.radk0[o]; pp = a.radp[o];
+  for (int p = tid; p < np; p += H1E_NT) {
+    const int ip = ir0 + p;
+    const bool ex = ip >= 1 && ip <= Nr;
+    Pd[p] = (ex && p != nd) ? band_at(a.radp, nd, ip, ip) : 0.0;
+    Xr[p] = ex ? a.xrad[ip] : 1.0;
+  }
+  for (int q2 = tid; q2 < H1E_LC * np; q2 += H1E_NT) {
+    const int lc = q2 / np, p = q2 % np, l = l0 + lc, ip = ir0 + p;
+    TD[q2] = (l < L1 && ip >= 1 && ip <= Nr) ? a.tdiag[(size_t)l * Nr + ip - 1] : 0.0;
+  }
+  for (int q2 = tid; q2 < nfun * lh; q2 += H1E_NT) {
+    const int f = q2 / lh, lq = q2 % lh, l = l0 - 1 + lq;
+    const int m = a.mval[f];
+    if (lq == 0) MV[f] = m;
+    AL[q2] = (l >= 0 && l < L1) ? a.alph[(size_t)(m + a.mmax1) * L1 + l] : 0.0;
+    cplx xl = mkc(0, 0), xr = mkc(0, 0);
+    if (a.finalize && f >= f_lo && l >= 0 && l < L1) {
+      const size_t row = (size_t)f * L1 + l;
+      if (e >= 1) xl = a.xb[row * nb + e - 1];
+      if (e + 1 < nfe) xr = a.xb[row * nb + e];
     }
-    const int d = jb * H1O_TILE + q;
-    sb[d] = k0; sb[H1O_TILE * bw + d] = k1; sb[2 * H1O_TILE * bw + d] = pp;
+    XB[2 * q2] = xl; XB[2 * q2 + 1] = xr;
   }
-  const int m = a.mval[f];
-  const int am = m < 0 ? -m : m;
-  for (int e = threadIdx.x; e < L1 * W; e += blockDim.x) {
-    const int l = e / W, q = e % W;
-    const int r = r0 - nd + q;
-    so[e] = (r >= 0 && r < Nr) ? in[(size_t)l * Nr + r] : mkc(0.0, 0.0);
+  if (a.finalize) {
+    for (int q2 = tid; q2 < lh * ni; q2 += H1E_NT) {
+      const int lq = q2 / ni, k = q2 % ni, l = l0 - 1 + lq;
+      const bool ok = l >= 0 && l < L1;
+      const size_t gi = (size_t)l * nfe * ni + eb + k;
+      GLs[q2] = ok ? F.gl[gi] : mkc(0, 0);
+      GRs[q2] = ok ? F.gr[gi] : mkc(0, 0);
+    }
+  }
+  if (a.make_rhs) {
+    for (int q2 = tid; q2 < H1E_LC * ni; q2 += H1E_NT) {
+      const int lc = q2 / ni, k = q2 % ni, l = l0 + lc;
+      const bool ok = l < L1;
+      const size_t vi = (size_t)l * nfe * ni + eb + k;
+      VLs[q2] = ok ? F.vl[vi] : mkc(0, 0);
+      VRs[q2] = ok ? F.vr[vi] : mkc(0, 0);
+    }
+    for (int q2 = tid; q2 < H1E_LC * ni * ni; q2 += H1E_NT) {
+      const int lc = q2 / (ni * ni), jk = q2 % (ni * ni), l = l0 + lc;
+      AI[q2] = l < L1 ? F.ainv[((size_t)l * nfe * ni + eb) * ni + jk] : mkc(0, 0);
+    }
   }
   __syncthreads();
-  const bool vel = a.igauge == 1;
-  const bool need_t = a.b.x != 0.0 || a.b.y != 0.0;
-  for (int e = threadIdx.x; e < L1 * H1O_TILE; e += blockDim.x) {
-    const int l = e / H1O_TILE, q = e % H1O_TILE;
-    const int r = r0 + q;
-    cplx hs = mkc(0.0, 0.0), ds = mkc(0.0, 0.0);
-    if (r < Nr && l >= am) {
-      const int ir = r + 1;
-      const int jll = max(1, ir - nd), jul = min(Nr, ir + nd);
-      const double* rk = sb + (l == 0 ? 0 : H1O_TILE * bw) + q;
-      const double* rp = sb + 2 * H1O_TILE * bw + q;
-      const double td = a.tdiag[(size_t)l * Nr + r];
-      const cplx* srow = so + (size_t)l * W + (nd + q);
-      for (int jr = jll; jr <= jul; ++jr) {
-        const int jb = nd + jr - ir;
-        const cplx w = srow[jr - ir];
-        if (need_t) {
-          const double t = (jr == ir) ? td : rk[jb * H1O_TILE];
-          hs.x = fma(w.x, t, hs.x); hs.y = fma(w.y, t, hs.y);
+  // 1. x on the element for l0-1 .. l0+LC
+#pragma unroll 4
+  for (int it = tid; it < nfun * lh * np; it += H1E_NT) {
+    const int f = it / (lh * np), lq = (it / np) % lh, p = it % np;
+    const int l = l0 - 1 + lq, ip = ir0 + p;
+    cplx x = mkc(0, 0);
+    if (f >= f_lo && l >= 0 && l < L1 && ip >= 1 && ip <= Nr) {
+      const size_t row = (size_t)f * L1 + l;
+      const cplx* xbr = XB + 2 * ((size_t)f * lh + lq);
+      if (!a.finalize) {
+        x = a.in[row * Nr + ip - 1];
+      } else if (p == 0) {
+        x = xbr[0];
+      } else if (p == nd) {
+        x = xbr[1];
+      } else {
+        const int k = p - 1;
+        const int m = MV[f];
+        x = a.z_in[row * nfe * ni + eb + k];
+        if (l >= (m < 0 ? -m : m)) {
+          x = csub(x, cmul(GLs[lq * ni + k], xbr[0]));
+          x = csub(x, cmul(GRs[lq * ni + k], xbr[1]));
         }
-        if (vel) { const double p = rp[jb * H1O_TILE]; ds.x = fma(w.x, p, ds.x); ds.y = fma(w.y, p, ds.y); }
       }
     }
-    sh[(size_t)l * H1O_TILE + q] = hs;
-    sdw[(size_t)l * H1O_TILE + q] = ds;
+    X[it] = x;
   }
   __syncthreads();
+  // 2. finished corrections: torb and the residual norm (owned points)
+  if (a.finalize) {
+    double nrm = 0.0;
+    for (int it = tid; it < nfun * H1E_LC * np; it += H1E_NT) {
+      const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC, p = it % np;
+      const int l = l0 + lc, ip = ir0 + p;
+      if (f < a.f_fin || l >= L1 || p == nd || ip < 1 || ip > Nr) continue;
+      const cplx x = X[((size_t)f * lh + lc + 1) * np + p];
+      nrm += cabs2(x);
+      if (f >= a.nfcore) {
+        const size_t gi = ((size_t)f * L1 + l) * Nr + ip - 1;
+        a.torb[gi] = a.accumulate ? cadd(a.torb[gi], x) : x;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    if ((tid & 31) == 0) red[tid >> 5] = nrm;
+  }
+  // 3. right-hand side r = a x + b T x + cz V1 x on the element's points
   const double zf = a.lfield ? a.lfield[2] : 0.0;
   const cplx cz = mkc(a.cz0.x * zf, a.cz0.y * zf);
-  const double* __restrict__ al = a.alph + (size_t)(m + a.mmax1) * L1;
-  for (int e = threadIdx.x; e < L1 * H1O_TILE; e += blockDim.x) {
-    const int l = e / H1O_TILE, q = e % H1O_TILE;
-    const int r = r0 + q;
-    if (r >= Nr) continue;
-    const double x = a.xrad[r + 1];
-    const cplx* sc = so + nd + q;  // sc[l * W] = in(r, l)
-    cplx h = mkc(0.0, 0.0);
-    if (vel) {  // unit-field velocity-gauge coupling (hprod_pzprod.F90:114-213)
-      if (l - 1 >= am) {
-        const double alp = al[l - 1];
-        const double t1 = -alp, t2 = (-alp * (double)l) / x;
-        const cplx dwv = sdw[(size_t)(l - 1) * H1O_TILE + q], wv = sc[(size_t)(l - 1) * W];
-        h.x = h.x - dwv.y * t1; h.y = h.y + dwv.x * t1;
-        h.x = h.x + wv.y * t2;  h.y = h.y - wv.x * t2;
+  const bool do_t = a.b.x != 0.0 || a.b.y != 0.0;
+  const bool do_v = cz.x != 0.0 || cz.y != 0.0;
+  const bool vel = a.igauge == 1;
+  if (a.make_rhs) {
+    for (int it = tid; it < nfun * H1E_LC * np; it += H1E_NT) {
+      const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC, p = it % np;
+      const int l = l0 + lc, ip = ir0 + p;
+      if (f < a.f_rhs || l >= L1) continue;
+      cplx r = mkc(0, 0);
+      if (ip >= 1 && ip <= Nr) {
+        const int m = MV[f], am = m < 0 ? -m : m;
+        const bool owner = p != nd;       // the right bridge belongs to the next element
+        const bool dyn = f >= a.nfcore;   // frozen-core rows take the a-term only
+        const cplx* xl = X + ((size_t)f * lh + lc + 1) * np;  // x(l, .)
+        if (owner) r = cmul(a.a, xl[p]);
+        if (do_t && dyn && l >= am) {
+          const double* tb = (l == 0 ? Tb0 : Tb1) + p * np;
+          cplx t = mkc(0, 0);
+          for (int q = 0; q < np; ++q) { t.x = fma(tb[q], xl[q].x, t.x); t.y = fma(tb[q], xl[q].y, t.y); }
+          if (owner) {
+            const double d = TD[lc * np + p];
+            t.x = fma(d, xl[p].x, t.x); t.y = fma(d, xl[p].y, t.y);
+          }
+          cfma(r, a.b, t);
+        }
+        if (do_v && dyn) {
+          const double* alq = AL + (size_t)f * lh;  // alq[lq] = alpha(l0 - 1 + lq)
+          const double xr = Xr[p];
+          cplx h = mkc(0, 0);
+          for (int side = 0; side < 2; ++side) {
+            // side 0: coupling from l-1 (l-1 >= |m|); side 1: from l+1 (l >= |m|, l+1 < L1)
+            if (side == 0 ? (l - 1 < am) : (l < am || l + 1 >= L1)) continue;
+            const double alp = side == 0 ? alq[lc] : alq[lc + 1];
+            const cplx* xs = X + ((size_t)f * lh + lc + (side == 0 ? 0 : 2)) * np;
+            if (vel) {
+              // -i alpha (d/dr x_s) (this element's share) and -/+ i alpha (l_s/r) x_s (owner)
+              const double* pr = Pb + p * np;
+              cplx dw = mkc(0, 0);
+              for (int q = 0; q < np; ++q) { dw.x = fma(pr[q], xs[q].x, dw.x); dw.y = fma(pr[q], xs[q].y, dw.y); }
+              dw.x = fma(Pd[p], xs[p].x, dw.x); dw.y = fma(Pd[p], xs[p].y, dw.y);
+              const double t1 = -alp;
+              h.x = h.x - dw.y * t1; h.y = h.y + dw.x * t1;
+              if (owner) {
+                const double t2 = side == 0 ? (-alp * (double)l) / xr : (-alp * (double)(l + 1)) / xr;
+                const cplx wv = xs[p];
+                if (side == 0) { h.x = h.x + wv.y * t2; h.y = h.y - wv.x * t2; }
+                else { h.x = h.x - wv.y * t2; h.y = h.y + wv.x * t2; }
+              }
+            } else if (owner) {
+              const double t = xr * alp;
+              h.x = fma(xs[p].x, t, h.x); h.y = fma(xs[p].y, t, h.y);
+            }
+          }
+          cfma(r, cz, h);
+        }
       }
-      if (l >= am && l <= L1 - 2) {
-        const double alp = al[l];
-        const double t1 = -alp, t2 = (-alp * (double)(l + 1)) / x;
-        const cplx dwv = sdw[(size_t)(l + 1) * H1O_TILE + q], wv = sc[(size_t)(l + 1) * W];
-        h.x = h.x - dwv.y * t1; h.y = h.y + dwv.x * t1;
-        h.x = h.x - wv.y * t2;  h.y = h.y + wv.x * t2;
-      }
-    } else {  // unit-field length-gauge coupling (hprod_zprod.F90:108-135)
-      if (l - 1 >= am) {
-        const double t = x * al[l - 1];
-        const cplx wv = sc[(size_t)(l - 1) * W];
-        h.x = fma(wv.x, t, h.x); h.y = fma(wv.y, t, h.y);
-      }
-      if (l >= am && l <= L1 - 2) {
-        const double t = x * al[l];
-        const cplx wv = sc[(size_t)(l + 1) * W];
-        h.x = fma(wv.x, t, h.x); h.y = fma(wv.y, t, h.y);
+      R[it] = r;
+    }
+  }
+  __syncthreads();
+  if (a.make_rhs) {
+    // 4. z_e = A_e^-1 r(I_e): thread per (l, k, orbital group)
+    for (int it = tid; it < H1E_LC * ni * H1E_FG; it += H1E_NT) {
+      const int g = it / (H1E_LC * ni), lc = (it / ni) % H1E_LC, k = it % ni;
+      const int l = l0 + lc;
+      if (l >= L1) continue;
+      const cplx* av = AI + (size_t)lc * ni * ni + k;  // av[j * ni] = Ainv(k, j)
+      for (int f = a.f_rhs + g; f < nfun; f += H1E_FG) {
+        const int m = MV[f];
+        const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np + 1;
+        cplx zv;
+        if (l < (m < 0 ? -m : m)) {
+          zv = rf[k];
+        } else {
+          zv = mkc(0, 0);
+#pragma unroll
+          for (int j = 0; j < (NDT > 0 ? NDT - 1 : 0); ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
+          for (int j = (NDT > 0 ? NDT - 1 : 0); j < ni; ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
+        }
+        Z[((size_t)f * H1E_LC + lc) * ni + k] = zv;
+        a.z_out[((size_t)f * L1 + l) * nfe * ni + eb + k] = zv;
       }
     }
-    cplx o = cmul(a.a, sc[(size_t)l * W]);
-    cfma(o, a.b, sh[(size_t)l * H1O_TILE + q]);
-    cfma(o, cz, h);
-    out[(size_t)l * Nr + r] = o;
+    __syncthreads();
+    // bridge shares: left (e >= 1) r(0) - vL.z, right (e < nfe - 1) r(nd) - vR.z
+    for (int it = tid; it < nfun * H1E_LC * 2; it += H1E_NT) {
+      const int f = it / (H1E_LC * 2), lc = (it / 2) % H1E_LC, side = it % 2;
+      const int l = l0 + lc;
+      if (f < a.f_rhs || l >= L1) continue;
+      if (side == 0 ? e < 1 : e + 1 >= nfe) continue;
+      const int m = MV[f];
+      const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np;
+      cplx c = side == 0 ? rf[0] : rf[nd];
+      if (l >= (m < 0 ? -m : m)) {
+        const cplx* v = (side == 0 ? VLs : VRs) + (size_t)lc * ni;
+        const cplx* zr = Z + ((size_t)f * H1E_LC + lc) * ni;
+        cplx s = mkc(0, 0);
+        for (int k = 0; k < ni; ++k) cfma(s, v[k], zr[k]);
+        c = csub(c, s);
+      }
+      a.cb[(((size_t)f * L1 + l) * nfe + e) * 2 + side] = c;
+    }
+  }
+  // residual norm of the finished corrections: the last CTA decides
+  if (a.finalize && a.do_norm) {
+    const int nblk = gridDim.x * gridDim.y;
+    if (tid == 0) {
+      double s = 0.0;
+      for (int w = 0; w < H1E_NT / 32; ++w) s += red[w];
+      a.partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+      __threadfence();
+      last = atomicAdd(a.ticket, 1u) == (unsigned)(nblk - 1);
+    }
+    __syncthreads();
+    if (last && tid < 32) {
+      __threadfence();
+      double s = 0.0;
+      for (int b = tid; b < nblk; b += 32) s += __ldcg(a.partial + b);
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (tid == 0) {
+        *a.done = sqrt(s / a.norm_div) < a.thresh ? 1 : 0;
+        *a.ticket = 0u;
+      }
+    }
   }
 }
 
-size_t h1op_smem(int L1, int nd) {
-  const int W = H1O_TILE + 2 * nd;
-  return sizeof(cplx) * ((size_t)L1 * W + 2 * (size_t)L1 * H1O_TILE) + sizeof(double) * 3 * H1O_TILE * (2 * nd + 1);
+// per l: bridge right-hand sides from the two element shares, then the
+// pivoted tridiagonal solve (ZGTTRS algorithm) for every orbital column
+constexpr int H1B_NT = 256;
+
+__global__ void __launch_bounds__(H1B_NT) h1bridge_kernel(H1ElemArgs a) {
+  if (a.check_skip && *a.done) return;
+  extern __shared__ cplx sb2[];
+  const H1Fac& F = a.fac;
+  const int l = blockIdx.x, nb = F.nb, nfe = F.nfe, L1 = a.L1, nfun = a.nfun, tid = threadIdx.x;
+  if (nb <= 0) return;
+  cplx* dl = sb2;
+  cplx* di = dl + nb;
+  cplx* du = di + nb;
+  cplx* du2 = du + nb;
+  cplx* g = du2 + nb;  // [nfun][nb]
+  int* ip = reinterpret_cast<int*>(g + (size_t)nfun * nb);
+  for (int q = tid; q < nb; q += H1B_NT) {
+    const size_t o = (size_t)l * nb + q;
+    dl[q] = F.tdl[o]; di[q] = F.tdi[o]; du[q] = F.tdu[o]; du2[q] = F.tdu2[o]; ip[q] = F.tpiv[o];
+  }
+  for (int it = tid; it < nfun * nb; it += H1B_NT) {
+    const int f = it / nb, b = it % nb;
+    if (f < a.f_rhs) continue;
+    const size_t c0 = ((size_t)f * L1 + l) * nfe;
+    g[it] = cadd(a.cb[(c0 + b) * 2 + 1], a.cb[(c0 + b + 1) * 2 + 0]);
+  }
+  __syncthreads();
+  if (tid == 0 && l == 0 && a.ncyc && a.check_skip) atomicAdd(a.ncyc, 1);
+  const int f = a.f_rhs + tid;
+  if (f >= nfun) return;
+  const int m = a.mval[f];
+  cplx* x = g + (size_t)f * nb;
+  if (l >= (m < 0 ? -m : m)) {
+    for (int i = 0; i + 1 < nb; ++i) {
+      const cplx bi = x[i], bn = x[i + 1];
+      if (ip[i] == i) {
+        x[i + 1] = csub(bn, cmul(dl[i], bi));
+      } else {
+        x[i] = bn;
+        x[i + 1] = csub(bi, cmul(dl[i], bn));
+      }
+    }
+    x[nb - 1] = cmul(x[nb - 1], di[nb - 1]);
+    if (nb > 1) x[nb - 2] = cmul(csub(x[nb - 2], cmul(du[nb - 2], x[nb - 1])), di[nb - 2]);
+    for (int i = nb - 3; i >= 0; --i) {
+      cplx v = csub(x[i], cmul(du[i], x[i + 1]));
+      v = csub(v, cmul(du2[i], x[i + 2]));
+      x[i] = cmul(v, di[i]);
+    }
+  }
+  cplx* out = a.xb + ((size_t)f * L1 + l) * nb;
+  for (int b = 0; b < nb; ++b) out[b] = x[b];
 }
 
 // raise a kernel's dynamic shared memory limit to at least smem (once per size)
@@ -337,213 +579,39 @@ int ensure_smem(K kernel, size_t smem, size_t& cur) {
   return 0;
 }
 
-int launch_h1op(const H1OpArgs& a, cudaStream_t st) {
-  const size_t smem = h1op_smem(a.L1, a.nd);
+size_t h1elem_smem(int nd, int nfun) { return H1ElemSmem{nd + 1, nfun, H1E_LC + 2}.bytes(); }
+
+template <int NDT>
+int launch_h1elem_t(const H1ElemArgs& a, cudaStream_t st) {
   static size_t cur = 0;
-  if (smem > 227 * 1024) return ST_CONFIG;
-  if (int e = ensure_smem(h1op_kernel, smem, cur)) return e;
-  if (a.nfun - a.f0 <= 0) return 0;
-  dim3 grid((a.Nr + H1O_TILE - 1) / H1O_TILE, a.nfun - a.f0);
-  h1op_kernel<<<grid, 256, smem, st>>>(a);
+  const size_t smem = h1elem_smem(a.fac.nd, a.nfun);
+  if (smem > 220 * 1024) return ST_CONFIG;
+  if (int e = ensure_smem(h1elem_kernel<NDT>, smem, cur)) return e;
+  dim3 grid(a.fac.nfe, (a.L1 + H1E_LC - 1) / H1E_LC);
+  h1elem_kernel<NDT><<<grid, H1E_NT, smem, st>>>(a);
   return (int)cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// x = M_l^-1 b for CG orbital columns of one l per CTA (steps 1-4 above),
-// then out = x, torb = x or torb += x (orbitals >= nfcore), and the residual
-// norm of the columns; the last CTA to finish sets *done = (rms < thresh).
-// ---------------------------------------------------------------------------
-constexpr int H1S_NT = 256;
-
-template <int CG>
-__global__ void __launch_bounds__(H1S_NT) h1solve_kernel(H1SolveArgs a) {
-  if (a.check_skip && *a.done) return;
-  extern __shared__ cplx s1[];
-  const H1Fac& F = a.fac;
-  const int Nr = a.Nr, l = blockIdx.x, ni = F.ni, nd = F.nd, nfe = F.nfe, nb = F.nb, L1 = a.L1;
-  const int nint = nfe * ni;
-  cplx* fr = s1;                       // [CG][Nr] right-hand side, then x
-  cplx* zs = fr + (size_t)CG * Nr;     // [CG][nint] interior solutions z
-  cplx* tb = zs + (size_t)CG * nint;   // [4][nb] dl, 1/d, du, du2 of channel l
-  int* tp = reinterpret_cast<int*>(tb + 4 * (size_t)(nb > 0 ? nb : 1));  // [nb]
-  __shared__ double red[H1S_NT / 32];
-  __shared__ int col_f[CG], col_solve[CG];
-  __shared__ bool last;
-  const int tid = threadIdx.x;
-  if (tid < CG) {
-    const int fo = a.fs0 + blockIdx.y * CG + tid;
-    int fv = -1, sv = 0;
-    if (fo < a.nfun) {
-      fv = fo;
-      const int m = a.mval[fo];
-      sv = l >= (m < 0 ? -m : m);  // channels l < |m| pass through (the reference skips the solve)
-    }
-    col_f[tid] = fv;
-    col_solve[tid] = sv;
-  }
-  for (int q = tid; q < nb; q += H1S_NT) {
-    const size_t o = (size_t)l * nb + q;
-    tb[q] = F.tdl[o]; tb[nb + q] = F.tdi[o]; tb[2 * nb + q] = F.tdu[o]; tb[3 * nb + q] = F.tdu2[o];
-    tp[q] = F.tpiv[o];
-  }
-  __syncthreads();
-  for (int c = 0; c < CG; ++c) {
-    const int fo = col_f[c];
-    if (fo < 0) continue;
-    const cplx* src = a.in + ((size_t)fo * L1 + l) * Nr;
-    for (int r = tid; r < Nr; r += H1S_NT) fr[(size_t)c * Nr + r] = src[r];
-  }
-  __syncthreads();
-  const size_t eb = (size_t)l * nfe * ni;
-  // 1. z_e = A_e^-1 b(I_e)
-  for (int it = tid; it < nint; it += H1S_NT) {
-    const int e = it / ni, k = it % ni;
-    const cplx* av = F.ainv + (eb + (size_t)e * ni) * ni + k;  // av[j * ni] = Ainv(k, j)
-    cplx acc[CG];
-#pragma unroll
-    for (int c = 0; c < CG; ++c) acc[c] = mkc(0, 0);
-    for (int j = 0; j < ni; ++j) {
-      const cplx av_j = av[(size_t)j * ni];
-#pragma unroll
-      for (int c = 0; c < CG; ++c) cfma(acc[c], av_j, fr[(size_t)c * Nr + nd * e + j]);
-    }
-#pragma unroll
-    for (int c = 0; c < CG; ++c) zs[(size_t)c * nint + it] = acc[c];
-  }
-  __syncthreads();
-  // 2. bridge right-hand sides g = b(B) - M(B, I) z
-  for (int it = tid; it < nb * CG; it += H1S_NT) {
-    const int bb = it % nb, c = it / nb;
-    if (!col_solve[c]) continue;
-    const cplx* vr = F.vr + eb + (size_t)bb * ni;
-    const cplx* vl = F.vl + eb + (size_t)(bb + 1) * ni;
-    const cplx* zl = zs + (size_t)c * nint + (size_t)bb * ni;
-    const cplx* zr = zl + ni;
-    cplx s = mkc(0, 0);
-    for (int j = 0; j < ni; ++j) { cfma(s, vr[j], zl[j]); cfma(s, vl[j], zr[j]); }
-    cplx* g = fr + (size_t)c * Nr + nd * (bb + 1) - 1;
-    *g = csub(*g, s);
-  }
-  __syncthreads();
-  // 3. S x(B) = g (ZGTTRS algorithm on the factored tridiagonal)
-  if (tid < CG && col_solve[tid] && nb > 0) {
-    cplx* g = fr + (size_t)tid * Nr + nd - 1;  // g[nd * bb] = bridge bb
-    const cplx *dl = tb, *di = tb + nb, *du = tb + 2 * nb, *du2 = tb + 3 * nb;
-    for (int i = 0; i + 1 < nb; ++i) {
-      const cplx bi = g[(size_t)nd * i], bn = g[(size_t)nd * (i + 1)];
-      if (tp[i] == i) {
-        g[(size_t)nd * (i + 1)] = csub(bn, cmul(dl[i], bi));
-      } else {
-        g[(size_t)nd * i] = bn;
-        g[(size_t)nd * (i + 1)] = csub(bi, cmul(dl[i], bn));
-      }
-    }
-    g[(size_t)nd * (nb - 1)] = cmul(g[(size_t)nd * (nb - 1)], di[nb - 1]);
-    if (nb > 1) {
-      const int i = nb - 2;
-      g[(size_t)nd * i] = cmul(csub(g[(size_t)nd * i], cmul(du[i], g[(size_t)nd * (i + 1)])), di[i]);
-    }
-    for (int i = nb - 3; i >= 0; --i) {
-      cplx v = csub(g[(size_t)nd * i], cmul(du[i], g[(size_t)nd * (i + 1)]));
-      v = csub(v, cmul(du2[i], g[(size_t)nd * (i + 2)]));
-      g[(size_t)nd * i] = cmul(v, di[i]);
-    }
-  }
-  __syncthreads();
-  // 4. x(I_e) = z_e - GL_e x(left bridge) - GR_e x(right bridge)
-  for (int it = tid; it < nint * CG; it += H1S_NT) {
-    const int c = it / nint, q = it % nint;
-    if (!col_solve[c]) continue;
-    const int e = q / ni, k = q % ni;
-    cplx x = zs[(size_t)c * nint + q];
-    const cplx* frc = fr + (size_t)c * Nr;
-    if (e >= 1) x = csub(x, cmul(F.gl[eb + q], frc[nd * e - 1]));
-    if (e + 1 < nfe) x = csub(x, cmul(F.gr[eb + q], frc[nd * (e + 1) - 1]));
-    fr[(size_t)c * Nr + nd * e + k] = x;
-  }
-  __syncthreads();
-  // write-out and residual norm
-  double nrm = 0.0;
-  for (int c = 0; c < CG; ++c) {
-    const int fo = col_f[c];
-    if (fo < 0) continue;
-    const size_t row = ((size_t)fo * L1 + l) * Nr;
-    const bool dyn = fo >= a.nfcore;
-    for (int r = tid; r < Nr; r += H1S_NT) {
-      const cplx x = fr[(size_t)c * Nr + r];
-      nrm += cabs2(x);
-      if (dyn) {
-        if (a.out) a.out[row + r] = x;
-        a.torb[row + r] = a.accumulate ? cadd(a.torb[row + r], x) : x;
-      }
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-  if ((tid & 31) == 0) red[tid >> 5] = nrm;
-  __syncthreads();
-  const int nblk = gridDim.x * gridDim.y;
-  if (tid == 0) {
-    double s = 0.0;
-    for (int w = 0; w < H1S_NT / 32; ++w) s += red[w];
-    a.partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
-    __threadfence();
-    last = atomicAdd(a.ticket, 1u) == (unsigned)(nblk - 1);
-  }
-  __syncthreads();
-  if (last && tid < 32) {
-    __threadfence();
-    double s = 0.0;
-    for (int b = tid; b < nblk; b += 32) s += __ldcg(a.partial + b);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (tid == 0) {
-      const double rms = sqrt(s / a.norm_div);
-      *a.done = rms < a.thresh ? 1 : 0;
-      if (a.ncyc && a.check_skip) *a.ncyc += 1;
-      *a.ticket = 0u;
-    }
+int launch_h1elem(const H1ElemArgs& a, cudaStream_t st) {
+  switch (a.fac.nd) {  // 21-, 9- and 8-point Lobatto elements get the unrolled inverse rows
+    case 20: return launch_h1elem_t<20>(a, st);
+    case 8: return launch_h1elem_t<8>(a, st);
+    case 7: return launch_h1elem_t<7>(a, st);
+    default: return launch_h1elem_t<0>(a, st);
   }
 }
 
-size_t h1solve_smem(int CG, int Nr, int nfe, int ni, int nb) {
-  const int nbp = nb > 0 ? nb : 1;
-  return sizeof(cplx) * ((size_t)CG * Nr + (size_t)CG * nfe * ni + 4 * (size_t)nbp) + sizeof(int) * nbp;
-}
-
-int h1solve_groups(int ncol, int CG) { return (ncol + CG - 1) / CG; }
-
-int launch_h1solve(const H1SolveArgs& a, int CG, cudaStream_t st) {
-  const H1Fac& F = a.fac;
-  const int ncol = a.nfun - a.fs0;
-  if (ncol <= 0) return 0;
-  const size_t smem = h1solve_smem(CG, a.Nr, F.nfe, F.ni, F.nb);
-  if (smem > 226 * 1024) return ST_CONFIG;
-  dim3 grid(a.L1, h1solve_groups(ncol, CG));
-  static size_t cur[3] = {0, 0, 0};
-  switch (CG) {
-    case 1:
-      if (int e = ensure_smem(h1solve_kernel<1>, smem, cur[0])) return e;
-      h1solve_kernel<1><<<grid, H1S_NT, smem, st>>>(a);
-      break;
-    case 2:
-      if (int e = ensure_smem(h1solve_kernel<2>, smem, cur[1])) return e;
-      h1solve_kernel<2><<<grid, H1S_NT, smem, st>>>(a);
-      break;
-    case 4:
-      if (int e = ensure_smem(h1solve_kernel<4>, smem, cur[2])) return e;
-      h1solve_kernel<4><<<grid, H1S_NT, smem, st>>>(a);
-      break;
-    default:
-      return ST_CONFIG;
-  }
+int launch_h1bridge(const H1ElemArgs& a, cudaStream_t st) {
+  if (a.fac.nb <= 0) return 0;
+  if (a.nfun - a.f_rhs > H1B_NT) return ST_CONFIG;
+  const size_t smem = sizeof(cplx) * (size_t)a.fac.nb * (4 + a.nfun) + sizeof(int) * a.fac.nb;
+  static size_t cur = 0;
+  if (smem > 220 * 1024) return ST_CONFIG;
+  if (int e = ensure_smem(h1bridge_kernel, smem, cur)) return e;
+  h1bridge_kernel<<<a.L1, H1B_NT, smem, st>>>(a);
   return (int)cudaGetLastError();
 }
 
-// the largest column group (4, 2, 1) whose shared memory fits one CTA (the
-// kernel's static arrays take well under 1 KB of the 227 KB)
-int h1solve_pick_cg(int Nr, int nfe, int ni, int nb) {
-  for (int cg : {4, 2, 1})
-    if (h1solve_smem(cg, Nr, nfe, ni, nb) <= 226 * 1024) return cg;
-  return 0;
-}
+size_t h1elem_partials(int nfe, int L1) { return (size_t)nfe * ((L1 + H1E_LC - 1) / H1E_LC); }
 
 }  // namespace td1c

@@ -141,11 +141,11 @@ struct Ctx {
   struct H1Slot { double cre = 0, cim = 0; H1Fac f; };
   H1Slot h1slot[4];
   int n_h1 = 0;
-  cplx *h1_orb = nullptr, *h1_horb = nullptr;  // correction and laser product [nbas * nfun]
+  cplx* h1_z[2] = {nullptr, nullptr};  // interior solutions (alternating passes)
+  cplx *h1_cb = nullptr, *h1_xb = nullptr;  // bridge shares, bridge values
   double* h1_partial = nullptr;
   unsigned* h1_ticket = nullptr;
   int* h1_flags = nullptr;  // [0] done, [1] cycles of the last application
-  int h1_cg = 0;
   // phase timing (off during graph capture)
   bool profile = false;
   cudaEvent_t ev[16] = {};
@@ -1394,6 +1394,7 @@ struct RkBufs {
   const void* s_tab[2] = {nullptr, nullptr}; double s_dt[2] = {0, 0}; int s_cyc[2] = {0, 0}; double s_thr[2] = {0, 0};
   int s_split[2] = {-1, -1}; int s_mask[2] = {-1, -1}; long s_per[2] = {0, 0};
   const void* s_ro[2] = {nullptr, nullptr};
+  int g_ctl = -1, s_ctl[2] = {-1, -1};  // control flags (icomp, igauge) the graphs were captured with
 };
 RkBufs g_rk;
 
@@ -1433,13 +1434,14 @@ int h1_factor(Ctx& c, cplx fac, H1Fac* out) {
 }
 
 int h1_bufs(Ctx& c) {
-  if (c.h1_orb) return 0;
-  const size_t so = c.nbas * c.nfun;
-  c.h1_orb = dalloc<cplx>(so);
-  c.h1_horb = dalloc<cplx>(so);
-  c.h1_cg = h1solve_pick_cg(c.Nr, c.nfe, c.nd - 1, c.nfe - 1);
-  if (c.h1_cg == 0 || h1op_smem(c.L1, c.nd) > 227 * 1024) return ST_CONFIG;
-  c.h1_partial = dalloc<double>((size_t)c.L1 * h1solve_groups(c.nfun, c.h1_cg));
+  if (c.h1_z[0]) return 0;
+  const size_t nrow = (size_t)c.nfun * c.L1;
+  if (c.nfun - c.nfcore > 64 || h1elem_smem(c.nd, c.nfun) > 220 * 1024) return ST_CONFIG;
+  c.h1_z[0] = dalloc<cplx>(nrow * c.nfe * (c.nd - 1));
+  c.h1_z[1] = dalloc<cplx>(nrow * c.nfe * (c.nd - 1));
+  c.h1_cb = dalloc<cplx>(nrow * c.nfe * 2);
+  c.h1_xb = dalloc<cplx>(nrow * std::max(1, c.nfe - 1));
+  c.h1_partial = dalloc<double>(h1elem_partials(c.nfe, c.L1));
   c.h1_ticket = dalloc<unsigned>(1);  // zero (dalloc clears)
   c.h1_flags = dalloc<int>(2);
   return 0;
@@ -1449,8 +1451,10 @@ int h1_bufs(Ctx& c) {
 // Crank-Nicolson factor 1 + (i dtime / 2) T; pade = true: dpade_prod
 // (dpade_prod.F90:2-124), (1 + (i dtime / alpha) (T + V))^-1.  Imaginary
 // time (icomp = 0) drops the i.  d_lf: device lfield of the call.  The
-// non-frozen orbitals of wfn are replaced; launches are fixed in number
-// (maxcyc correction cycles, skipped on the device once converged).
+// non-frozen orbitals of wfn are replaced.  Launches are fixed in number: a
+// first element pass and bridge solve, maxcyc correction cycles (element +
+// bridge pass, skipped on the device once the residual norm is below thresh)
+// and a last pass that adds the final correction.
 int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cplx alpha, int maxcyc, double thresh) {
   cudaStream_t st = c.st;
   int rc = h1_bufs(c);
@@ -1469,37 +1473,48 @@ int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cpl
   H1Fac F;
   rc = h1_factor(c, fac, &F);
   if (rc) return rc;
-  H1OpArgs op{};
-  op.Nr = c.Nr; op.L1 = c.L1; op.nd = c.nd; op.nfun = c.nfun; op.nfcore = c.nfcore; op.mmax1 = c.mmax1;
-  op.igauge = c.igauge; op.radk = c.radk; op.radk0 = c.radk0; op.radp = c.radp; op.tdiag = c.tdiag; op.xrad = c.xrad;
-  op.alph = c.alph; op.mval = c.d_mval; op.lfield = d_lf;
-  H1SolveArgs sv{};
-  sv.fac = F; sv.Nr = c.Nr; sv.L1 = c.L1; sv.nfun = c.nfun; sv.nfcore = c.nfcore; sv.mval = c.d_mval;
-  sv.thresh = thresh; sv.norm_div = (double)c.nfun; sv.partial = c.h1_partial; sv.ticket = c.h1_ticket;
-  sv.done = c.h1_flags; sv.ncyc = c.h1_flags + 1;
-  cudaMemsetAsync(c.h1_flags + 1, 0, sizeof(int), st);
-  if (!pade) {
-    // orb = wfn + zfac1 (T + [zfield V]) wfn on the non-frozen orbitals, then M^-1 on all
-    op.f0 = 0; op.a = mkc(1, 0); op.b = zf0; op.cz0 = c.isplit == 1 ? zf0 : mkc(0, 0); op.afc = mkc(1, 0);
-    op.in = wfn; op.out = c.h1_horb; op.skip = nullptr;
-    rc |= launch_h1op(op, st);
-    sv.fs0 = 0; sv.in = c.h1_horb;
-  } else {
-    sv.fs0 = c.nfcore; sv.in = wfn;
-  }
-  sv.out = c.h1_orb; sv.torb = wfn; sv.accumulate = 0; sv.check_skip = 0;
-  rc |= launch_h1solve(sv, c.h1_cg, st);
-  c.launches += pade ? 1 : 2;
-  if (c.isplit == 1) {
-    op.f0 = c.nfcore; op.a = mkc(0, 0); op.b = mkc(0, 0); op.cz0 = zf0; op.afc = mkc(0, 0);
-    op.in = c.h1_orb; op.out = c.h1_horb; op.skip = c.h1_flags;
-    sv.fs0 = c.nfcore; sv.in = c.h1_horb; sv.out = c.h1_orb; sv.accumulate = 1; sv.check_skip = 1;
-    for (int k = 0; k < maxcyc; ++k) {
-      rc |= launch_h1op(op, st);
-      rc |= launch_h1solve(sv, c.h1_cg, st);
+  H1ElemArgs E{};
+  E.fac = F; E.Nr = c.Nr; E.L1 = c.L1; E.nfun = c.nfun; E.nfcore = c.nfcore; E.mmax1 = c.mmax1; E.igauge = c.igauge;
+  E.mval = c.d_mval; E.radk = c.radk; E.radk0 = c.radk0; E.radp = c.radp; E.tdiag = c.tdiag; E.xrad = c.xrad;
+  E.alph = c.alph; E.lfield = d_lf; E.cb = c.h1_cb; E.xb = c.h1_xb; E.torb = wfn;
+  E.thresh = thresh; E.norm_div = (double)c.nfun; E.partial = c.h1_partial; E.ticket = c.h1_ticket;
+  E.done = c.h1_flags; E.ncyc = c.h1_flags + 1;
+  cudaMemsetAsync(c.h1_flags, 0, 2 * sizeof(int), st);
+  int zb = 0;  // z buffer the next pass writes
+  // h1itr also solves the frozen-core columns once: their first correction
+  // enters the residual norm of the first cycle (h1itr_prop.F90:105-129)
+  const int f_first = pade ? c.nfcore : 0;
+  // first right-hand side: wfn (dpade) or wfn + zfac1 (T + zfield V) wfn (h1itr)
+  E.finalize = 0; E.make_rhs = 1; E.check_skip = 0; E.f_rhs = f_first; E.f_fin = c.nfun; E.in = wfn;
+  E.a = mkc(1, 0);
+  E.b = pade ? mkc(0, 0) : zf0;
+  E.cz0 = (!pade && c.isplit == 1) ? zf0 : mkc(0, 0);
+  E.z_in = c.h1_z[1 - zb]; E.z_out = c.h1_z[zb];
+  rc |= launch_h1elem(E, st);
+  rc |= launch_h1bridge(E, st);
+  c.launches += 2;
+  zb = 1 - zb;
+  const bool cycles = c.isplit == 1 && maxcyc > 0;
+  if (cycles) {
+    E.a = mkc(0, 0); E.b = mkc(0, 0); E.cz0 = zf0; E.in = nullptr;
+    for (int k = 1; k <= maxcyc; ++k) {
+      E.finalize = 1; E.do_norm = 1; E.make_rhs = 1; E.check_skip = 1;
+      E.f_fin = k == 1 ? f_first : c.nfcore;
+      E.accumulate = k > 1;
+      E.f_rhs = c.nfcore;
+      E.z_in = c.h1_z[1 - zb]; E.z_out = c.h1_z[zb];
+      rc |= launch_h1elem(E, st);
+      rc |= launch_h1bridge(E, st);
       c.launches += 2;
+      zb = 1 - zb;
     }
   }
+  // the last correction (or the only solve) into torb
+  E.finalize = 1; E.do_norm = 0; E.make_rhs = 0; E.f_fin = c.nfcore; E.f_rhs = c.nfun;
+  E.accumulate = cycles ? 1 : 0; E.check_skip = cycles ? 1 : 0;
+  E.z_in = c.h1_z[1 - zb]; E.z_out = c.h1_z[zb];
+  rc |= launch_h1elem(E, st);
+  c.launches++;
   return rc ? ST_CUDA : 0;
 }
 
@@ -1660,13 +1675,15 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
     int s0 = 0;
     cudaGraphExec_t& ge = c.graph_exec[kind];
     bool cached;
+    const int ctl = c.icomp * 2 + c.igauge;
     if (kind == 0) {
-      cached = ge && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt && b.g_ro == b.reset_orb;
+      cached = ge && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt && b.g_ro == b.reset_orb &&
+               b.g_ctl == ctl;
     } else {
       const int q = kind - 1;
       cached = ge && b.s_y[q] == y && b.s_yc[q] == yc && b.s_tab[q] == c.field_tab && b.s_dt[q] == dt &&
                b.s_cyc[q] == maxcyc && b.s_thr[q] == thresh && b.s_split[q] == c.isplit &&
-               b.s_mask[q] == (int)do_mask && b.s_ro[q] == b.reset_orb;
+               b.s_mask[q] == (int)do_mask && b.s_ro[q] == b.reset_orb && b.s_ctl[q] == ctl;
     }
     if (!cached) {
       rc |= step();
@@ -1683,11 +1700,12 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
       c.launches = l0;
       if (kind == 0) {
         b.g_per = per_step; b.g_y = y; b.g_yc = yc; b.g_tab = c.field_tab; b.g_dt = dt; b.g_ro = b.reset_orb;
+        b.g_ctl = ctl;
       } else {
         const int q = kind - 1;
         b.s_per[q] = per_step; b.s_y[q] = y; b.s_yc[q] = yc; b.s_tab[q] = c.field_tab; b.s_dt[q] = dt;
         b.s_cyc[q] = maxcyc; b.s_thr[q] = thresh; b.s_split[q] = c.isplit; b.s_mask[q] = (int)do_mask;
-        b.s_ro[q] = b.reset_orb;
+        b.s_ro[q] = b.reset_orb; b.s_ctl[q] = ctl;
       }
     }
     const long per_step = kind == 0 ? b.g_per : b.s_per[kind - 1];

@@ -183,6 +183,17 @@ int launch_ci_dvec(const CiArgs& a, int maxsec, cudaStream_t st);
 int launch_ci_rdm(const CiArgs& a, cudaStream_t st);
 int launch_ci_sigma(const CiArgs& a, int maxsec, cudaStream_t st);
 
+// Columns coupled to row ir (1-based radial index) by the FEDVR kinetic and
+// derivative operators: the points of the row's finite element, both
+// elements for a bridge point (ir a multiple of nd); clipped to 1..Nr.
+__device__ __forceinline__ void fedvr_row_span(int ir, int nd, int Nr, int& jlo, int& jhi) {
+  const int e = ir / nd;
+  if (ir == e * nd) { jlo = ir - nd; jhi = ir + nd; }
+  else { jlo = e * nd; jhi = e * nd + nd; }
+  jlo = jlo < 1 ? 1 : jlo;
+  jhi = jhi > Nr ? Nr : jhi;
+}
+
 // ---- one-body propagators of the split schemes (h1prop.cu) ----------------
 // Condensed inverse of M_l = 1 + c T_l, l = 0..L1-1: per finite element the
 // inverse of the interior block and its couplings to the two bridge points,
@@ -210,46 +221,40 @@ struct H1FacSrc {
 };
 int launch_h1fac(const H1FacSrc& s, H1Fac& f, cudaStream_t st);
 
-// out = a in + b T in + (cz0 lfield[2]) V1 in for orbitals >= nfcore, afc in
-// below (orbitals f0 .. nfun-1); V1 the unit-field laser coupling of igauge
-struct H1OpArgs {
-  int Nr, L1, nd, nfun, nfcore, mmax1, igauge, f0;
+// One pass of the element-by-element application of M^-1 (h1prop.cu):
+// finish the previous correction (finalize), add it to torb and the residual
+// norm, and form the next right-hand side r = a x + b T x + (cz0 lfield[2]) V1 x
+// (make_rhs) with its interior solutions z and bridge shares cb; the bridge
+// kernel then solves for the bridge values xb.
+struct H1ElemArgs {
+  H1Fac fac;
+  int Nr, L1, nfun, nfcore, mmax1, igauge;
+  int f_fin, f_rhs;      // first orbital of the finalize / right-hand-side work
+  int finalize, make_rhs, accumulate, do_norm, check_skip;
+  const int* mval;
   const double* radk;
   const double* radk0;
   const double* radp;
   const double* tdiag;
   const double* xrad;
   const double* alph;
-  const int* mval;
   const double* lfield;  // device lfield(1:3,1:3) (may be null: no laser term)
-  cplx a, b, cz0, afc;
-  const cplx* in;
-  cplx* out;
-  const int* skip;       // when non-null and *skip != 0 the launch does nothing
-};
-int launch_h1op(const H1OpArgs& a, cudaStream_t st);
-size_t h1op_smem(int L1, int nd);
-
-// x = M_l^-1 in on the orbital columns fs0 .. nfun-1 (channels l < |m| pass
-// through); out = x and torb = x or += x on orbitals >= nfcore; the last CTA
-// sets *done = sqrt(sum |x|^2 / norm_div) < thresh
-struct H1SolveArgs {
-  H1Fac fac;
-  int Nr, L1, nfun, nfcore, fs0;
-  const int* mval;
-  const cplx* in;
-  cplx* out;             // may be null
-  cplx* torb;
-  int accumulate;
+  cplx a, b, cz0;
+  const cplx* in;        // input vector of a first pass (finalize == 0), [nfun][L1][Nr]
+  const cplx* z_in;      // [nfun][L1][nfe][nd - 1] interior solutions of the previous pass
+  cplx* z_out;           // same layout, this pass (a different buffer than z_in)
+  cplx* cb;              // [nfun][L1][nfe][2] bridge shares (left, right)
+  cplx* xb;              // [nfun][L1][nfe - 1] bridge solutions
+  cplx* torb;            // rows of orbitals >= nfcore: = x or += x
   double thresh, norm_div;
-  double* partial;       // [L1 * column groups]
+  double* partial;       // [h1elem_partials]
   unsigned* ticket;      // zero between launches
-  int* done;
-  int* ncyc;             // cycles run (incremented by launches with check_skip)
-  int check_skip;        // the launch does nothing when *done != 0
+  int* done;             // residual norm below thresh (set by finalize passes with do_norm)
+  int* ncyc;             // correction cycles run (bridge passes with check_skip)
 };
-int launch_h1solve(const H1SolveArgs& a, int CG, cudaStream_t st);
-int h1solve_pick_cg(int Nr, int nfe, int ni, int nb);
-int h1solve_groups(int ncol, int CG);
+int launch_h1elem(const H1ElemArgs& a, cudaStream_t st);
+int launch_h1bridge(const H1ElemArgs& a, cudaStream_t st);
+size_t h1elem_smem(int nd, int nfun);
+size_t h1elem_partials(int nfe, int L1);
 
 }  // namespace td1c

@@ -63,7 +63,8 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
     int r = r0 + q;
     if (r >= Nr) continue;
     const int ir = r + 1;  // Fortran irad
-    const int jll = max(1, ir - nd), jul = min(Nr, ir + nd);
+    int jll, jul;
+    fedvr_row_span(ir, nd, Nr, jll, jul);  // the band is zero outside the row's element(s)
     cplx hs = mkc(0.0, 0.0), ds = mkc(0.0, 0.0);
     if (l >= am) {
       const double* rk = sb + (l == 0 ? 0 : OB_TILE * bw) + q;

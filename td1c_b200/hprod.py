@@ -157,6 +157,11 @@ class HProd:
         self._check(self.lib.td1c_gpu_relax(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(dt), int(ncyc), _dp(ene)))
         return ene[: int(ncyc)]
 
+    def set_time_kind(self, icomp):
+        """icomp of control_bind_ (1 real time, 0 imaginary time), keeping the context."""
+        self.wl = dict(self.wl, icomp=int(icomp))
+        self._check(self.lib.td1c_gpu_bind_control(int(icomp), int(self.wl["igauge"])))
+
     # ---- one-body propagators of the split schemes (src/prop: clh1itr, cldpade)
     def set_split(self, split_type):
         """split_type of control_bind_: 0 full H in the RHS, 1 two-body part only, 2 h0 left out."""

@@ -75,3 +75,26 @@ def seeded_cic(wl, lcic, stra=None, strb=None, detoff=None, afirst=None, acount=
             s[k] = 0.5 * (c[k] + c[idx[(b, a)]])
         c = s
     return c / np.linalg.norm(c)
+
+
+def velocity_gauge_phase(wl, orb, rad, ang, A):
+    """The non-frozen orbitals times exp(-i A r cos(theta)): a length-gauge state
+    expressed in the velocity gauge at vector potential A (the phase the RHS
+    gives the frozen core, hprod_orbin.F90:68-105).  orb has shape
+    (nfun, lmax1+1, nrad-1); returns a new array.  The product is formed on the
+    Gauss-Legendre theta grid and projected back onto l <= lmax1."""
+    orbs = wl["orbitals"]
+    nfun = len(orbs)
+    L1, nlat, mmax1 = ang["lmax1"] + 1, ang["nlat"], ang["mmax1"]
+    Nr = orb.shape[-1]
+    lf1 = np.asarray(ang["legf1"]).reshape(2 * mmax1 + 1, nlat, L1)
+    lb1 = np.asarray(ang["legb1"]).reshape(2 * mmax1 + 1, L1, nlat)
+    r = np.asarray(rad["xrad"])[1:Nr + 1]
+    ph = np.exp(-1j * A * np.outer(np.asarray(ang["cost"]), r))
+    out = np.array(orb, dtype=np.complex128, copy=True).reshape(nfun, L1, Nr)
+    for f, (_n, _l, m, typ) in enumerate(orbs):
+        if typ == -1:
+            continue
+        g = lf1[m + mmax1] @ out[f]
+        out[f] = lb1[m + mmax1] @ (g * ph)
+    return out
