@@ -230,28 +230,45 @@ constexpr int H1E_NT = 256;
 constexpr int H1E_LC = 4;   // l channels per CTA
 constexpr int H1E_FG = 3;   // orbital groups of the interior solve
 
+// shared memory of one element pass; ZI (the previous z rows, read once in
+// step 1) aliases R and Z, which are written only afterwards
 struct H1ElemSmem {
   int np, nf, lh;  // points per element (nd + 1), orbitals, halo rows (LC + 2)
   __host__ __device__ int ni() const { return np - 2; }
   __host__ __device__ size_t x_off() const { return 0; }
   __host__ __device__ size_t r_off() const { return x_off() + (size_t)nf * lh * np; }
   __host__ __device__ size_t z_off() const { return r_off() + (size_t)nf * H1E_LC * np; }
-  __host__ __device__ size_t xb_off() const { return z_off() + (size_t)nf * H1E_LC * ni(); }
+  __host__ __device__ size_t rz_end() const {
+    const size_t rz = z_off() + (size_t)nf * H1E_LC * ni();
+    const size_t zi = r_off() + (size_t)nf * lh * ni();
+    return rz > zi ? rz : zi;
+  }
+  __host__ __device__ size_t ts_off() const { return rz_end(); }
+  __host__ __device__ size_t xb_off() const { return ts_off() + (size_t)nf * H1E_LC * np; }
   __host__ __device__ size_t g_off() const { return xb_off() + (size_t)nf * lh * 2; }
   __host__ __device__ size_t v_off() const { return g_off() + (size_t)2 * lh * ni(); }
   __host__ __device__ size_t ai_off() const { return v_off() + (size_t)2 * H1E_LC * ni(); }
   __host__ __device__ size_t cplx_count() const { return ai_off() + (size_t)H1E_LC * ni() * ni(); }
   __host__ __device__ size_t dbl_count() const { return (size_t)3 * np * np + 2 * np + (size_t)H1E_LC * np + (size_t)nf * lh; }
-  __host__ __device__ size_t bytes() const { return sizeof(cplx) * cplx_count() + sizeof(double) * dbl_count() + sizeof(int) * nf; }
+  __host__ __device__ size_t bytes() const { return sizeof(cplx) * cplx_count() + sizeof(double) * dbl_count(); }
 };
 
-// band value at (irad ip, irad iq), |ip - iq| <= nd, of a (2nd+1) x (nrad+1) table
-__device__ __forceinline__ double band_at(const double* band, int nd, int ip, int iq) {
-  return band[(size_t)(2 * nd + 1) * ip + nd + iq - ip];
+// asynchronous global -> shared copies (LDGSTS); a copy with ok == false
+// reads nothing and zero-fills its destination
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cpa16(void* dst, const void* src, bool ok) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 16u : 0u) : "memory");
+}
+__device__ __forceinline__ void cpa8(void* dst, const void* src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 8u : 0u) : "memory");
+}
+__device__ __forceinline__ void cpa_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 template <int NDT>
-__global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
+__global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
   if (a.check_skip && *a.done) return;
   extern __shared__ cplx sm[];
   const H1Fac& F = a.fac;
@@ -263,6 +280,8 @@ __global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
   cplx* X = sm + lay.x_off();     // [f][lh][np]  rows l0-1 .. l0+LC
   cplx* R = sm + lay.r_off();     // [f][LC][np]
   cplx* Z = sm + lay.z_off();     // [f][LC][ni]
+  cplx* ZI = sm + lay.r_off();    // [f][lh][ni] previous z (step 1 only; aliases R, Z)
+  cplx* TS = sm + lay.ts_off();   // [f][LC][np] torb before the update
   cplx* XB = sm + lay.xb_off();   // [f][lh][2] bridge values left / right of the element
   cplx* GLs = sm + lay.g_off();   // [lh][ni]
   cplx* GRs = GLs + lh * ni;      // [lh][ni]
@@ -276,111 +295,133 @@ __global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
   double* Xr = Pd + np;           // [np] radial coordinate
   double* TD = Xr + np;           // [LC][np] kinetic diagonal
   double* AL = TD + H1E_LC * np;  // [f][lh] alpha_lm of l0-1 .. l0+LC
-  int* MV = reinterpret_cast<int*>(AL + (size_t)nfun * lh);  // [f] m
   __shared__ double red[H1E_NT / 32];
   __shared__ bool last;
   const int ir0 = nd * e;  // irad of local point 0
-  const int f_lo = a.finalize ? min(a.f_fin, a.f_rhs) : a.f_rhs;
+  const cplx* z_in = a.z_in;
+  cplx* z_out = a.z_out;
+  int f_fin = a.f_fin, accumulate = a.accumulate;
+  if (a.iter_mode == 1) {
+    const int k = *a.iter + 1;
+    f_fin = k == 1 ? a.f_first : a.nfcore;
+    accumulate = k > 1;
+    z_in = ((k - 1) & 1) ? a.zb1 : a.zb0;
+    z_out = (k & 1) ? a.zb1 : a.zb0;
+  } else if (a.iter_mode == 2) {
+    z_in = (*a.iter & 1) ? a.zb1 : a.zb0;
+  }
+  const int f_lo = a.finalize ? min(f_fin, a.f_rhs) : a.f_rhs;
   const size_t eb = (size_t)e * ni;
-  // 0. tables of the element and the chunk, loaded together
+  const int bw = 2 * nd + 1;
+  auto valid = [&](int ip) { return ip >= 1 && ip <= Nr; };
+  // 0. every table and input of the pass, copied asynchronously
   for (int q2 = tid; q2 < np * np; q2 += H1E_NT) {
-    const int p = q2 / np, q = q2 % np;
-    const int ip = ir0 + p, iq = ir0 + q;
-    double pv = 0.0, t0 = 0.0, t1 = 0.0;
-    if (p != q && ip >= 1 && ip <= Nr && iq >= 1 && iq <= Nr) {
-      pv = band_at(a.radp, nd, ip, iq);
-      t0 = band_at(a.radk, nd, ip, iq);
-      t1 = band_at(a.radk0, nd, ip, iq);
-    }
-    Pb[q2] = pv; Tb0[q2] = t0; Tb1[q2] = t1;
+    const int p = q2 / np, q = q2 % np, ip = ir0 + p, iq = ir0 + q;
+    const bool ok = p != q && valid(ip) && valid(iq);
+    const size_t o = ok ? (size_t)bw * ip + nd + iq - ip : 0;
+    cpa8(Pb + q2, a.radp + o, ok);
+    cpa8(Tb0 + q2, a.radk + o, ok);
+    cpa8(Tb1 + q2, a.radk0 + o, ok);
   }
   for (int p = tid; p < np; p += H1E_NT) {
     const int ip = ir0 + p;
-    const bool ex = ip >= 1 && ip <= Nr;
-    Pd[p] = (ex && p != nd) ? band_at(a.radp, nd, ip, ip) : 0.0;
-    Xr[p] = ex ? a.xrad[ip] : 1.0;
+    const bool ok = valid(ip);
+    cpa8(Pd + p, a.radp + (ok ? (size_t)bw * ip + nd : 0), ok && p != nd);
+    cpa8(Xr + p, a.xrad + (ok ? ip : 0), ok);
   }
   for (int q2 = tid; q2 < H1E_LC * np; q2 += H1E_NT) {
     const int lc = q2 / np, p = q2 % np, l = l0 + lc, ip = ir0 + p;
-    TD[q2] = (l < L1 && ip >= 1 && ip <= Nr) ? a.tdiag[(size_t)l * Nr + ip - 1] : 0.0;
+    const bool ok = l < L1 && valid(ip);
+    cpa8(TD + q2, a.tdiag + (ok ? (size_t)l * Nr + ip - 1 : 0), ok);
   }
   for (int q2 = tid; q2 < nfun * lh; q2 += H1E_NT) {
     const int f = q2 / lh, lq = q2 % lh, l = l0 - 1 + lq;
-    const int m = a.mval[f];
-    if (lq == 0) MV[f] = m;
-    AL[q2] = (l >= 0 && l < L1) ? a.alph[(size_t)(m + a.mmax1) * L1 + l] : 0.0;
-    cplx xl = mkc(0, 0), xr = mkc(0, 0);
-    if (a.finalize && f >= f_lo && l >= 0 && l < L1) {
-      const size_t row = (size_t)f * L1 + l;
-      if (e >= 1) xl = a.xb[row * nb + e - 1];
-      if (e + 1 < nfe) xr = a.xb[row * nb + e];
-    }
-    XB[2 * q2] = xl; XB[2 * q2 + 1] = xr;
+    const bool lok = l >= 0 && l < L1;
+    cpa8(AL + q2, a.alph + (lok ? (size_t)(a.mv[f] + a.mmax1) * L1 + l : 0), lok);
+    const bool fok = a.finalize && f >= f_lo && lok;
+    const size_t row = (size_t)f * L1 + (lok ? l : 0);
+    cpa16(XB + 2 * q2, a.xb + (fok && e >= 1 ? row * nb + e - 1 : 0), fok && e >= 1);
+    cpa16(XB + 2 * q2 + 1, a.xb + (fok && e + 1 < nfe ? row * nb + e : 0), fok && e + 1 < nfe);
   }
   if (a.finalize) {
     for (int q2 = tid; q2 < lh * ni; q2 += H1E_NT) {
       const int lq = q2 / ni, k = q2 % ni, l = l0 - 1 + lq;
       const bool ok = l >= 0 && l < L1;
-      const size_t gi = (size_t)l * nfe * ni + eb + k;
-      GLs[q2] = ok ? F.gl[gi] : mkc(0, 0);
-      GRs[q2] = ok ? F.gr[gi] : mkc(0, 0);
+      const size_t gi = ok ? (size_t)l * nfe * ni + eb + k : 0;
+      cpa16(GLs + q2, F.gl + gi, ok);
+      cpa16(GRs + q2, F.gr + gi, ok);
+    }
+    for (int q2 = tid; q2 < nfun * lh * ni; q2 += H1E_NT) {
+      const int f = q2 / (lh * ni), lq = (q2 / ni) % lh, k = q2 % ni, l = l0 - 1 + lq;
+      const bool ok = f >= f_lo && l >= 0 && l < L1;
+      cpa16(ZI + q2, z_in + (ok ? ((size_t)f * L1 + l) * nfe * ni + eb + k : 0), ok);
+    }
+    if (accumulate) {
+      for (int q2 = tid; q2 < nfun * H1E_LC * np; q2 += H1E_NT) {
+        const int f = q2 / (H1E_LC * np), lc = (q2 / np) % H1E_LC, p = q2 % np, l = l0 + lc, ip = ir0 + p;
+        const bool ok = f >= f_fin && f >= a.nfcore && l < L1 && p != nd && valid(ip);
+        cpa16(TS + q2, a.torb + (ok ? ((size_t)f * L1 + l) * Nr + ip - 1 : 0), ok);
+      }
+    }
+  } else {
+    for (int q2 = tid; q2 < nfun * lh * np; q2 += H1E_NT) {
+      const int f = q2 / (lh * np), lq = (q2 / np) % lh, p = q2 % np, l = l0 - 1 + lq, ip = ir0 + p;
+      const bool ok = f >= f_lo && l >= 0 && l < L1 && valid(ip);
+      cpa16(X + q2, a.in + (ok ? ((size_t)f * L1 + l) * Nr + ip - 1 : 0), ok);
     }
   }
   if (a.make_rhs) {
     for (int q2 = tid; q2 < H1E_LC * ni; q2 += H1E_NT) {
       const int lc = q2 / ni, k = q2 % ni, l = l0 + lc;
       const bool ok = l < L1;
-      const size_t vi = (size_t)l * nfe * ni + eb + k;
-      VLs[q2] = ok ? F.vl[vi] : mkc(0, 0);
-      VRs[q2] = ok ? F.vr[vi] : mkc(0, 0);
+      const size_t vi = ok ? (size_t)l * nfe * ni + eb + k : 0;
+      cpa16(VLs + q2, F.vl + vi, ok);
+      cpa16(VRs + q2, F.vr + vi, ok);
     }
     for (int q2 = tid; q2 < H1E_LC * ni * ni; q2 += H1E_NT) {
       const int lc = q2 / (ni * ni), jk = q2 % (ni * ni), l = l0 + lc;
-      AI[q2] = l < L1 ? F.ainv[((size_t)l * nfe * ni + eb) * ni + jk] : mkc(0, 0);
+      const bool ok = l < L1;
+      cpa16(AI + q2, F.ainv + (ok ? ((size_t)l * nfe * ni + eb) * ni + jk : 0), ok);
     }
   }
+  cpa_wait_all();
   __syncthreads();
-  // 1. x on the element for l0-1 .. l0+LC
-#pragma unroll 4
-  for (int it = tid; it < nfun * lh * np; it += H1E_NT) {
-    const int f = it / (lh * np), lq = (it / np) % lh, p = it % np;
-    const int l = l0 - 1 + lq, ip = ir0 + p;
-    cplx x = mkc(0, 0);
-    if (f >= f_lo && l >= 0 && l < L1 && ip >= 1 && ip <= Nr) {
-      const size_t row = (size_t)f * L1 + l;
-      const cplx* xbr = XB + 2 * ((size_t)f * lh + lq);
-      if (!a.finalize) {
-        x = a.in[row * Nr + ip - 1];
-      } else if (p == 0) {
-        x = xbr[0];
-      } else if (p == nd) {
-        x = xbr[1];
-      } else {
-        const int k = p - 1;
-        const int m = MV[f];
-        x = a.z_in[row * nfe * ni + eb + k];
-        if (l >= (m < 0 ? -m : m)) {
-          x = csub(x, cmul(GLs[lq * ni + k], xbr[0]));
-          x = csub(x, cmul(GRs[lq * ni + k], xbr[1]));
+  // 1. x on the element for l0-1 .. l0+LC (the previous correction finished)
+  if (a.finalize) {
+    for (int it = tid; it < nfun * lh * np; it += H1E_NT) {
+      const int f = it / (lh * np), lq = (it / np) % lh, p = it % np;
+      const int l = l0 - 1 + lq, ip = ir0 + p;
+      cplx x = mkc(0, 0);
+      if (f >= f_lo && l >= 0 && l < L1 && valid(ip)) {
+        const cplx* xbr = XB + 2 * ((size_t)f * lh + lq);
+        if (p == 0) {
+          x = xbr[0];
+        } else if (p == nd) {
+          x = xbr[1];
+        } else {
+          const int k = p - 1;
+          const int m = a.mv[f];
+          x = ZI[((size_t)f * lh + lq) * ni + k];
+          if (l >= (m < 0 ? -m : m)) {
+            x = csub(x, cmul(GLs[lq * ni + k], xbr[0]));
+            x = csub(x, cmul(GRs[lq * ni + k], xbr[1]));
+          }
         }
       }
+      X[it] = x;
     }
-    X[it] = x;
+    __syncthreads();
   }
-  __syncthreads();
   // 2. finished corrections: torb and the residual norm (owned points)
   if (a.finalize) {
     double nrm = 0.0;
     for (int it = tid; it < nfun * H1E_LC * np; it += H1E_NT) {
       const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC, p = it % np;
       const int l = l0 + lc, ip = ir0 + p;
-      if (f < a.f_fin || l >= L1 || p == nd || ip < 1 || ip > Nr) continue;
+      if (f < f_fin || l >= L1 || p == nd || !valid(ip)) continue;
       const cplx x = X[((size_t)f * lh + lc + 1) * np + p];
       nrm += cabs2(x);
-      if (f >= a.nfcore) {
-        const size_t gi = ((size_t)f * L1 + l) * Nr + ip - 1;
-        a.torb[gi] = a.accumulate ? cadd(a.torb[gi], x) : x;
-      }
+      if (f >= a.nfcore) a.torb[((size_t)f * L1 + l) * Nr + ip - 1] = accumulate ? cadd(TS[it], x) : x;
     }
     for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
     if ((tid & 31) == 0) red[tid >> 5] = nrm;
@@ -397,8 +438,8 @@ __global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
       const int l = l0 + lc, ip = ir0 + p;
       if (f < a.f_rhs || l >= L1) continue;
       cplx r = mkc(0, 0);
-      if (ip >= 1 && ip <= Nr) {
-        const int m = MV[f], am = m < 0 ? -m : m;
+      if (valid(ip)) {
+        const int m = a.mv[f], am = m < 0 ? -m : m;
         const bool owner = p != nd;       // the right bridge belongs to the next element
         const bool dyn = f >= a.nfcore;   // frozen-core rows take the a-term only
         const cplx* xl = X + ((size_t)f * lh + lc + 1) * np;  // x(l, .)
@@ -456,7 +497,7 @@ __global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
       if (l >= L1) continue;
       const cplx* av = AI + (size_t)lc * ni * ni + k;  // av[j * ni] = Ainv(k, j)
       for (int f = a.f_rhs + g; f < nfun; f += H1E_FG) {
-        const int m = MV[f];
+        const int m = a.mv[f];
         const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np + 1;
         cplx zv;
         if (l < (m < 0 ? -m : m)) {
@@ -468,7 +509,7 @@ __global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
           for (int j = (NDT > 0 ? NDT - 1 : 0); j < ni; ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
         }
         Z[((size_t)f * H1E_LC + lc) * ni + k] = zv;
-        a.z_out[((size_t)f * L1 + l) * nfe * ni + eb + k] = zv;
+        z_out[((size_t)f * L1 + l) * nfe * ni + eb + k] = zv;
       }
     }
     __syncthreads();
@@ -478,7 +519,7 @@ __global__ void __launch_bounds__(H1E_NT) h1elem_kernel(H1ElemArgs a) {
       const int l = l0 + lc;
       if (f < a.f_rhs || l >= L1) continue;
       if (side == 0 ? e < 1 : e + 1 >= nfe) continue;
-      const int m = MV[f];
+      const int m = a.mv[f];
       const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np;
       cplx c = side == 0 ? rf[0] : rf[nd];
       if (l >= (m < 0 ? -m : m)) {
@@ -609,6 +650,17 @@ int launch_h1bridge(const H1ElemArgs& a, cudaStream_t st) {
   if (smem > 220 * 1024) return ST_CONFIG;
   if (int e = ensure_smem(h1bridge_kernel, smem, cur)) return e;
   h1bridge_kernel<<<a.L1, H1B_NT, smem, st>>>(a);
+  return (int)cudaGetLastError();
+}
+
+__global__ void h1loop_ctl_kernel(int* iter, const int* done, int maxcyc, cudaGraphConditionalHandle h) {
+  const int k = *iter + 1;
+  *iter = k;
+  cudaGraphSetConditional(h, (*done == 0 && k < maxcyc) ? 1u : 0u);
+}
+
+int launch_h1loop_ctl(int* iter, const int* done, int maxcyc, cudaGraphConditionalHandle h, cudaStream_t st) {
+  h1loop_ctl_kernel<<<1, 1, 0, st>>>(iter, done, maxcyc, h);
   return (int)cudaGetLastError();
 }
 

@@ -145,7 +145,8 @@ struct Ctx {
   cplx *h1_cb = nullptr, *h1_xb = nullptr;  // bridge shares, bridge values
   double* h1_partial = nullptr;
   unsigned* h1_ticket = nullptr;
-  int* h1_flags = nullptr;  // [0] done, [1] cycles of the last application
+  int* h1_flags = nullptr;  // [0] done, [1] cycles of the last application, [2] cycle counter of a graph loop
+  cudaStream_t st4 = nullptr;  // stream on which graph-loop bodies are captured
   // phase timing (off during graph capture)
   bool profile = false;
   cudaEvent_t ev[16] = {};
@@ -1443,7 +1444,7 @@ int h1_bufs(Ctx& c) {
   c.h1_xb = dalloc<cplx>(nrow * std::max(1, c.nfe - 1));
   c.h1_partial = dalloc<double>(h1elem_partials(c.nfe, c.L1));
   c.h1_ticket = dalloc<unsigned>(1);  // zero (dalloc clears)
-  c.h1_flags = dalloc<int>(2);
+  c.h1_flags = dalloc<int>(3);
   return 0;
 }
 
@@ -1479,7 +1480,9 @@ int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cpl
   E.alph = c.alph; E.lfield = d_lf; E.cb = c.h1_cb; E.xb = c.h1_xb; E.torb = wfn;
   E.thresh = thresh; E.norm_div = (double)c.nfun; E.partial = c.h1_partial; E.ticket = c.h1_ticket;
   E.done = c.h1_flags; E.ncyc = c.h1_flags + 1;
-  cudaMemsetAsync(c.h1_flags, 0, 2 * sizeof(int), st);
+  E.iter = c.h1_flags + 2; E.zb0 = c.h1_z[0]; E.zb1 = c.h1_z[1]; E.iter_mode = 0;
+  for (int f = 0; f < c.nfun && f < 16; ++f) E.mv[f] = c.mval[f];
+  cudaMemsetAsync(c.h1_flags, 0, 3 * sizeof(int), st);
   int zb = 0;  // z buffer the next pass writes
   // h1itr also solves the frozen-core columns once: their first correction
   // enters the residual norm of the first cycle (h1itr_prop.F90:105-129)
@@ -1495,6 +1498,47 @@ int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cpl
   c.launches += 2;
   zb = 1 - zb;
   const bool cycles = c.isplit == 1 && maxcyc > 0;
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(st, &cst);
+  if (cycles && cst == cudaStreamCaptureStatusActive) {
+    // inside a graph capture: the correction cycles become a conditional
+    // while-loop node whose body (element pass, bridge pass, loop control)
+    // runs until the residual norm is below thresh or maxcyc cycles have run;
+    // the control kernel advances the cycle counter every iteration, so the
+    // loop ends after at most maxcyc iterations
+    E.a = mkc(0, 0); E.b = mkc(0, 0); E.cz0 = zf0; E.in = nullptr;
+    E.f_first = f_first;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndep = 0;
+    cudaStreamCaptureStatus cs2;
+    if (cudaStreamGetCaptureInfo(st, &cs2, nullptr, &g, &deps, &ndep) != cudaSuccess) return ST_CUDA;
+    cudaGraphConditionalHandle hnd;
+    if (cudaGraphConditionalHandleCreate(&hnd, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) return ST_CUDA;
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hnd;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, deps, ndep, &np) != cudaSuccess) return ST_CUDA;
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return ST_CUDA;
+    if (cudaStreamBeginCaptureToGraph(c.st4, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return ST_CUDA;
+    E.finalize = 1; E.do_norm = 1; E.make_rhs = 1; E.check_skip = 1; E.f_rhs = c.nfcore; E.iter_mode = 1;
+    rc |= launch_h1elem(E, c.st4);
+    rc |= launch_h1bridge(E, c.st4);
+    rc |= launch_h1loop_ctl(c.h1_flags + 2, c.h1_flags, maxcyc, hnd, c.st4);
+    cudaGraph_t body_out = nullptr;
+    if (cudaStreamEndCapture(c.st4, &body_out) != cudaSuccess) return ST_CUDA;
+    c.launches += 3;
+    E.finalize = 1; E.do_norm = 0; E.make_rhs = 0; E.f_fin = c.nfcore; E.f_rhs = c.nfun;
+    E.accumulate = 1; E.check_skip = 1; E.iter_mode = 2;
+    rc |= launch_h1elem(E, st);
+    c.launches++;
+    return rc ? ST_CUDA : 0;
+  }
   if (cycles) {
     E.a = mkc(0, 0); E.b = mkc(0, 0); E.cz0 = zf0; E.in = nullptr;
     for (int k = 1; k <= maxcyc; ++k) {
@@ -1793,7 +1837,9 @@ void hprod_init_(void) {
   if (c.nfun > 16) { c.status |= ST_CONFIG; return; }
   // one library stream for the process lifetime: callers may hold it
   // (td1c_gpu_stream) beyond hprod_final_
-  static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr, lib_stream3 = nullptr;
+  static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr, lib_stream3 = nullptr, lib_stream4 = nullptr;
+  if (!lib_stream4) cudaStreamCreateWithFlags(&lib_stream4, cudaStreamNonBlocking);
+  c.st4 = lib_stream4;
   if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
   if (!lib_stream2) cudaStreamCreateWithFlags(&lib_stream2, cudaStreamNonBlocking);
   if (!lib_stream3) cudaStreamCreateWithFlags(&lib_stream3, cudaStreamNonBlocking);

@@ -251,8 +251,20 @@ struct H1ElemArgs {
   unsigned* ticket;      // zero between launches
   int* done;             // residual norm below thresh (set by finalize passes with do_norm)
   int* ncyc;             // correction cycles run (bridge passes with check_skip)
+  // device-driven cycles (the body of a graph loop): iter_mode 1 takes the
+  // cycle k = *iter + 1 from the device and derives f_fin (f_first on cycle 1),
+  // accumulate (k > 1) and the z buffers (zb[(k-1)&1] in, zb[k&1] out);
+  // iter_mode 2 (the last pass) reads z from zb[*iter & 1]
+  int iter_mode, f_first;
+  int mv[16];            // m of every orbital (nfun <= 16)
+  const int* iter;
+  cplx* zb0;
+  cplx* zb1;
 };
 int launch_h1elem(const H1ElemArgs& a, cudaStream_t st);
+// graph-loop control: *iter += 1, then the loop continues while the residual
+// norm is not below thresh (*done == 0) and *iter < maxcyc
+int launch_h1loop_ctl(int* iter, const int* done, int maxcyc, cudaGraphConditionalHandle h, cudaStream_t st);
 int launch_h1bridge(const H1ElemArgs& a, cudaStream_t st);
 size_t h1elem_smem(int nd, int nfun);
 size_t h1elem_partials(int nfe, int L1);
