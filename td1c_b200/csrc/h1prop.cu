@@ -571,17 +571,26 @@ __global__ void __launch_bounds__(H1B_NT) h1bridge_kernel(H1ElemArgs a) {
   cplx* du = di + nb;
   cplx* du2 = du + nb;
   cplx* g = du2 + nb;  // [nfun][nb]
-  int* ip = reinterpret_cast<int*>(g + (size_t)nfun * nb);
+  int* ip = reinterpret_cast<int*>(g + (size_t)3 * nfun * nb);
+  // factors and both bridge shares copied asynchronously; the shares are
+  // added once they have landed
+  cplx* gs = g + (size_t)nfun * nb;  // [nfun][nb][2] shares (right of element b, left of b+1)
   for (int q = tid; q < nb; q += H1B_NT) {
     const size_t o = (size_t)l * nb + q;
-    dl[q] = F.tdl[o]; di[q] = F.tdi[o]; du[q] = F.tdu[o]; du2[q] = F.tdu2[o]; ip[q] = F.tpiv[o];
+    cpa16(dl + q, F.tdl + o, true); cpa16(di + q, F.tdi + o, true);
+    cpa16(du + q, F.tdu + o, true); cpa16(du2 + q, F.tdu2 + o, true);
   }
   for (int it = tid; it < nfun * nb; it += H1B_NT) {
     const int f = it / nb, b = it % nb;
-    if (f < a.f_rhs) continue;
+    const bool ok = f >= a.f_rhs;
     const size_t c0 = ((size_t)f * L1 + l) * nfe;
-    g[it] = cadd(a.cb[(c0 + b) * 2 + 1], a.cb[(c0 + b + 1) * 2 + 0]);
+    cpa16(gs + 2 * it, a.cb + (ok ? (c0 + b) * 2 + 1 : 0), ok);
+    cpa16(gs + 2 * it + 1, a.cb + (ok ? (c0 + b + 1) * 2 : 0), ok);
   }
+  for (int q = tid; q < nb; q += H1B_NT) ip[q] = F.tpiv[(size_t)l * nb + q];
+  cpa_wait_all();
+  __syncthreads();
+  for (int it = tid; it < nfun * nb; it += H1B_NT) g[it] = cadd(gs[2 * it], gs[2 * it + 1]);
   __syncthreads();
   if (tid == 0 && l == 0 && a.ncyc && a.check_skip) atomicAdd(a.ncyc, 1);
   const int f = a.f_rhs + tid;
@@ -645,7 +654,7 @@ int launch_h1elem(const H1ElemArgs& a, cudaStream_t st) {
 int launch_h1bridge(const H1ElemArgs& a, cudaStream_t st) {
   if (a.fac.nb <= 0) return 0;
   if (a.nfun - a.f_rhs > H1B_NT) return ST_CONFIG;
-  const size_t smem = sizeof(cplx) * (size_t)a.fac.nb * (4 + a.nfun) + sizeof(int) * a.fac.nb;
+  const size_t smem = sizeof(cplx) * (size_t)a.fac.nb * (4 + 3 * a.nfun) + sizeof(int) * a.fac.nb;
   static size_t cur = 0;
   if (smem > 220 * 1024) return ST_CONFIG;
   if (int e = ensure_smem(h1bridge_kernel, smem, cur)) return e;
