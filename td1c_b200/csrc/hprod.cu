@@ -84,6 +84,7 @@ struct Ctx {
   double *tdiag = nullptr, *d2ll = nullptr, *d2rinv = nullptr, *rpl0 = nullptr, *rpl1 = nullptr, *invr = nullptr, *fac2 = nullptr, *fac1 = nullptr;
   double *ps_tabf = nullptr, *ps_tabb = nullptr;  // Poisson row tables (forward, backward)
   PoissonArgs ps_main{}, ps_fcfc{};  // Poisson arguments with encoded tensor maps (RHS pairs, fcfc pairs)
+  PsCondArgs ps_cond{};  // condensed Poisson of the RHS pairs (factors and work buffers)
   MfprodArgs mf{};  // mean-field action arguments with encoded tensor maps
   int* d_mval = nullptr;
   // ---- pairs
@@ -639,6 +640,23 @@ int build_tables(Ctx& c) {
     PoissonArgs pa = poisson_args(c, c.npair, 0);
     if (launch_poisson_tables(pa, c.ps_tabf, c.ps_tabb, 0)) return ST_CUDA;
   }
+  {
+    // condensed factors of the same matrices for the per-RHS solve (the banded
+    // factor above serves the frozen-core set-up)
+    if (c.nd < 2 || c.nfe < 1 || c.nfe * c.nd - 1 != Nr) return ST_CONFIG;
+    PsCond& f = c.ps_cond.f;
+    f.nfe = c.nfe; f.nd = c.nd; f.ni = c.nd - 1; f.nb = c.nfe - 1; f.L2 = c.L2; f.Nr = Nr;
+    f.er = (f.ni * f.ni + 3 * f.ni + 2 + 1) / 2 * 2;
+    f.sr = (3 * f.nd + 1) / 2 * 2;
+    const size_t ne = (size_t)c.L2 * f.nfe * f.ni, nbt = (size_t)c.L2 * std::max(1, f.nb);
+    f.erec = dalloc<double>((size_t)c.L2 * f.nfe * f.er);
+    f.srec = dalloc<double>((size_t)c.L2 * f.nfe * f.sr);
+    f.gl = dalloc<double>(ne); f.gr = dalloc<double>(ne); f.vl = dalloc<double>(ne); f.vr = dalloc<double>(ne);
+    f.tm = dalloc<double>(nbt); f.tw = dalloc<double>(nbt); f.tu = dalloc<double>(nbt);
+    if (launch_ps_cond_setup(f, c.xrad, c.radk, c.invr, c.rpl0, c.rpl1, c.fac2, dstat, 0)) return ST_CUDA;
+    cudaMemcpy(&hst, dstat, sizeof(int), cudaMemcpyDeviceToHost);
+    if (hst) { fprintf(stderr, "td1c_b200: condensed Poisson factorisation failed\n"); return ST_CHOLESKY; }
+  }
   c.tdiag = dalloc<double>((size_t)Nr * c.L1);
   c.v2jfc = dalloc<double>(Nr);
   tdiag_kernel<<<(Nr * c.L1 + 255) / 256, 256>>>(Nr, c.L1, c.nd, c.znuc, c.xrad, c.radk, c.radk0, nullptr, c.tdiag);
@@ -689,6 +707,16 @@ int build_state(Ctx& c) {
   c.ps_main = poisson_args(c, c.npair, 0);
   c.ps_fcfc = poisson_args(c, c.nfcfc, c.npair);
   if (poisson_encode_maps(c.ps_main) || poisson_encode_maps(c.ps_fcfc)) return ST_CUDA;
+  {
+    PsCondArgs& a = c.ps_cond;
+    a.Nr = c.Nr; a.L2 = c.L2; a.npair = c.npair; a.pair_m = c.pair_m; a.rho2 = c.rho2; a.v2sph = c.v2sph;
+    a.fac1 = c.fac1;
+    const size_t nl = (size_t)c.L2 * std::max(1, c.npair);
+    a.cb = dalloc<cplx>(nl * c.nfe * 2);
+    a.tpart = dalloc<cplx>(nl * c.nfe);
+    a.xb = dalloc<cplx>(nl * std::max(1, c.nfe - 1));
+    a.t = dalloc<cplx>(nl);
+  }
   return 0;
 }
 
@@ -1220,8 +1248,8 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   if (c.neltot >= 2 && c.npair > 0) {
     rc |= chk("rho gemm", gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true));
     mark();  // end rho_gemm
-    rc |= chk("poisson", launch_poisson(c.ps_main, st));
-    c.launches++;
+    rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
+    c.launches += 3;
     // int2e needs only rho2 and v2sph: third stream, overlapping l->theta,
     // mfprod and the theta->l transforms; joins before smallmat
     if (c.nact > 0) {

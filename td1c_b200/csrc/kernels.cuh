@@ -72,6 +72,38 @@ int poisson_encode_maps(PoissonArgs& a);  // fills boxp, tm_rho, tm_v2 from rho2
 int launch_poisson_tables(const PoissonArgs& a, double* tabf, double* tabb, cudaStream_t st);
 int launch_poisson(const PoissonArgs& a, cudaStream_t st);
 
+// ---- Poisson by static condensation (poisson_cond.cu): A_l = l(l+1)/r^2 + 2T
+// inverted element by element; the bridge Schur complement is tridiagonal
+struct PsCond {
+  int nfe = 0, nd = 0, ni = 0, nb = 0, L2 = 0, Nr = 0;  // ni = nd - 1 interior points, nb = nfe - 1 bridges
+  int er = 0, sr = 0;      // doubles per element / share record (even)
+  double* erec = nullptr;  // [L2][nfe][er]: W(j, k) = fac2(k) (A_e^-1)(k, j) invr(j) as [j][k]; fac2 GL; fac2 GR;
+                           //   fac2 rpl1 (interior points); fac2 and fac2 rpl1 at the left bridge
+  double* srec = nullptr;  // [L2][nfe][sr]: coefficient rows (t, left share, right share) over the nd owned points
+  double* gl = nullptr;    // [L2][nfe][ni]: A_e^-1 A(I_e, left bridge)   (set-up)
+  double* gr = nullptr;    // [L2][nfe][ni]: A_e^-1 A(I_e, right bridge)  (set-up)
+  double* vl = nullptr;    // [L2][nfe][ni]: A(left bridge, I_e)          (set-up)
+  double* vr = nullptr;    // [L2][nfe][ni]: A(right bridge, I_e)         (set-up)
+  double* tm = nullptr;    // [L2][nb] LU of the bridge system: multipliers,
+  double* tw = nullptr;    //   reciprocal pivots,
+  double* tu = nullptr;    //   superdiagonal
+};
+struct PsCondArgs {
+  PsCond f;
+  int Nr, L2, npair;
+  const int* pair_m;     // [npair]
+  const cplx* rho2;      // [npair][L2][Nr]
+  cplx* v2sph;           // [npair][L2][Nr]
+  const double* fac1;    // [L2]
+  cplx* cb;              // [L2][nfe][2][npair] element shares of the bridge right-hand sides
+  cplx* tpart;           // [L2][nfe][npair] element shares of t
+  cplx* xb;              // [L2][nb][npair] bridge values
+  cplx* t;               // [L2][npair]
+};
+int launch_ps_cond_setup(PsCond& f, const double* xrad, const double* radk, const double* invr, const double* rpl0,
+                         const double* rpl1, const double* fac2, int* status, cudaStream_t st);
+int launch_ps_cond(const PsCondArgs& a, cudaStream_t st);
+
 // ---- mean-field action on the (r, theta) grid (hprod_mfprod2.F90)
 struct Act2Block {     // one dense (ij) x (kl) block of the 2-RDM contraction
   int row0, nrow;      // rows: (ia, ja) entries rows[row0 .. row0+nrow)
