@@ -4,7 +4,8 @@ Counts follow the loops of the reference routines with the m-selection and
 l >= |m| bounds applied (only work the reference performs is counted):
   orbin      sph2ang1 over dynamic orbitals           bas_sph2ang1.F90:88-156
   rho_gemm   pair products + theta->l                 hprod_mkrho2.F90, bas_ang2sph2.F90:330-482
-  poisson    two band substitutions per (pair, l, re|im)  hprod_mkv2mf.F90:118-182
+  poisson    per (pair, l): element shares, bridge solve, interior products
+             (static condensation of the same linear system)  hprod_mkv2mf.F90:118-182
   w_gemm     l->theta                                 bas_sph2ang2.F90:334-463
   mfprod     core J/K + active J/K + 2-RDM contraction hprod_mfprod2.F90
   gorb_gemm  theta->l of g and v2                     bas_ang2sph1.F90:88-158
@@ -41,9 +42,16 @@ def rhs_work(wl, dims):
     # pair density + theta->l
     f_rho = sum((L2 - abs(m[b] - m[a])) * nlat * 2 * Nr * 2 + 6 * nlat * Nr for a, b in pairs)
     w["rho_gemm"] = (f_rho, C * (nfun * ngrid + npair * nbas2))
-    # Poisson
-    nsys = sum(2 * (L2 - abs(m[b] - m[a])) for a, b in pairs)
-    w["poisson"] = (nsys * Nr * (4 * nd + 8), C * 2 * npair * nbas2 + 8 * L2 * Nr * (nd + 1))
+    # Poisson by static condensation, per complex (pair, l) system: three share rows over
+    # the nd owned points of each element, the interior products (ni x ni, real matrix on
+    # complex data) with their finalisation, and the tridiagonal bridge solve.  Bytes: rho2
+    # read by the share and the element passes, v2sph written once, the per-(l, element)
+    # records read once.
+    nfe, ni = (Nr + 1) // nd, nd - 1
+    nsys = sum(L2 - abs(m[b] - m[a]) for a, b in pairs)
+    f_sys = nfe * (3 * nd * 4 + ni * ni * 4 + ni * 8 + 8) + (nfe - 1) * 16
+    rec = 8 * L2 * nfe * ((ni * ni + 3 * ni + 3) // 2 * 2 + (3 * nd + 1) // 2 * 2)
+    w["poisson"] = (nsys * f_sys, C * 3 * npair * nbas2 + rec)
     # l->theta
     f_w = sum(nlat * (L2 - abs(m[b] - m[a])) * 2 * Nr * 2 for a, b in pairs)
     w["w_gemm"] = (f_w, C * npair * (nbas2 + ngrid))
