@@ -197,7 +197,7 @@ __device__ __forceinline__ void mfd_cp16(void* dst, const void* src, unsigned by
 }
 
 static size_t mfd_smem_bytes(const MfprodArgs& a) {
-  return sizeof(cplx) * ((size_t)(a.npair + 1) * MFD_WP + (size_t)a.ncoef_d + (size_t)a.nfun * MFD_TQ +
+  return sizeof(cplx) * ((size_t)(a.npair + 1) * MFD_WP + (size_t)a.ncoef_d + 2 * (size_t)a.nfun * MFD_TQ +
                          (size_t)a.nrow * MFD_TQ + (size_t)a.nact * MFD_TQ);
 }
 static bool mfd_fits(const MfprodArgs& a) {
@@ -210,8 +210,8 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
   const int nact = a.nact, ncore = a.ncore, nfcore = a.nfcore, nfun = a.nfun, npair = a.npair;
   cplx* sW = mfd_smem;                                   // [npair + 1][WP]
   cplx* sC = sW + (size_t)(npair + 1) * MFD_WP;          // [ncoef_d]
-  cplx* sPhi = sC + a.ncoef_d;                           // [nfun][TQ]
-  cplx* sD = sPhi + (size_t)nfun * MFD_TQ;               // [nrow][TQ]
+  cplx* sPhi2 = sC + a.ncoef_d;                          // 2 x [nfun][TQ]: this tile's and the next
+  cplx* sD = sPhi2 + 2 * (size_t)nfun * MFD_TQ;          // [nrow][TQ]
   cplx* sTw = sD + (size_t)a.nrow * MFD_TQ;              // [nact][TQ]
   __shared__ MfdBlock sblk[MFD_MAXB];
   __shared__ int2 scol[MFD_MAXCOL];
@@ -237,23 +237,35 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
   for (int e = tid; e < nfun * nfun; e += MFD_NT) { spo[e] = a.pair_of[e]; spc[e] = a.pair_cj[e]; }
   for (int e = tid; e < nfun; e += MFD_NT) smv[e] = a.mval[e];
 
-  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+  // a tile's W rows and orbitals; row npair of the W slice is zero.  The
+  // copies of tile k + 1 are issued once tile k's DMMA phase has read sW, so
+  // they land while tile k's twfn and v2orbg phase runs (the orbitals are
+  // double-buffered: that phase still reads tile k's).
+  auto stage = [&](int tile, int buf) {
+    if (tile < ntile) {
+      const size_t q0 = (size_t)tile * MFD_TQ;
+      for (int e = tid; e < npair * MFD_TQ; e += MFD_NT) {
+        const int p = e / MFD_TQ, t = e % MFD_TQ;
+        const bool in = q0 + t < ng;
+        mfd_cp16(sW + (size_t)p * MFD_WP + t, a.W + (size_t)p * ng + (in ? q0 + t : 0), in ? 16u : 0u);
+      }
+      cplx* ph = sPhi2 + (size_t)buf * nfun * MFD_TQ;
+      for (int e = tid; e < nfun * MFD_TQ; e += MFD_NT) {
+        const int f = e / MFD_TQ, t = e % MFD_TQ;
+        const bool in = q0 + t < ng;
+        mfd_cp16(ph + e, a.orbg + (size_t)f * ng + (in ? q0 + t : 0), in ? 16u : 0u);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  stage(blockIdx.x, 0);
+  int buf = 0;
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x, buf ^= 1) {
   const size_t q0 = (size_t)tile * MFD_TQ;
-  __syncthreads();  // the previous tile's reads of sW, sPhi, sD, sTw are done
-  // ---- 1. this tile's W rows and orbitals
-  for (int e = tid; e < npair * MFD_TQ; e += MFD_NT) {
-    const int p = e / MFD_TQ, t = e % MFD_TQ;
-    const bool in = q0 + t < ng;
-    mfd_cp16(sW + (size_t)p * MFD_WP + t, a.W + (size_t)p * ng + (in ? q0 + t : 0), in ? 16u : 0u);
-  }
-  for (int e = tid; e < nfun * MFD_TQ; e += MFD_NT) {
-    const int f = e / MFD_TQ, t = e % MFD_TQ;
-    const bool in = q0 + t < ng;
-    mfd_cp16(sPhi + e, a.orbg + (size_t)f * ng + (in ? q0 + t : 0), in ? 16u : 0u);
-  }
-  asm volatile("cp.async.commit_group;" ::: "memory");
+  // ---- 1. this tile's W rows and orbitals (staged during the previous tile)
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
+  const cplx* sPhi = sPhi2 + (size_t)buf * nfun * MFD_TQ;
 
   auto PHI = [&](int f, int t) { return sPhi[(size_t)f * MFD_TQ + t]; };
   auto WXY = [&](int x, int y, int t) {  // W(x, y) at point t from the stored pair
@@ -303,6 +315,8 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
       const int t = e % MFD_TQ;
       if (q0 + t < ng) a.v2orbg[(size_t)(ncore + e / MFD_TQ) * ng + q0 + t] = mkc(0, 0);
     }
+    __syncthreads();  // phase 2's reads of sW are done
+    stage(tile + gridDim.x, buf ^ 1);
     continue;
   }
   // ---- 3. D2V tiles on the tensor cores: each warp runs its (block,
@@ -345,7 +359,8 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
       }
     }
   }
-  __syncthreads();
+  __syncthreads();  // also: phases 2 and 3 have read sW
+  stage(tile + gridDim.x, buf ^ 1);
   // ---- 4. twfn, then v2orbg of the active orbitals
   for (int e = tid; e < nact * MFD_TQ; e += MFD_NT) {
     const int x = e / MFD_TQ, t = e % MFD_TQ;

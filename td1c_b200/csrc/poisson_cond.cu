@@ -302,14 +302,16 @@ __global__ void __launch_bounds__(PSE_NT) ps_share_kernel(PsCondArgs a) {
 }
 
 // 2. per (l, pair chunk): bridge right-hand sides, tridiagonal solve, t.
-// One thread per pair; everything the recurrence reads is staged first.
-constexpr int PSB_NT = 32;
+// One thread per pair; everything the recurrence reads is staged first, by
+// all PSB_STAGE threads of the CTA.
+constexpr int PSB_NT = 32;      // pairs per CTA (threads of the recurrence)
+constexpr int PSB_STAGE = 128;  // threads of the CTA
 
 size_t ps_bridge_smem(int nfe, int nb) {
   return sizeof(cplx) * (size_t)PSB_NT * nfe * 3 + sizeof(double) * 3 * (size_t)nb;
 }
 
-__global__ void __launch_bounds__(PSB_NT) ps_bridge_kernel(PsCondArgs a) {
+__global__ void __launch_bounds__(PSB_STAGE) ps_bridge_kernel(PsCondArgs a) {
   extern __shared__ cplx psb_sm[];
   const PsCond& F = a.f;
   const int l = blockIdx.x, p0 = blockIdx.y * PSB_NT, nb = F.nb, nfe = F.nfe, npair = a.npair, tid = threadIdx.x;
@@ -318,17 +320,17 @@ __global__ void __launch_bounds__(PSB_NT) ps_bridge_kernel(PsCondArgs a) {
   double* tm = reinterpret_cast<double*>(TP + (size_t)PSB_NT * nfe);
   double* tw = tm + nb;
   double* tu = tw + nb;
-  for (int q = tid; q < PSB_NT * nfe * 2; q += PSB_NT) {
+  for (int q = tid; q < PSB_NT * nfe * 2; q += PSB_STAGE) {
     const int r = q / PSB_NT, pc = q % PSB_NT, p = p0 + pc;
     const bool ok = p < npair && ((r & 1) ? r < 2 * nfe - 1 : r >= 2);  // shares that exist
     psc_cp16(CB + q, a.cb + (ok ? ((size_t)l * nfe * 2 + r) * npair + p : 0), ok);
   }
-  for (int q = tid; q < PSB_NT * nfe; q += PSB_NT) {
+  for (int q = tid; q < PSB_NT * nfe; q += PSB_STAGE) {
     const int r = q / PSB_NT, pc = q % PSB_NT, p = p0 + pc;
     const bool ok = p < npair;
     psc_cp16(TP + q, a.tpart + (ok ? ((size_t)l * nfe + r) * npair + p : 0), ok);
   }
-  for (int q = tid; q < nb; q += PSB_NT) {
+  for (int q = tid; q < nb; q += PSB_STAGE) {
     const size_t o = (size_t)l * nb + q;
     psc_cp8(tm + q, F.tm + o, true);
     psc_cp8(tw + q, F.tw + o, true);
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(PSB_NT) ps_bridge_kernel(PsCondArgs a) {
   psc_wait_all();
   __syncthreads();
   const int p = p0 + tid;
-  if (p >= npair) return;
+  if (tid >= PSB_NT || p >= npair) return;
   const int m = a.pair_m[p];
   if (l < (m < 0 ? -m : m)) return;
   cplx* xb = a.xb + (size_t)l * nb * npair + p;  // xb[b * npair]
@@ -546,7 +548,7 @@ int launch_ps_cond(const PsCondArgs& a, cudaStream_t st) {
       if (e != cudaSuccess) return (int)e;
       cur = smem;
     }
-    ps_bridge_kernel<<<dim3(a.L2, (a.npair + PSB_NT - 1) / PSB_NT), PSB_NT, smem, st>>>(a);
+    ps_bridge_kernel<<<dim3(a.L2, (a.npair + PSB_NT - 1) / PSB_NT), PSB_STAGE, smem, st>>>(a);
     rc = (int)cudaGetLastError();
     if (rc) return rc;
   }
