@@ -225,10 +225,14 @@ int launch_ci_rdm(const CiArgs& a, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
-int launch_ci_sigma(const CiArgs& a, int maxsec, cudaStream_t st) {
+int launch_ci_tvec(const CiArgs& a, int maxsec, cudaStream_t st) {
   const int n = a.t.nact;
   dim3 grid((maxsec + 127) / 128, n * n);
   ci_tvec_kernel<<<grid, 128, 0, st>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int launch_ci_sigma(const CiArgs& a, cudaStream_t st) {
   ci_sigma_kernel<<<(a.t.lcic + 3) / 4, 128, 0, st>>>(a);
   return (int)cudaGetLastError();
 }

@@ -1251,14 +1251,17 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
     c.launches += 3;
     // int2e needs only rho2 and v2sph: third stream, overlapping l->theta,
-    // mfprod and the theta->l transforms; joins before smallmat
+    // mfprod and the theta->l transforms; then the CI T vectors, which need
+    // only int2e and the D vectors of the CI chain; joins before smallmat
     if (c.nact > 0) {
       cudaEventRecord(c.ev_i2_fork, st);
       cudaStreamWaitEvent(c.st3, c.ev_i2_fork, 0);
       if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, c.st3));
       else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, c.st3));
+      cudaStreamWaitEvent(c.st3, c.ev_join, 0);
+      rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, c.st3));
       cudaEventRecord(c.ev_i2_join, c.st3);
-      c.launches += 3;
+      c.launches += 4;
       i2_forked = true;
     }
     mark();  // end poisson
@@ -1284,7 +1287,8 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   } else if (c.nact > 0) {
     if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
     else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
-    c.launches += 3;
+    rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, st));  // the CI chain joined before mfprod
+    c.launches += 4;
   }
   mark();  // end int2e (its wait for the third stream)
   SmallArgs sa{};
@@ -1295,13 +1299,14 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   smallmat_kernel<<<1, 256, 0, st>>>(sa);
   c.launches++;
   mark();  // end smallmat
-  // CI sigma (ormas_xact2 -> ormas_hcic) on the side stream, concurrently with dtorb
+  // CI sigma (ormas_xact2 -> ormas_hcic) on the side stream, concurrently with
+  // dtorb (its T vectors were formed after int2e)
   if (c.nact > 0) {
     cudaEventRecord(c.ev_sig_fork, st);
     cudaStreamWaitEvent(c.st2, c.ev_sig_fork, 0);
-    rc |= chk("ci sigma", launch_ci_sigma(ca, c.maxsec, c.st2));
+    rc |= chk("ci sigma", launch_ci_sigma(ca, c.st2));
     cudaEventRecord(c.ev_sig_join, c.st2);
-    c.launches += 2;
+    c.launches += 1;
   } else {
     cudaMemsetAsync(hcic, 0, sizeof(cplx), st);
   }

@@ -213,7 +213,8 @@ struct CiArgs {
 };
 int launch_ci_dvec(const CiArgs& a, int maxsec, cudaStream_t st);
 int launch_ci_rdm(const CiArgs& a, cudaStream_t st);
-int launch_ci_sigma(const CiArgs& a, int maxsec, cudaStream_t st);
+int launch_ci_tvec(const CiArgs& a, int maxsec, cudaStream_t st);  // T_rs = sum_pq (rs|pq) D_pq: int2e and D only
+int launch_ci_sigma(const CiArgs& a, cudaStream_t st);              // sigma from T, D and int1e
 
 // Columns coupled to row ir (1-based radial index) by the FEDVR kinetic and
 // derivative operators: the points of the row's finite element, both

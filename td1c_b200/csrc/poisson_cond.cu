@@ -259,10 +259,12 @@ __global__ void __launch_bounds__(PSE_NT) ps_share_kernel(PsCondArgs a) {
     const bool ok = p < npair && l < L2 && ip >= 1 && ip <= Nr;
     psc_cp16(RHO + pc * S + lc * nd + pt, a.rho2 + (ok ? ((size_t)p * L2 + l) * Nr + ip - 1 : 0), ok);
   }
-  for (int q = tid; q < PSE_LC * (sr / 2); q += PSE_NT) {
-    const int lc = q / (sr / 2), c = q % (sr / 2), l = l0 + lc;
+  {
+    const int lc = tid / (PSE_NT / PSE_LC), l = l0 + lc;  // PSE_NT / LC threads per record
     const bool ok = l < L2;
-    psc_cp16(REC + lc * sr + 2 * c, F.srec + (ok ? ((size_t)l * nfe + e) * sr + 2 * c : 0), ok);
+    const double* src = F.srec + (ok ? ((size_t)l * nfe + e) * sr : 0);
+    for (int c = tid % (PSE_NT / PSE_LC); c < sr / 2; c += PSE_NT / PSE_LC)
+      psc_cp16(REC + lc * sr + 2 * c, src + (ok ? 2 * c : 0), ok);
   }
   for (int q = tid; q < PSE_PC; q += PSE_NT) psc_cp4(PM + q, a.pair_m + (p0 + q < npair ? p0 + q : 0), p0 + q < npair);
   psc_wait_all();
@@ -414,10 +416,12 @@ __global__ void __launch_bounds__(PSE_NT, 3) ps_elem_kernel(PsCondArgs a) {
     const bool ok = p < npair && l < L2;
     psc_cp16(RHO + pc * S + lc * ni + k, a.rho2 + (ok ? ((size_t)p * L2 + l) * Nr + ir0 + k : 0), ok);  // point ir0 + k + 1
   }
-  for (int q = tid; q < PSE_LC * (er / 2); q += PSE_NT) {
-    const int lc = q / (er / 2), c = q % (er / 2), l = l0 + lc;
+  {
+    const int lc = tid / (PSE_NT / PSE_LC), l = l0 + lc;  // PSE_NT / LC threads per record
     const bool ok = l < L2;
-    psc_cp16(REC + lc * er + 2 * c, F.erec + (ok ? ((size_t)l * nfe + e) * er + 2 * c : 0), ok);
+    const double* src = F.erec + (ok ? ((size_t)l * nfe + e) * er : 0);
+    for (int c = tid % (PSE_NT / PSE_LC); c < er / 2; c += PSE_NT / PSE_LC)
+      psc_cp16(REC + lc * er + 2 * c, src + (ok ? 2 * c : 0), ok);
   }
   for (int q = tid; q < 3 * PSE_LC * PSE_PC; q += PSE_NT) {
     // q < 2 LC PC: bridge values (side 0: bridge e - 1, side 1: bridge e), zero where the
@@ -535,6 +539,7 @@ int launch_ps_pass(const PsCondArgs& a, bool share, cudaStream_t st) {
 
 int launch_ps_cond(const PsCondArgs& a, cudaStream_t st) {
   static_assert(PSE_NT == 64 * PSE_LC && PSE_PC == 32, "element pass: two warps of 16 pairs per multipole");
+  static_assert(PSE_NT % PSE_LC == 0, "record staging: PSE_NT / LC threads per record");
   if (a.npair <= 0) return 0;
   if (a.f.nd - 1 > 8 * PSE_MT || a.f.nd - 1 > 4 * PSE_KS) return ST_CONFIG;
   int rc = launch_ps_pass(a, true, st);
