@@ -459,11 +459,19 @@ __global__ void __launch_bounds__(256) smallmat_kernel(SmallArgs a) {
   __syncthreads();
   // ene_act = Re sum int1e(i,j) den1(j,i) + 1/2 Re sum int2e(i,j,k,l) den2(j,i,l,k)
   double part = 0.0;
-  const int n2 = n * n, n4 = n2 * n2;
-  for (int e = tid; e < n4; e += blockDim.x) {
-    int i = e % n, j = (e / n) % n, k = (e / n2) % n, l = e / (n2 * n);
-    cplx p = cmul(a.int2e[e], a.den2[j + n * (i + n * (l + n * k))]);
-    part += 0.5 * p.x;
+  const int n2 = n * n;
+  // thread (ij, g) sums the l = g, g + ng, ... slices of its (i, j): int2e index ij + n2 (k + n l),
+  // den2 index ji + n2 (l + n k), no divisions inside the loop
+  if (n2 > 0) {
+    const int ng = blockDim.x / n2, ij = tid % n2, g = tid / n2;
+    if (g < ng) {
+      const int i = ij % n, j = ij / n, ji = j + n * i;
+      for (int l = g; l < n; l += ng)
+        for (int k = 0; k < n; ++k) {
+          const cplx p = cmul(a.int2e[ij + n2 * (k + n * l)], a.den2[ji + n2 * (l + n * k)]);
+          part += 0.5 * p.x;
+        }
+    }
   }
   for (int e = tid; e < n2; e += blockDim.x) {
     int i = e % n, j = e / n;
@@ -798,8 +806,7 @@ int build_reductions(Ctx& c) {
   c.od.nbas = (int)c.nbas; c.od.nfun = c.nfun; c.od.nent = (int)c.h_ent.size();
   c.od.orb = c.orb; c.od.h0orb = c.h0orb; c.od.h1orb = c.h1orb; c.od.gorb = c.gorb; c.od.v2orb = c.v2orb;
   c.od.ent = dupload(c.h_ent);
-  const int nchunk = (int)((c.nbas + 127) / 128);
-  c.od.partial = dalloc<cplx>((size_t)nchunk * std::max(1, c.od.nent));
+  c.od.partial = dalloc<cplx>((size_t)orbdots_nchunk(c.nbas) * std::max(1, c.od.nent));
   c.od.result = dalloc<cplx>(std::max(1, c.od.nent));
   // int2e blocks by delta = m_i - m_j
   const int n = c.nact, nc = c.ncore;

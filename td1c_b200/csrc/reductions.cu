@@ -85,8 +85,10 @@ __global__ void sum_partials_kernel(const cplx* __restrict__ partial, int nchunk
   if (lane == 0) out[t] = s;
 }
 
+int orbdots_nchunk(size_t nbas) { return (int)((nbas + OD_CHUNK - 1) / OD_CHUNK); }
+
 int launch_orbdots(const OrbdotsArgs& a, cudaStream_t st) {
-  const int nchunk = (a.nbas + OD_CHUNK - 1) / OD_CHUNK;
+  const int nchunk = orbdots_nchunk((size_t)a.nbas);
   size_t smem = sizeof(cplx) * 5 * (size_t)a.nfun * OD_CHUNK;
   static bool attr = false;
   if (!attr) {

@@ -11,6 +11,7 @@ struct OrbdotsArgs {
   cplx* partial;     // [nchunk][nent]
   cplx* result;      // [nent]
 };
+int orbdots_nchunk(size_t nbas);  // chunks (CTAs) of the orbdots pass; the partial buffer holds nchunk x nent
 int launch_orbdots(const OrbdotsArgs& a, cudaStream_t st);
 
 struct Int2eBlock { int row0, nrow, col0, ncol, ent0, pad0, pad1, pad2; };
