@@ -169,6 +169,13 @@ int td1c_gpu_split2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, d
  * alpha = 2, src/prop/cletdrk2.cpp:36-61; tdse_prop12 mask per step). */
 int td1c_gpu_etdrk2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
                     double cep, int maxcyc, double thresh, int use_graph);
+/* ETD-RK4 (cletdrk4::prop, src/prop/cletdrk4.cpp:53-114) with the rational
+ * one-body functions of clh1rat at the default orders 2/2 (clh1rat.cpp:15-47,
+ * h1rat_prod.F90:2-95: numerator by one-body products, each denominator
+ * factor a banded solve with the laser by correction cycles); tdse_prop12
+ * mask per step.  Twelve factor sets are built on the first step. */
+int td1c_gpu_etdrk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                    double cep, int maxcyc, double thresh, int use_graph);
 /* init_prop12 with cletdrk2 (src/main/init.cpp:250-319): per cycle ene[s] =
  * total energy, one zero-field ETD-RK2 step of dt (no mask), td1c_gpu_orth;
  * needs icomp = 0. */

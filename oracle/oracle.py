@@ -48,7 +48,8 @@ def _load():
     lib.orc_dpade_prod.restype = ctypes.c_int
     lib.orc_dpade_prod.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_double, dp]
-    for name in ("orc_split2", "orc_etdrk2"):
+    lib.orc_etd4_fun.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+    for name in ("orc_split2", "orc_etdrk2", "orc_etdrk4"):
         getattr(lib, name).argtypes = [vp, ctypes.POINTER(OrcPulse), ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_double, dp, dp, dp]
     lib.orc_relax_etdrk2.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp]
@@ -213,6 +214,19 @@ class Oracle:
     def etdrk2(self, wfn, cic, t0, dt, nstep, maxcyc=20, thresh=1e-10):
         """ETD-RK2 with the Pade one-body inverse (mask per step); returns (wfn, cic, dipole per step)."""
         return self._prop("orc_etdrk2", wfn, cic, t0, dt, nstep, maxcyc, thresh)
+
+    def etdrk4(self, wfn, cic, t0, dt, nstep, maxcyc=20, thresh=1e-10):
+        """ETD-RK4 with the rational one-body functions of clh1rat (orders 2/2, mask per step);
+        returns (wfn, cic, dipole per step)."""
+        return self._prop("orc_etdrk4", wfn, cic, t0, dt, nstep, maxcyc, thresh)
+
+    def etd4_fun(self, which, dt):
+        """Coefficients of ETD-RK4 function `which` (0 exp1, 1 exp2, 2 gfun, 3 f0, 4 f1, 5 f2):
+        dict n[3], d0[2], d1[2], rk (complex) and dt."""
+        out = np.zeros(17)
+        self.lib.orc_etd4_fun(int(which), float(dt), int(self.wl.get("icomp", 1)), _dp(out))
+        z = out[:16].view(np.complex128)
+        return {"n": z[0:3], "d0": z[3:5], "d1": z[5:7], "rk": z[7], "dt": out[16]}
 
     def relax_etdrk2(self, wfn, cic, dt, ncyc, maxcyc=20, thresh=1e-10):
         """Imaginary-time relaxation with ETD-RK2 steps (icomp = 0); returns (wfn, cic, energy per cycle)."""

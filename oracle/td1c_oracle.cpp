@@ -1383,14 +1383,20 @@ struct Oracle {
   // number of corrections added.
   int dpade_prod(const double* lfield, double dtime, cd alpha, int maxcyc, double thresh, cd* wfn) {
     const cd fac = cfg.icomp == 1 ? IU * dtime / alpha : cd(dtime) / alpha;
+    return shifted_inverse(lfield, fac, maxcyc, thresh, isplit == 1, wfn);
+  }
+  // (1 + fac (T + V))^-1 on the non-frozen orbitals, V of the laser by the
+  // correction cycles (factor -fac lfield(3,1)) when `cycles`: the common
+  // core of dpade_prod and of one denominator factor of h1rat_prod
+  int shifted_inverse(const double* lfield, cd fac, int maxcyc, double thresh, bool cycles, cd* wfn) {
     const auto& lus = h1lu(fac);
     const size_t n = (size_t)nbas * nfun, nf = (size_t)nbas * nfcore;
-    const cd zfac = (cfg.icomp == 1 ? -IU * dtime / alpha : cd(-dtime) / alpha) * lfield[2];
+    const cd zfac = -fac * lfield[2];
     std::vector<cd> o(wfn, wfn + n), h(n, 0.0), t;
     h1inv(lus, o);
     t = o;
     int ncorr = 0;
-    if (isplit == 1) {
+    if (cycles) {
       for (int icyc = 1; icyc <= maxcyc; ++icyc) {
         if (rms_res(o, nfcore) < thresh) break;
         std::fill(h.begin(), h.end(), cd(0.0));
@@ -1403,6 +1409,39 @@ struct Oracle {
     }
     for (size_t k = nf; k < n; ++k) wfn[k] = t[k];
     return ncorr;
+  }
+  // One rational function of the one-body Hamiltonian (clh1rat.cpp:15-47,
+  // h1rat_gen.F90, h1rat_prod.F90:2-95): numerator sum_k n_k (dt H1)^k with
+  // H1 = T + V + laser (hprod_h1tot), then per denominator factor
+  // (d0 + d1 (T + V))^-1 with the laser by correction cycles (real time,
+  // split_type 1), written as (1 + (d1/d0)(T + V))^-1 of the input over d0.
+  struct RatFun {
+    int dimn = 2, dimd = 2;
+    cd n[3], d0[2], d1[2], rk;
+    double dt = 0;
+    cd limit() const { cd d = 1.0; for (int k = 0; k < dimd; ++k) d *= d0[k]; return n[0] / d; }
+  };
+  void h1rat_prod(const double* lfield, const RatFun& F, int maxcyc, double thresh, cd* wfn) {
+    const size_t n = (size_t)nbas * nfun, nf = (size_t)nbas * nfcore;
+    if (isplit == 0) {  // clh1rat::prod with split_type 0: the function at 0
+      const cd lim = F.limit();
+      for (size_t k = nf; k < n; ++k) wfn[k] *= lim;
+      return;
+    }
+    std::vector<cd> o(wfn, wfn + n), t(wfn, wfn + n), h(n);
+    for (size_t k = nf; k < n; ++k) o[k] *= F.n[0];
+    for (int k = 1; k <= F.dimn; ++k) {
+      std::fill(h.begin(), h.end(), cd(0.0));
+      tprod(t, h, nfcore, nfun);
+      laser_dyn(cd(lfield[2]), t, h);
+      for (size_t q = nf; q < n; ++q) { t[q] = F.dt * h[q]; o[q] += F.n[k] * t[q]; }
+    }
+    for (int k = 0; k < F.dimd; ++k) {
+      if (std::abs(F.d1[k]) < 1e-10) continue;  // h1rat_thresh
+      for (size_t q = nf; q < n; ++q) o[q] /= F.d0[k];
+      shifted_inverse(lfield, F.d1[k] / F.d0[k], maxcyc, thresh, isplit == 1 && cfg.icomp == 1, o.data());
+    }
+    for (size_t k = nf; k < n; ++k) wfn[k] = o[k];
   }
 };
 
@@ -1633,6 +1672,120 @@ void orc_etdrk2(void* h, const orc_pulse* p, double t0, double dt, int nstep, in
     mask_orbitals(o, Y);
     if (dip) dip[s] = o->dipole(Y, C);
   }
+}
+// cletdrk4::gen_exp/gen_gfun/gen_f0fun/gen_f1fun/gen_f2fun (cletdrk4.cpp:
+// 134-935) at the default orders etd_dim_numer = etd_dim_denom = 2 (not the
+// pade_old forms): Pade numerators n(x), denominators dfac (x - r0)(x - r1),
+// then x -> tunit dt_f H with tunit = -i (real time) or -1, the numerator
+// times pref, and the CI part times rk
+static Oracle::RatFun etd4_fun(int which, double dt, int icomp) {
+  Oracle::RatFun F;
+  const cd tunit = icomp == 0 ? cd(-1.0) : -IU;
+  const double s3 = std::sqrt(3.0);
+  double nn[3];
+  cd dfac, r0, r1, pref = 1.0, rk = 1.0;
+  double dtf = dt;
+  switch (which) {
+    case 0: case 1:  // exp(x) = (x^2 + 6x + 12) / (x^2 - 6x + 12); exp1 over dt, exp2 over dt/2
+      nn[0] = 12; nn[1] = 6; nn[2] = 1; dfac = 1.0; r0 = cd(3, -s3); r1 = cd(3, s3);
+      dtf = which == 0 ? dt : 0.5 * dt;
+      break;
+    case 2:  // gfun(x) = (exp(x) - 1)/x = (x^2 + 6x + 60) / (3x^2 - 24x + 60), dt/2 gfun(-i H dt/2)
+      nn[0] = 60; nn[1] = 6; nn[2] = 1; dfac = 3.0; r0 = cd(4, -2); r1 = cd(4, 2);
+      dtf = 0.5 * dt; pref = 0.5 * dt; rk = 0.5 * dt;
+      break;
+    case 3:  // f0 = (-4 - x + e^x (4 - 3x + x^2))/x^3
+      nn[0] = 34860; nn[1] = 19620; nn[2] = 2657; dfac = 13260.0;
+      r0 = cd(762.0, -std::sqrt(189762.0)) / 221.0; r1 = cd(762.0, std::sqrt(189762.0)) / 221.0;
+      pref = dt; rk = dt / 6.0;
+      break;
+    case 4:  // f1 = 2 (2 + x + e^x (x - 2))/x^3
+      nn[0] = 2940; nn[1] = 450; nn[2] = 41; dfac = 330.0;
+      r0 = cd(51.0, -std::sqrt(633.0)) / 11.0; r1 = cd(51.0, std::sqrt(633.0)) / 11.0;
+      pref = dt; rk = dt / 3.0;
+      break;
+    default:  // f2 = (-4 - 3x - x^2 + e^x (4 - x))/x^3
+      nn[0] = 1260; nn[1] = -420; nn[2] = -13; dfac = 300.0;
+      r0 = cd(21.0, -3.0 * std::sqrt(21.0)) / 5.0; r1 = cd(21.0, 3.0 * std::sqrt(21.0)) / 5.0;
+      pref = dt; rk = dt / 6.0;
+      break;
+  }
+  cd tt = pref;
+  for (int k = 0; k <= 2; ++k) { F.n[k] = nn[k] * tt; tt *= tunit; }
+  F.d1[0] = dfac * tunit * dtf; F.d0[0] = -dfac * r0;
+  F.d1[1] = tunit * dtf; F.d0[1] = -r1;
+  F.dt = dtf;
+  F.rk = rk;
+  return F;
+}
+// cletdrk4::prop (cletdrk4.cpp:53-114): prod1 = copy, CI times rk, orbitals
+// by the function; prod2 = the same in place on the input, added to the
+// output.  All function products take the field at t + dt/2.
+static void etdrk4_step(Oracle* o, const orc_pulse* p, double t, double dt, int maxcyc, double thresh, cd* Y, cd* C) {
+  const size_t no = (size_t)o->nbas * o->nfun, nc = o->lcic, n = no + nc;
+  Oracle::RatFun fn[6];
+  for (int k = 0; k < 6; ++k) fn[k] = etd4_fun(k, dt, o->cfg.icomp);
+  const Oracle::RatFun &exp1 = fn[0], &exp2 = fn[1], &gfun = fn[2];
+  std::vector<cd> w0(n), w1(n), w2(n), w3(n), h0(n), h1(n), h2(n), h3(n), tw(n), w(n);
+  for (size_t q = 0; q < no; ++q) w0[q] = Y[q];
+  for (size_t q = 0; q < nc; ++q) w0[no + q] = C[q];
+  double lf[9], lh[9];
+  orc_field(p, t + 0.5 * dt, lh);
+  auto prod1 = [&](const Oracle::RatFun& F, const std::vector<cd>& in, std::vector<cd>& out) {
+    out = in;
+    for (size_t q = no; q < n; ++q) out[q] *= F.rk;
+    o->h1rat_prod(lh, F, maxcyc, thresh, out.data());
+  };
+  auto prod2 = [&](const Oracle::RatFun& F, std::vector<cd>& in, std::vector<cd>& out) {
+    for (size_t q = no; q < n; ++q) in[q] *= F.rk;
+    o->h1rat_prod(lh, F, maxcyc, thresh, in.data());
+    for (size_t q = 0; q < n; ++q) out[q] += in[q];
+  };
+  auto htot = [&](double tt, std::vector<cd>& in, std::vector<cd>& out) {
+    orc_field(p, tt, lf);
+    o->htot(1.0, lf, in.data(), in.data() + no, out.data(), out.data() + no);
+  };
+  htot(t, w0, h0);
+  prod1(gfun, h0, w1);
+  prod1(exp2, w0, tw);
+  for (size_t q = 0; q < n; ++q) w1[q] += tw[q];
+  htot(t + 0.5 * dt, w1, h1);
+  prod1(gfun, h1, w2);
+  for (size_t q = 0; q < n; ++q) w2[q] += tw[q];
+  htot(t + 0.5 * dt, w2, h2);
+  for (size_t q = 0; q < n; ++q) tw[q] = 2.0 * h2[q] - h0[q];
+  prod1(gfun, tw, w3);
+  prod1(exp2, w1, tw);
+  for (size_t q = 0; q < n; ++q) w3[q] += tw[q];
+  htot(t + dt, w3, h3);
+  for (size_t q = 0; q < n; ++q) h2[q] += h1[q];
+  prod1(exp1, w0, w);
+  prod2(fn[3], h0, w);
+  prod2(fn[4], h2, w);
+  prod2(fn[5], h3, w);
+  for (size_t q = 0; q < no; ++q) Y[q] = w[q];
+  for (size_t q = 0; q < nc; ++q) C[q] = w[no + q];
+}
+// tdse_prop12 (tdse.cpp:268-310) with H2P = cletdrk4: per step the ETD-RK4
+// update, then wfn_mask
+void orc_etdrk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh, double* wfn,
+                double* cic, double* dip) {
+  Oracle* o = static_cast<Oracle*>(h);
+  cd* Y = reinterpret_cast<cd*>(wfn);
+  cd* C = reinterpret_cast<cd*>(cic);
+  for (int s = 0; s < nstep; ++s) {
+    etdrk4_step(o, p, t0 + dt * s, dt, maxcyc, thresh, Y, C);
+    mask_orbitals(o, Y);
+    if (dip) dip[s] = o->dipole(Y, C);
+  }
+}
+// the scalar coefficients of one ETD-RK4 function (for the device path's tests):
+// out = n0, n1, n2, d0[0], d0[1], d1[0], d1[1] (complex) then dt, rk (complex)
+void orc_etd4_fun(int which, double dt, int icomp, double* out) {
+  const Oracle::RatFun F = etd4_fun(which, dt, icomp);
+  const cd v[8] = {F.n[0], F.n[1], F.n[2], F.d0[0], F.d0[1], F.d1[0], F.d1[1], F.rk};
+  for (int k = 0; k < 8; ++k) { out[2 * k] = v[k].real(); out[2 * k + 1] = v[k].imag(); }
+  out[16] = F.dt;
 }
 // init_prop12 (init.cpp:250-319) with H2P = cletdrk2: per cycle the energy
 // of the current state, one zero-field ETD-RK2 step (no mask), wfn_orth

@@ -99,6 +99,12 @@ void  orc_split2(void* h, const orc_pulse* p, double t0, double dt, int nstep, i
 /* tdse_prop12 with cletdrk2 (+ cldpade, alpha = 2) and wfn_mask per step.   */
 void  orc_etdrk2(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh,
                  double* wfn, double* cic, double* dip);
+/* tdse_prop12 with cletdrk4 (+ clh1rat, default orders 2/2) and wfn_mask
+ * per step; orc_etd4_fun: the coefficients of function `which` (exp1, exp2,
+ * gfun, f0, f1, f2): n0..n2, d0[2], d1[2], rk as (re, im) pairs, then dt.  */
+void  orc_etdrk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh,
+                 double* wfn, double* cic, double* dip);
+void  orc_etd4_fun(int which, double dt, int icomp, double* out);
 /* init_prop12 with cletdrk2: per cycle ene[s], one zero-field ETD-RK2 step
  * (no mask), orc_orth (needs icomp = 0).                                     */
 void  orc_relax_etdrk2(void* h, double dt, int ncyc, int maxcyc, double thresh, double* wfn, double* cic,

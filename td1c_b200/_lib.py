@@ -88,7 +88,7 @@ def load():
     lib.td1c_gpu_h1itr.argtypes = [vp, dp, c_double, c_int, c_double, ip]
     lib.td1c_gpu_dpade.restype = c_int
     lib.td1c_gpu_dpade.argtypes = [vp, dp, c_double, c_double, c_double, c_int, c_double, ip]
-    for name in ("td1c_gpu_split2", "td1c_gpu_etdrk2"):
+    for name in ("td1c_gpu_split2", "td1c_gpu_etdrk2", "td1c_gpu_etdrk4"):
         getattr(lib, name).restype = c_int
         getattr(lib, name).argtypes = [vp, vp, c_double, c_double, c_int, c_double, c_double, c_double, c_double,
                                        c_int, c_double, c_int]
@@ -109,6 +109,6 @@ EXPORTED = [
     "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
     "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset", "td1c_gpu_int2e_static", "td1c_gpu_dipole",
     "td1c_gpu_orth", "td1c_gpu_relax", "td1c_gpu_bind_split", "td1c_gpu_h1itr", "td1c_gpu_dpade",
-    "td1c_gpu_split2", "td1c_gpu_etdrk2", "td1c_gpu_relax_etdrk2",
+    "td1c_gpu_split2", "td1c_gpu_etdrk2", "td1c_gpu_etdrk4", "td1c_gpu_relax_etdrk2",
     "h1itr_gen_cninv_", "h1itr_prop_", "dpade_gen_", "dpade_prod_",
 ]

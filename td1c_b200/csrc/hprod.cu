@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -140,7 +141,8 @@ struct Ctx {
   cplx *relax_hw = nullptr, *relax_hc = nullptr;  // RHS outputs of the energy evaluation in td1c_gpu_relax
   // one-body propagators: condensed factors of 1 + c T per c, and scratch
   struct H1Slot { double cre = 0, cim = 0; H1Fac f; };
-  H1Slot h1slot[4];
+  static constexpr int kH1Slots = 16;  // factor sets kept: split2/ETD-RK2 use 1-2, ETD-RK4 12
+  H1Slot h1slot[kH1Slots];
   int n_h1 = 0;
   cplx* h1_z[2] = {nullptr, nullptr};  // interior solutions (alternating passes)
   cplx *h1_cb = nullptr, *h1_xb = nullptr;  // bridge shares, bridge values
@@ -1383,6 +1385,12 @@ __global__ void lincomb_kernel(size_t n, cplx* __restrict__ z, const cplx* __res
   else { o.x = (xv.x - yv.x) * a; o.y = (xv.y - yv.y) * a; }
   z[t] = o;
 }
+// z = a x + b y with complex a, b (the complex axpy / scal of clh1rat)
+__global__ void zaxpby_kernel(size_t n, cplx* z, const cplx* x, const cplx* y, cplx a, cplx b) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  z[t] = cadd(cmul(a, x[t]), cmul(b, y[t]));
+}
 __global__ void counter_inc_kernel(int* counter) { if (threadIdx.x == 0) *counter += 1; }
 
 // sin^2 pulse (clfield1.cpp:15-115 set-up, 253-300 E explicit, 472-500
@@ -1430,12 +1438,12 @@ struct RkBufs {
   const void* g_y = nullptr; const void* g_yc = nullptr; const void* g_tab = nullptr;
   const void* g_ro = nullptr; double g_dt = 0; long g_per = 0;
   int h_counter[2] = {0, 0};
-  // cached graphs of one split2 / ETD-RK2 step
-  const void* s_y[2] = {nullptr, nullptr}; const void* s_yc[2] = {nullptr, nullptr};
-  const void* s_tab[2] = {nullptr, nullptr}; double s_dt[2] = {0, 0}; int s_cyc[2] = {0, 0}; double s_thr[2] = {0, 0};
-  int s_split[2] = {-1, -1}; int s_mask[2] = {-1, -1}; long s_per[2] = {0, 0};
-  const void* s_ro[2] = {nullptr, nullptr};
-  int g_ctl = -1, s_ctl[2] = {-1, -1};  // control flags (icomp, igauge) the graphs were captured with
+  // cached graphs of one split2 / ETD-RK2 / ETD-RK4 step
+  const void* s_y[3] = {nullptr, nullptr, nullptr}; const void* s_yc[3] = {nullptr, nullptr, nullptr};
+  const void* s_tab[3] = {nullptr, nullptr, nullptr}; double s_dt[3] = {0, 0, 0}; int s_cyc[3] = {0, 0, 0};
+  double s_thr[3] = {0, 0, 0}; int s_split[3] = {-1, -1, -1}; int s_mask[3] = {-1, -1, -1}; long s_per[3] = {0, 0, 0};
+  const void* s_ro[3] = {nullptr, nullptr, nullptr};
+  int g_ctl = -1, s_ctl[3] = {-1, -1, -1};  // control flags (icomp, igauge) the graphs were captured with
 };
 RkBufs g_rk;
 
@@ -1451,7 +1459,7 @@ int h1_factor(Ctx& c, cplx fac, H1Fac* out) {
   for (int i = 0; i < c.n_h1 && !sl; ++i)
     if (std::isnan(c.h1slot[i].cre)) sl = &c.h1slot[i];  // invalidated by a change of T
   if (sl) {
-  } else if (c.n_h1 < 4) {
+  } else if (c.n_h1 < Ctx::kH1Slots) {
     sl = &c.h1slot[c.n_h1++];
     H1Fac& f = sl->f;
     f.nfe = c.nfe; f.nd = c.nd; f.ni = c.nd - 1; f.nb = c.nfe - 1; f.L1 = c.L1;
@@ -1462,8 +1470,8 @@ int h1_factor(Ctx& c, cplx fac, H1Fac* out) {
     f.tpiv = dalloc<int>(nbt);
   } else {
     // all slots taken: rebuild the oldest in place
-    for (int i = 0; i < 3; ++i) std::swap(c.h1slot[i], c.h1slot[i + 1]);
-    sl = &c.h1slot[3];
+    for (int i = 0; i < Ctx::kH1Slots - 1; ++i) std::swap(c.h1slot[i], c.h1slot[i + 1]);
+    sl = &c.h1slot[Ctx::kH1Slots - 1];
   }
   sl->cre = fac.x; sl->cim = fac.y;
   H1FacSrc src{};
@@ -1496,10 +1504,10 @@ int h1_bufs(Ctx& c) {
 // first element pass and bridge solve, maxcyc correction cycles (element +
 // bridge pass, skipped on the device once the residual norm is below thresh)
 // and a last pass that adds the final correction.
+int h1_run(Ctx& c, bool pade, cplx fac, cplx zf0, bool allow_cycles, const double* d_lf, cplx* wfn, int maxcyc,
+           double thresh);
+
 int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cplx alpha, int maxcyc, double thresh) {
-  cudaStream_t st = c.st;
-  int rc = h1_bufs(c);
-  if (rc) return rc;
   const bool rt = c.icomp == 1;
   cplx fac, zf0;  // M = 1 + fac T; laser factor zf0 * lfield[2]
   if (pade) {
@@ -1511,6 +1519,17 @@ int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cpl
     fac = rt ? mkc(0, dtime * 0.5) : mkc(dtime * 0.5, 0);
     zf0 = rt ? mkc(0, -dtime * 0.5) : mkc(-dtime * 0.5, 0);
   }
+  return h1_run(c, pade, fac, zf0, true, d_lf, wfn, maxcyc, thresh);
+}
+
+// h1itr (pade false) or the shifted inverse (1 + fac (T + V))^-1 (pade true)
+// of the non-frozen orbitals, the laser by correction cycles of factor
+// zf0 lfield[2] when isplit is 1 and allow_cycles
+int h1_run(Ctx& c, bool pade, cplx fac, cplx zf0, bool allow_cycles, const double* d_lf, cplx* wfn, int maxcyc,
+           double thresh) {
+  cudaStream_t st = c.st;
+  int rc = h1_bufs(c);
+  if (rc) return rc;
   H1Fac F;
   rc = h1_factor(c, fac, &F);
   if (rc) return rc;
@@ -1537,7 +1556,7 @@ int h1_apply(Ctx& c, bool pade, const double* d_lf, cplx* wfn, double dtime, cpl
   rc |= launch_h1bridge(E, st);
   c.launches += 2;
   zb = 1 - zb;
-  const bool cycles = c.isplit == 1 && maxcyc > 0;
+  const bool cycles = c.isplit == 1 && maxcyc > 0 && allow_cycles;
   cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(st, &cst);
   if (cycles && cst == cudaStreamCaptureStatusActive) {
@@ -1704,7 +1723,159 @@ int etdrk2_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double 
   return rc;
 }
 
-// Propagation driver of td1c_gpu_rk4 / _split2 / _etdrk2 (kind 0 / 1 / 2):
+// ETD-RK4 (cletdrk4.cpp) with clh1rat (clh1rat.cpp, h1rat_gen.F90,
+// h1rat_prod.F90:2-95) at the default orders etd_dim_numer = etd_dim_denom
+// = 2.  Each of the six functions is a Pade form n(x) / (dfac (x - r0)(x - r1))
+// of x = tunit dt_f H (tunit = -i in real time, -1 in imaginary time), with
+// the numerator times pref and the CI part times rk (cletdrk4::gen_exp,
+// gen_gfun, gen_f0fun, gen_f1fun, gen_f2fun, cletdrk4.cpp:134-935).
+struct Etd4Fun {
+  cplx n[3], d0[2], d1[2], rk;
+  double dt;
+};
+Etd4Fun etd4_fun(int which, double dt, int icomp) {
+  const std::complex<double> I(0.0, 1.0), tunit = icomp == 0 ? std::complex<double>(-1.0) : -I;
+  const double s3 = std::sqrt(3.0);
+  double nn[3] = {0, 0, 0}, dfac = 1.0, dtf = dt, pref = 1.0, rk = 1.0;
+  std::complex<double> r0, r1;
+  switch (which) {
+    case 0: case 1:  // exp(x) = (x^2 + 6x + 12) / (x^2 - 6x + 12): exp1 over dt, exp2 over dt/2
+      nn[0] = 12; nn[1] = 6; nn[2] = 1; r0 = {3, -s3}; r1 = {3, s3}; dtf = which == 0 ? dt : 0.5 * dt;
+      break;
+    case 2:  // (exp(x) - 1)/x = (x^2 + 6x + 60) / (3x^2 - 24x + 60), times dt/2 over dt/2
+      nn[0] = 60; nn[1] = 6; nn[2] = 1; dfac = 3; r0 = {4, -2}; r1 = {4, 2}; dtf = 0.5 * dt; pref = rk = 0.5 * dt;
+      break;
+    case 3:  // (-4 - x + e^x (4 - 3x + x^2))/x^3
+      nn[0] = 34860; nn[1] = 19620; nn[2] = 2657; dfac = 13260;
+      r0 = std::complex<double>(762.0, -std::sqrt(189762.0)) / 221.0; r1 = std::conj(r0); pref = dt; rk = dt / 6.0;
+      break;
+    case 4:  // 2 (2 + x + e^x (x - 2))/x^3
+      nn[0] = 2940; nn[1] = 450; nn[2] = 41; dfac = 330;
+      r0 = std::complex<double>(51.0, -std::sqrt(633.0)) / 11.0; r1 = std::conj(r0); pref = dt; rk = dt / 3.0;
+      break;
+    default:  // (-4 - 3x - x^2 + e^x (4 - x))/x^3
+      nn[0] = 1260; nn[1] = -420; nn[2] = -13; dfac = 300;
+      r0 = std::complex<double>(21.0, -3.0 * std::sqrt(21.0)) / 5.0; r1 = std::conj(r0); pref = dt; rk = dt / 6.0;
+      break;
+  }
+  auto C = [](std::complex<double> z) { return mkc(z.real(), z.imag()); };
+  Etd4Fun F;
+  std::complex<double> tt = pref;
+  for (int k = 0; k <= 2; ++k) { F.n[k] = C(nn[k] * tt); tt *= tunit; }
+  F.d1[0] = C(dfac * tunit * dtf); F.d0[0] = C(-dfac * r0);
+  F.d1[1] = C(tunit * dtf); F.d0[1] = C(-r1);
+  F.rk = mkc(rk, 0);
+  F.dt = dtf;
+  return F;
+}
+
+struct Etd4Bufs {
+  cplx *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *h2 = nullptr, *h3 = nullptr, *tmp = nullptr;
+  size_t cap = 0;
+};
+Etd4Bufs g_e4;
+
+void zaxpby(Ctx& c, size_t n, cplx* z, const cplx* x, const cplx* y, cplx a, cplx b) {
+  if (!n) return;
+  zaxpby_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c.st>>>(n, z, x, y, a, b);
+  c.launches++;
+}
+
+// clh1rat::prod on the orbitals w: numerator sum_k n_k (dt H1)^k, H1 = T + V
+// + laser (hprod_h1tot: the one-body kernel's h0 + h1), then per denominator
+// factor (d0 + d1 (T + V))^-1 as the shifted inverse with fac = d1/d0 of the
+// input over d0 (laser by correction cycles in real time, isplit 1).  With
+// isplit 0 the orbitals are scaled by the function's value at 0.
+int h1rat_run(Ctx& c, const Etd4Fun& F, const double* d_lf, cplx* w, int maxcyc, double thresh) {
+  const size_t nf = c.nbas * c.nfcore, nd = c.nbas * (c.nfun - c.nfcore), no = c.nbas * c.nfun;
+  cudaStream_t st = c.st;
+  if (c.isplit == 0) {
+    cplx lim = F.n[0];
+    for (int k = 0; k < 2; ++k) {
+      const double den = F.d0[k].x * F.d0[k].x + F.d0[k].y * F.d0[k].y;
+      lim = cmul(lim, mkc(F.d0[k].x / den, -F.d0[k].y / den));
+    }
+    zaxpby(c, nd, w + nf, w + nf, w + nf, lim, mkc(0, 0));
+    return 0;
+  }
+  int rc = 0;
+  cplx* t = g_e4.tmp;
+  cudaMemcpyAsync(t, w, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  zaxpby(c, nd, w + nf, w + nf, w + nf, F.n[0], mkc(0, 0));
+  OneBodyArgs ob{};
+  ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = c.nfcore; ob.mmax1 = c.mmax1; ob.igauge = c.igauge;
+  ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
+  ob.mval = c.d_mval; ob.orb = t; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = d_lf;
+  for (int k = 1; k <= 2; ++k) {
+    rc |= launch_onebody(ob, st);
+    c.launches++;
+    zaxpby(c, nd, t + nf, c.h0orb + nf, c.h1orb + nf, mkc(F.dt, 0), mkc(F.dt, 0));  // t = dt H1 t
+    zaxpby(c, nd, w + nf, w + nf, t + nf, mkc(1, 0), F.n[k]);
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (std::hypot(F.d1[k].x, F.d1[k].y) < 1e-10) continue;  // h1rat_thresh
+    const double den = F.d0[k].x * F.d0[k].x + F.d0[k].y * F.d0[k].y;
+    const cplx inv0 = mkc(F.d0[k].x / den, -F.d0[k].y / den);
+    zaxpby(c, nd, w + nf, w + nf, w + nf, inv0, mkc(0, 0));
+    const cplx fac = cmul(F.d1[k], inv0);
+    rc |= h1_run(c, true, fac, mkc(-fac.x, -fac.y), c.icomp == 1, d_lf, w, maxcyc, thresh);
+  }
+  return rc ? ST_CUDA : 0;
+}
+
+// cletdrk4::prop (cletdrk4.cpp:53-114) and wfn_mask (tdse_prop12).  Step
+// fields: t, t + dt/2, t + dt; every function product takes t + dt/2.
+int etdrk4_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double thresh, bool do_mask) {
+  cudaStream_t st = c.st;
+  step_begin(c, y_orb, y_cic, 27);
+  RkBufs& b = g_rk;
+  Etd4Bufs& e = g_e4;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic, n = no + nc;
+  const double* lf = b.lf_cur;
+  const double* lh = lf + 9;
+  Etd4Fun fn[6];
+  for (int k = 0; k < 6; ++k) fn[k] = etd4_fun(k, dt, c.icomp);
+  const cplx one = mkc(1, 0), zero = mkc(0, 0);
+  int rc = 0;
+  // prod1: out = in, CI times rk, orbitals by the function
+  auto prod1 = [&](const Etd4Fun& F, const cplx* in, cplx* out) {
+    cudaMemcpyAsync(out, in, n * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+    zaxpby(c, nc, out + no, out + no, out + no, F.rk, zero);
+    rc |= h1rat_run(c, F, lh, out, maxcyc, thresh);
+  };
+  cplx *W0 = b.y0, *tW = b.yt, *H0 = b.k, *H1 = b.k2;
+  cudaMemcpyAsync(W0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(W0 + no, y_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  rc |= run_htot(c, lf, W0, W0 + no, H0, H0 + no, 1.0);
+  prod1(fn[2], H0, e.w1);
+  prod1(fn[1], W0, tW);
+  zaxpby(c, n, e.w1, e.w1, tW, one, one);
+  rc |= run_htot(c, lf + 9, e.w1, e.w1 + no, H1, H1 + no, 1.0);
+  prod1(fn[2], H1, e.w2);
+  zaxpby(c, n, e.w2, e.w2, tW, one, one);
+  rc |= run_htot(c, lf + 9, e.w2, e.w2 + no, e.h2, e.h2 + no, 1.0);
+  zaxpby(c, n, tW, e.h2, H0, mkc(2, 0), mkc(-1, 0));
+  prod1(fn[2], tW, e.w3);
+  prod1(fn[1], e.w1, tW);
+  zaxpby(c, n, e.w3, e.w3, tW, one, one);
+  rc |= run_htot(c, lf + 18, e.w3, e.w3 + no, e.h3, e.h3 + no, 1.0);
+  zaxpby(c, n, e.h2, e.h2, H1, one, one);
+  // Wfn = exp1 Wfn0 + f0 hWfn0 + f1 (hWfn1 + hWfn2) + f2 hWfn3 (prod2 works in place on its input)
+  prod1(fn[0], W0, tW);
+  const int fi[3] = {3, 4, 5};
+  cplx* hin[3] = {H0, e.h2, e.h3};
+  for (int q = 0; q < 3; ++q) {
+    zaxpby(c, nc, hin[q] + no, hin[q] + no, hin[q] + no, fn[fi[q]].rk, zero);
+    rc |= h1rat_run(c, fn[fi[q]], lh, hin[q], maxcyc, thresh);
+    zaxpby(c, n, tW, tW, hin[q], one, one);
+  }
+  cudaMemcpyAsync(y_orb, tW, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(y_cic, tW + no, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  rc |= step_end(c, y_orb, do_mask);
+  return rc;
+}
+
+// Propagation driver of td1c_gpu_rk4 / _split2 / _etdrk2 / _etdrk4 (kind 0 / 1 / 2 / 3):
 // stages the fields of every step, then runs the steps eagerly or as one
 // CUDA graph per step (captured after one eager step that does the first-call
 // set-up: factor tables, scratch, kernel attributes).
@@ -1722,6 +1893,11 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
     if (!b.lf_cur) { b.lf_cur = dalloc<double>(54); b.counter = dalloc<int>(2); }
     b.cap = no + nc;
   }
+  if (kind == 3 && g_e4.cap < no + nc) {
+    Etd4Bufs& e = g_e4;
+    for (cplx** q : {&e.w1, &e.w2, &e.w3, &e.h2, &e.h3, &e.tmp}) *q = dalloc<cplx>(no + nc);
+    e.cap = no + nc;
+  }
   // fields of every step: RK4 stages t + dt c_s (clcrk.cpp:62-73); split2
   // adds the two h1itr fields; ETD-RK2 uses t and t + dt
   Pulse p;
@@ -1730,8 +1906,9 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
   static const double nodes_rk[4] = {0.0, 0.5, 0.5, 1.0};
   static const double nodes_s2[6] = {0.0, 0.5, 0.5, 1.0, 0.25, 0.75};
   static const double nodes_etd[2] = {0.0, 1.0};
-  const double* nodes = kind == 0 ? nodes_rk : (kind == 1 ? nodes_s2 : nodes_etd);
-  const int nf = kind == 0 ? 4 : (kind == 1 ? 6 : 2), per = 9 * nf;
+  static const double nodes_etd4[3] = {0.0, 0.5, 1.0};
+  const double* nodes = kind == 0 ? nodes_rk : (kind == 1 ? nodes_s2 : (kind == 2 ? nodes_etd : nodes_etd4));
+  const int nf = kind == 0 ? 4 : (kind == 1 ? 6 : (kind == 2 ? 2 : 3)), per = 9 * nf;
   std::vector<double> tab((size_t)nstep * per);
   for (int s = 0; s < nstep; ++s)
     for (int is = 0; is < nf; ++is) pulse_lfield(p, t0 + dt * s + dt * nodes[is], &tab[(size_t)s * per + 9 * is]);
@@ -1750,7 +1927,8 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
   auto step = [&]() -> int {
     if (kind == 0) return rk_step(c, y, yc, dt);
     if (kind == 1) return split2_step(c, y, yc, dt, maxcyc, thresh, do_mask);
-    return etdrk2_step(c, y, yc, dt, maxcyc, thresh, do_mask);
+    if (kind == 2) return etdrk2_step(c, y, yc, dt, maxcyc, thresh, do_mask);
+    return etdrk4_step(c, y, yc, dt, maxcyc, thresh, do_mask);
   };
   int rc = 0;
   if (!use_graph) {
@@ -1993,6 +2171,7 @@ void hprod_final_(void) {
   for (void* p : g_allocs) cudaFree(p);
   g_allocs.clear();
   g_rk = RkBufs();
+  g_e4 = Etd4Bufs();
   delete g;
   g = nullptr;
 }
@@ -2119,6 +2298,11 @@ int td1c_gpu_split2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, d
 int td1c_gpu_etdrk2(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
                     double cep, int maxcyc, double thresh, int use_graph) {
   return prop_run(2, d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, maxcyc, thresh, use_graph);
+}
+
+int td1c_gpu_etdrk4(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                    double cep, int maxcyc, double thresh, int use_graph) {
+  return prop_run(3, d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, maxcyc, thresh, use_graph);
 }
 
 // one h1itr_prop / dpade_prod on a device-resident state; cycles = correction

@@ -198,6 +198,10 @@ class HProd:
         """ETD-RK2 steps with the Pade one-body inverse (cletdrk2 + cldpade, mask) in place."""
         self._prop_dev(self.lib.td1c_gpu_etdrk2, d_wfn, d_cic, t0, dt, nstep, maxcyc, thresh, use_graph)
 
+    def etdrk4_dev(self, d_wfn, d_cic, t0, dt, nstep, maxcyc=20, thresh=1e-10, use_graph=True):
+        """ETD-RK4 steps with the rational one-body functions (cletdrk4 + clh1rat, orders 2/2, mask) in place."""
+        self._prop_dev(self.lib.td1c_gpu_etdrk4, d_wfn, d_cic, t0, dt, nstep, maxcyc, thresh, use_graph)
+
     def relax_etdrk2_dev(self, d_wfn, d_cic, dt, ncyc, maxcyc=20, thresh=1e-10):
         """Imaginary-time relaxation with ETD-RK2 steps (icomp = 0); returns the energy per cycle."""
         ene = np.zeros(max(1, int(ncyc)))

@@ -4,7 +4,8 @@ h1itr_prop (Crank-Nicolson of the one-body Hamiltonian with correction
 cycles for the laser coupling) and dpade_prod (the Pade inverse of ETD-RK2)
 on the device against the oracle's banded-LU restatement, through the device
 entry points and the drop-in symbols; split2 (h1itr + RK4 on the two-body
-RHS) and ETD-RK2 trajectories with their dipole traces; imaginary-time
+RHS), ETD-RK2 and ETD-RK4 (the rational one-body functions of clh1rat)
+trajectories with their dipole traces; imaginary-time
 relaxation with ETD-RK2 steps; the full-size Ne grid for the one-body step
 and a stability run at the workload's dt = 0.004.  Tolerance 1e-10 relative.
 """
@@ -94,10 +95,11 @@ def test_one_body_step_cycle_cap(cuda_ok):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["split2", "etdrk2"])
+@pytest.mark.parametrize("kind", ["split2", "etdrk2", "etdrk4"])
 @pytest.mark.parametrize("wl", [W.NE_SMALL, W.MIXED_SMALL, W.LENGTH_SMALL, W.HE_SMALL], ids=lambda w: w["name"])
 def test_split_trajectory(cuda_ok, wl, kind):
-    """dt = 0.01: outside full-H RK4's stability region on these grids."""
+    """dt = 0.01: outside full-H RK4's stability region on these grids.  etdrk4: cletdrk4 with
+    the twelve rational one-body factors of clh1rat (orders 2/2)."""
     import torch
     o, h, orb, cic = _setup(dict(wl, split_type=1))
     try:
@@ -108,7 +110,7 @@ def test_split_trajectory(cuda_ok, wl, kind):
         d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
         d_cic = torch.from_numpy(cic.copy()).cuda()
         h.rk4_reset(None, None)
-        step = h.split2_dev if kind == "split2" else h.etdrk2_dev
+        step = {"split2": h.split2_dev, "etdrk2": h.etdrk2_dev, "etdrk4": h.etdrk4_dev}[kind]
         dip_g = []
         for s in range(nstep):
             step(d_orb.data_ptr(), d_cic.data_ptr(), t0 + s * dt, dt, 1)

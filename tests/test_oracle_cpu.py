@@ -265,3 +265,35 @@ def test_split_propagators_beyond_rk4_limit():
     o.set_split(0)
     w, c, dip = o.rk4(orb, cic, 10.0, 0.05, 3)
     assert not np.all(np.abs(w) < 10)  # full-H RK4 blows up at this step
+
+
+def test_etdrk4_functions_and_order():
+    """cletdrk4's rational one-body functions (orders 2/2, as restated in the oracle) against the
+    exact exp / phi functions they approximate, and fourth-order convergence of the ETD-RK4
+    trajectory (mask moved outside the grid) against a fine split2 reference."""
+    from oracle.oracle import Oracle
+    from .helpers import oracle_state
+    wl = dict(W.HE_SMALL, split_type=1, rmask=1e9)
+    o = Oracle(wl)
+    o.set_split(1)
+    dt = 0.01
+    g = lambda x: (np.exp(x) - 1) / x
+    f0 = lambda x: (-4 - x + np.exp(x) * (4 - 3 * x + x * x)) / x**3
+    f1 = lambda x: 2 * (2 + x + np.exp(x) * (x - 2)) / x**3
+    f2 = lambda x: (-4 - 3 * x - x * x + np.exp(x) * (4 - x)) / x**3
+    exact = [lambda l: np.exp(-1j * l * dt), lambda l: np.exp(-1j * l * dt / 2), lambda l: dt / 2 * g(-1j * l * dt / 2),
+             lambda l: dt * f0(-1j * l * dt), lambda l: dt * f1(-1j * l * dt), lambda l: dt * f2(-1j * l * dt)]
+    for w in range(6):
+        F = o.etd4_fun(w, dt)
+        for lam in (3.0, 30.0):
+            num = sum(F["n"][k] * (F["dt"] * lam) ** k for k in range(3))
+            den = np.prod([F["d0"][k] + F["d1"][k] * lam for k in range(2)])
+            assert abs(num / den - exact[w](lam)) < 1e-5 * abs(exact[w](lam)), (w, lam)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    orb, cic = o.orth(orb, cic)
+    freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+    t0, T = 0.3 * wl["numcyc"] * 2 * np.pi / freq, 0.04
+    ref = o.split2(orb, cic, t0, T / 400, 400)[0]
+    err = [np.linalg.norm(o.etdrk4(orb, cic, t0, T / n, n)[0] - ref) / np.linalg.norm(ref) for n in (4, 8)]
+    assert err[1] < 1e-6 and err[0] / err[1] > 10, err
