@@ -130,6 +130,14 @@ long td1c_gpu_debug_get(const char* name, double* out, long capacity);
  * applied as the unit-field length-gauge coupling.  Uses the library stream
  * and its 1-RDM buffers; returns when the value is on the host. */
 int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out);
+/* hprod_dipole (src/hprod/hprod_dipole.F90:2-146) of a device state without
+ * frozen-core orbitals: out[9] = dip(1:3), vel(1:3), acc(1:3) (length,
+ * velocity and acceleration forms by the Ehrenfest traces hprod_trace1 of z,
+ * p_z and the nuclear acceleration operator, plus A_z N in the velocity
+ * gauge and -E_z N; the second components are 0).  lfield: host lfield(3,3).
+ * ST_CONFIG with frozen-core orbitals: their generalized-Fock corrections
+ * (hprod_gfock, hprod_projfc) are not built. */
+int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
 
 /* wfn_orth_cic + wfn_orth_orb (src/wfn/wfn_orth.F90:2-110): normalise the CI
  * vector and Gram-Schmidt the non-frozen orbitals against all earlier

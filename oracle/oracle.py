@@ -49,6 +49,8 @@ def _load():
     lib.orc_dpade_prod.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_double, dp]
     lib.orc_etd4_fun.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+    lib.orc_dipole3.restype = ctypes.c_int
+    lib.orc_dipole3.argtypes = [vp, dp, dp, dp, dp]
     for name in ("orc_split2", "orc_etdrk2", "orc_etdrk4"):
         getattr(lib, name).argtypes = [vp, ctypes.POINTER(OrcPulse), ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_double, dp, dp, dp]
@@ -219,6 +221,15 @@ class Oracle:
         """ETD-RK4 with the rational one-body functions of clh1rat (orders 2/2, mask per step);
         returns (wfn, cic, dipole per step)."""
         return self._prop("orc_etdrk4", wfn, cic, t0, dt, nstep, maxcyc, thresh)
+
+    def dipole3(self, wfn, cic, lfield):
+        """hprod_dipole without frozen-core orbitals: (dip[3], vel[3], acc[3]); None with a frozen core."""
+        wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
+        cic = np.ascontiguousarray(cic, dtype=np.complex128)
+        out = np.zeros(9)
+        rc = self.lib.orc_dipole3(self.h, _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)),
+                                  _dp(np.ascontiguousarray(lfield, dtype=np.float64)), _dp(out))
+        return None if rc else (out[0:3], out[3:6], out[6:9])
 
     def etd4_fun(self, which, dt):
         """Coefficients of ETD-RK4 function `which` (0 exp1, 1 exp2, 2 gfun, 3 f0, 4 f1, 5 f2):

@@ -1282,15 +1282,55 @@ struct Oracle {
     std::vector<cd> zo((size_t)nbas * nfun, 0.0), w(wfn, wfn + (size_t)nbas * nfun);
     zprod(1.0, w, zo, 0, nfun);
     mkden1(cic);
+    return trace1(w, zo).real();
+  }
+  // hprod_trace1(.true., den1, w, pw) (hprod_trace1.F90:2-88) with the current den1:
+  // 2 sum_core <w_f|pw_f> + sum_{ia, ja, m equal} <w_i|pw_j> den1(ja, ia)
+  cd trace1(const std::vector<cd>& w, const std::vector<cd>& pw) {
     cd s = 0.0;
-    for (int f = 0; f < ncore; ++f) s += 2.0 * dot_orb(w, f, zo, f);
+    for (int f = 0; f < ncore; ++f) s += 2.0 * dot_orb(w, f, pw, f);
     for (int ia = 0; ia < nact; ++ia)
       for (int ja = 0; ja < nact; ++ja) {
         int ifn = ncore + ia, jfn = ncore + ja;
         if (mval[ifn] != mval[jfn]) continue;
-        s += dot_orb(w, ifn, zo, jfn) * D1(den1, ja, ia);
+        s += dot_orb(w, ifn, pw, jfn) * D1(den1, ja, ia);
       }
-    return s.real();
+    return s;
+  }
+  // hprod_azprod (hprod_azprod.F90:100-135) with the plain-nucleus table
+  // bas_azfac(r, l, m) = -alph_lm(l, m) Z / r^2 (bas_gen_azfac.F90:68-72)
+  void azprod(cd zfac, const std::vector<cd>& w, std::vector<cd>& h, int f0, int f1) {
+    for (int f = f0; f < f1; ++f) {
+      int m = mval[f];
+      for (int l = std::abs(m); l <= lmax1 - 1; ++l) {
+        double a = alph[(m + mmax1) * L1 + l];
+        for (int ir = 0; ir < Nr; ++ir) {
+          const double x = xrad[ir + 1];
+          cd tmp = zfac * (-a * cfg.znuc / (x * x));
+          h[io(ir, l, f)] += w[io(ir, l + 1, f)] * tmp;
+          h[io(ir, l + 1, f)] += w[io(ir, l, f)] * tmp;
+        }
+      }
+    }
+  }
+  // hprod_dipole (hprod_dipole.F90:2-146) for a state without frozen-core
+  // orbitals (no generalized-Fock corrections, no pseudopotential): the
+  // length, velocity and acceleration forms by the Ehrenfest traces,
+  // out = dip(1:3), vel(1:3), acc(1:3).  Returns -1 with a frozen core.
+  int dipole3(const cd* wfn, const cd* cic, const double* lf, double* out) {
+    if (nfcore > 0) return -1;
+    const size_t n = (size_t)nbas * nfun;
+    std::vector<cd> w(wfn, wfn + n), zo(n, 0.0), po(n, 0.0), ao(n, 0.0);
+    mkden1(cic);
+    zprod(1.0, w, zo, 0, nfun);
+    pzprod(1.0, w, po, 0, nfun);
+    azprod(1.0, w, ao, 0, nfun);
+    double d = trace1(w, zo).real(), v = trace1(w, po).real(), a = trace1(w, ao).real();
+    if (cfg.igauge == 1) v += lf[8] * neltot;  // lfield(3,3): A_z
+    a -= lf[5] * neltot;                       // lfield(3,2): E_z
+    const double r[9] = {d, 0.0, d, v, 0.0, v, a, 0.0, a};
+    for (int k = 0; k < 9; ++k) out[k] = r[k];
+    return 0;
   }
 
   // =========================================================================
@@ -1778,6 +1818,9 @@ void orc_etdrk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, in
     mask_orbitals(o, Y);
     if (dip) dip[s] = o->dipole(Y, C);
   }
+}
+int orc_dipole3(void* h, const double* wfn, const double* cic, const double* lfield, double* out) {
+  return static_cast<Oracle*>(h)->dipole3(reinterpret_cast<const cd*>(wfn), reinterpret_cast<const cd*>(cic), lfield, out);
 }
 // the scalar coefficients of one ETD-RK4 function (for the device path's tests):
 // out = n0, n1, n2, d0[0], d0[1], d1[0], d1[1] (complex) then dt, rk (complex)

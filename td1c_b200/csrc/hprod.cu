@@ -138,6 +138,8 @@ struct Ctx {
   int* d_status = nullptr;  // device status word (ST_* bits)
   double* d_scalar = nullptr;
   int2* dip_ent = nullptr; int dip_nent = 0; cplx* dip_partial = nullptr;  // dipole entries and chunk sums
+  double* dip_lf = nullptr;   // unit lfield(3,1) for the velocity operator
+  double* dip_out = nullptr;  // [3] traces of z, p_z and the acceleration operator
   cplx *relax_hw = nullptr, *relax_hc = nullptr;  // RHS outputs of the energy evaluation in td1c_gpu_relax
   // one-body propagators: condensed factors of 1 + c T per c, and scratch
   struct H1Slot { double cre = 0, cim = 0; H1Fac f; };
@@ -2214,10 +2216,7 @@ int td1c_gpu_htot_dev(double dtime, const double* lfield, const void* d_wfn, con
 
 // length-form dipole <z> of a device-resident state (hprod_dipole.F90, dip(1));
 // uses the context's 1-RDM buffers and its stream, synchronous
-int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out) {
-  Ctx& c = ctx();
-  if (!c.initialized || !out) return ST_CONFIG;
-  cudaStream_t st = c.st;
+static void dipole_entries(Ctx& c) {
   if (!c.dip_ent) {
     std::vector<int2> ent;
     for (int f = 0; f < c.ncore; ++f) ent.push_back(make_int2(f, f));
@@ -2228,6 +2227,13 @@ int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out) {
     c.dip_ent = dupload(ent);
     c.dip_partial = dalloc<cplx>((size_t)std::max(1, dipole_partial_size(c.Nr, c.dip_nent)));
   }
+}
+
+int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  dipole_entries(c);
   int rc = 0;
   if (c.nact > 0) {
     CiArgs ca{};
@@ -2243,6 +2249,56 @@ int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out) {
   cudaMemcpyAsync(out, c.d_scalar + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
   cudaError_t e = cudaStreamSynchronize(st);
   return (rc || e != cudaSuccess) ? ST_CUDA : 0;
+}
+
+// hprod_dipole (hprod_dipole.F90:2-146) of a state without frozen-core
+// orbitals: the length, velocity and acceleration forms as 1-RDM traces of
+// z, p_z (the one-body kernel's velocity coupling at unit field) and the
+// acceleration operator, plus A_z N (velocity gauge) and -E_z N.
+// out = dip(1:3), vel(1:3), acc(1:3); ST_CONFIG with frozen-core orbitals
+// (their generalized-Fock corrections are not built).
+int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield, double* out) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out || !lfield) return ST_CONFIG;
+  if (c.nfcore > 0) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  dipole_entries(c);
+  int rc = 0;
+  if (c.nact > 0) {
+    CiArgs ca{};
+    ca.t = c.cit; ca.cic = (const cplx*)d_cic; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
+    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, st));
+    rc |= chk("ci rdm", launch_ci_rdm(ca, st));
+  }
+  if (!c.dip_lf) {
+    const double unit[9] = {0, 0, 1, 0, 0, 0, 0, 0, 0};  // lfield(3,1) = 1: the operator at unit field
+    c.dip_lf = dupload(std::vector<double>(unit, unit + 9));
+    c.dip_out = dalloc<double>(3);
+  }
+  // p_z phi: the velocity coupling of the one-body kernel (igauge 1, unit field) into h1orb
+  OneBodyArgs ob{};
+  ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = 0; ob.mmax1 = c.mmax1; ob.igauge = 1;
+  ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
+  ob.mval = c.d_mval; ob.orb = (const cplx*)d_wfn; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = c.dip_lf;
+  rc |= chk("onebody", launch_onebody(ob, st));
+  DipoleArgs da{};
+  da.Nr = c.Nr; da.L1 = c.L1; da.mmax1 = c.mmax1; da.ncore = c.ncore; da.nact = c.nact; da.nent = c.dip_nent;
+  da.xrad = c.xrad; da.alph = c.alph; da.mval = c.d_mval; da.ent = c.dip_ent; da.wfn = (const cplx*)d_wfn;
+  da.den1 = c.den1; da.partial = c.dip_partial; da.znuc = c.znuc;
+  for (int k = 0; k < 3; ++k) {  // z, p_z, acceleration
+    da.mode = k == 0 ? 0 : (k == 1 ? 2 : 1);
+    da.pv = k == 1 ? c.h1orb : nullptr;
+    da.out = c.dip_out + k;
+    rc |= chk("dipole", launch_dipole(da, st));
+  }
+  double tr[3];
+  cudaMemcpyAsync(tr, c.dip_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc || e != cudaSuccess) return ST_CUDA;
+  const double v = tr[1] + (c.igauge == 1 ? lfield[8] * c.neltot : 0.0), a = tr[2] - lfield[5] * c.neltot;
+  const double r[9] = {tr[0], 0.0, tr[0], v, 0.0, v, a, 0.0, a};
+  for (int k = 0; k < 9; ++k) out[k] = r[k];
+  return 0;
 }
 
 // wfn_orth_cic + wfn_orth_orb on a device-resident state (in place)

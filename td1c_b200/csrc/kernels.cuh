@@ -163,6 +163,9 @@ struct DipoleArgs {
   const cplx* den1;      // [nact][nact]
   cplx* partial;         // [nchunk][nent]
   double* out;           // device scalar
+  int mode = 0;          // operator: 0 z (radial factor r), 1 acceleration (radial factor -Z / r^2), 2 pv
+  double znuc = 0;       // nuclear charge (mode 1)
+  const cplx* pv = nullptr;  // mode 2: the operator applied to the orbitals, [nfun][L1][Nr]
 };
 int launch_dipole(const DipoleArgs& a, cudaStream_t st);
 int dipole_partial_size(int Nr, int nent);

@@ -18,7 +18,10 @@ namespace td1c {
 
 constexpr int DIP_CHUNK = 64;  // radial points per CTA
 
-// partial[chunk][e] = sum over the chunk's r and all l of conj(phi_i) (z phi_j)
+// partial[chunk][e] = sum over the chunk's r and all l of conj(phi_i) (P phi_j), with P
+// z (mode 0: hprod_zprod), the acceleration operator (mode 1: hprod_azprod,
+// hprod_azprod.F90:100-135, the same l +- 1 coupling with bas_azfac = -alph Z / r^2
+// in place of r alph, bas_gen_azfac.F90:68-72) or P phi given (mode 2)
 __global__ void __launch_bounds__(256) dipole_partial_kernel(DipoleArgs a) {
   const int r0 = blockIdx.x * DIP_CHUNK;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -29,14 +32,20 @@ __global__ void __launch_bounds__(256) dipole_partial_kernel(DipoleArgs a) {
     const double* al = a.alph + (size_t)(m + a.mmax1) * a.L1;
     const cplx* pi = a.wfn + (size_t)i * a.L1 * a.Nr;
     const cplx* pj = a.wfn + (size_t)j * a.L1 * a.Nr;
+    const cplx* vj = a.pv ? a.pv + (size_t)j * a.L1 * a.Nr : nullptr;
     cplx s = mkc(0, 0);
     for (int q = lane; q < DIP_CHUNK * a.L1; q += 32) {
       const int l = q / DIP_CHUNK, r = r0 + q % DIP_CHUNK;
       if (r >= a.Nr || l < am) continue;
-      const double x = a.xrad[r + 1];
       cplx zp = mkc(0, 0);
-      if (l - 1 >= am) { const cplx w = pj[(size_t)(l - 1) * a.Nr + r]; const double t = x * al[l - 1]; zp.x = fma(w.x, t, zp.x); zp.y = fma(w.y, t, zp.y); }
-      if (l + 1 < a.L1) { const cplx w = pj[(size_t)(l + 1) * a.Nr + r]; const double t = x * al[l]; zp.x = fma(w.x, t, zp.x); zp.y = fma(w.y, t, zp.y); }
+      if (a.mode == 2) {
+        zp = vj[(size_t)l * a.Nr + r];
+      } else {
+        const double x = a.xrad[r + 1];
+        const double g = a.mode == 1 ? -a.znuc / (x * x) : x;
+        if (l - 1 >= am) { const cplx w = pj[(size_t)(l - 1) * a.Nr + r]; const double t = g * al[l - 1]; zp.x = fma(w.x, t, zp.x); zp.y = fma(w.y, t, zp.y); }
+        if (l + 1 < a.L1) { const cplx w = pj[(size_t)(l + 1) * a.Nr + r]; const double t = g * al[l]; zp.x = fma(w.x, t, zp.x); zp.y = fma(w.y, t, zp.y); }
+      }
       s = cadd(s, cmulc(pi[(size_t)l * a.Nr + r], zp));
     }
     for (int o = 16; o > 0; o >>= 1) { s.x += __shfl_xor_sync(0xffffffffu, s.x, o); s.y += __shfl_xor_sync(0xffffffffu, s.y, o); }

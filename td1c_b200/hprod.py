@@ -147,6 +147,14 @@ class HProd:
         self._check(self.lib.td1c_gpu_dipole(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(out)))
         return float(out[0])
 
+    def dipole3_dev(self, d_wfn, d_cic, lfield):
+        """hprod_dipole of a device state without frozen-core orbitals: (dip[3], vel[3], acc[3]),
+        the length, velocity and acceleration forms."""
+        out = np.zeros(9)
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        self._check(self.lib.td1c_gpu_dipole3(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(lf), _dp(out)))
+        return out[0:3], out[3:6], out[6:9]
+
     def orth_dev(self, d_wfn, d_cic):
         """wfn_orth_cic + wfn_orth_orb in place on device buffers."""
         self._check(self.lib.td1c_gpu_orth(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic)))

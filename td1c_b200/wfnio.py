@@ -1,7 +1,7 @@
 """The reference's on-disk formats for states and the energy trace.
 
 Text files, as td1c writes and reads them (src/wfn/clwfn.cpp:156-305,
-src/main/tdse.cpp:352-354):
+src/main/tdse.cpp:352-366):
 
 ``.orb``  four header lines ``%10d``: nrad, lmax1, mmax1, nfun; then one
           line ``%25.15le%25.15le`` (real, imaginary) per orbital value, in
@@ -13,6 +13,9 @@ src/main/tdse.cpp:352-354):
 ``.ene``  one line per printed step: ``%10d`` step, then time, time in
           optical cycles, E_z(t), A_z(t) and the total energy as ``%20.10e``,
           separated by single spaces.
+``.op1``  the same five leading columns, then the total dipole in the length,
+          velocity and acceleration forms (dip(3), vel(3), acc(3) of
+          hprod_dipole; tdse.cpp:365-366).
 
 Reading follows ``clwfn::read_orb`` / ``clwfn::read_cic``: an orbital file
 written on another basis is projected onto the current one (values of
@@ -102,6 +105,13 @@ def ene_line(step, time, ncyc, efield, afield, ene):
     """One line of the ``.ene`` trace (tdse.cpp:353-354): step, time (au), time in optical
     cycles, E_z(t) = lfield(3, 2), A_z(t) = lfield(3, 3), total energy."""
     return "%10d %20.10e %20.10e %20.10e %20.10e %20.10e\n" % (step, time, ncyc, efield, afield, ene)
+
+
+def op1_line(step, time, ncyc, efield, afield, dip, vel, acc):
+    """One line of the ``.op1`` trace (tdse.cpp:365-366): the ``.ene`` leading columns, then
+    the length, velocity and acceleration forms of the total dipole."""
+    return "%10d %20.10e %20.10e %20.10e %20.10e %20.10e %20.10e %20.10e\n" % (step, time, ncyc, efield, afield, dip,
+                                                                              vel, acc)
 
 
 def read_ene(path):

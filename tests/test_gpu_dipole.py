@@ -1,0 +1,69 @@
+"""The three forms of hprod_dipole on the device against the oracle.
+
+Length, velocity and acceleration forms (hprod_dipole.F90:2-146) of states
+without frozen-core orbitals, at several points of a field-driven split2
+trajectory on the device, within 1e-10 of the oracle's restatement; a
+context with frozen-core orbitals refuses the call with ST_CONFIG.
+"""
+import numpy as np
+import pytest
+
+from td1c_b200 import workloads as W
+
+from .helpers import oracle_tables, oracle_state
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.HE_SMALL, W.HE_TDHF], ids=lambda w: w["name"])
+def test_dipole_forms_match_oracle(cuda_ok, base):
+    import torch
+    from oracle.oracle import Oracle
+    from td1c_b200.hprod import HProd
+    wl = dict(base, split_type=1)
+    o = Oracle(wl)
+    o.set_split(1)
+    rad, ang = oracle_tables(o)
+    h = HProd(wl, rad, ang)
+    try:
+        orb, cic = oracle_state(o)
+        o.set_wfn0(orb, cic)
+        h.set_wfn0(orb, cic)
+        orb, cic = o.orth(orb, cic)
+        freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+        t0, dt = 0.5 * wl["numcyc"] * 2 * np.pi / freq, 0.004
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        h.rk4_reset(None, None)
+        for s in range(3):
+            t = t0 + 2 * s * dt
+            lf = o.field(t)
+            g = h.dipole3_dev(d_orb.data_ptr(), d_cic.data_ptr(), lf)
+            ref = o.dipole3(d_orb.cpu().numpy().reshape(orb.shape), d_cic.cpu().numpy(), lf)
+            for gv, rv in zip(g, ref):
+                scale = max(1e-3, np.abs(rv).max())
+                assert np.abs(gv - rv).max() < 1e-10 * scale, (s, g, ref)
+            assert g[1][2] != 0.0 and g[2][2] != 0.0
+            h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), t, dt, 2)
+            h.sync()
+    finally:
+        h.final()
+
+
+@pytest.mark.gpu
+def test_dipole_forms_refused_with_frozen_core(cuda_ok):
+    import torch
+    from oracle.oracle import Oracle
+    from td1c_b200.hprod import HProd, StatusError
+    wl = dict(W.MIXED_SMALL, split_type=1)
+    o = Oracle(wl)
+    rad, ang = oracle_tables(o)
+    h = HProd(wl, rad, ang)
+    try:
+        orb, cic = oracle_state(o)
+        h.set_wfn0(orb, cic)
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        with pytest.raises(StatusError):
+            h.dipole3_dev(d_orb.data_ptr(), d_cic.data_ptr(), np.zeros(9))
+    finally:
+        h.final()

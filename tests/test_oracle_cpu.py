@@ -297,3 +297,33 @@ def test_etdrk4_functions_and_order():
     ref = o.split2(orb, cic, t0, T / 400, 400)[0]
     err = [np.linalg.norm(o.etdrk4(orb, cic, t0, T / n, n)[0] - ref) / np.linalg.norm(ref) for n in (4, 8)]
     assert err[1] < 1e-6 and err[0] / err[1] > 10, err
+
+
+def test_dipole_forms_ehrenfest():
+    """hprod_dipole without a frozen core (He, velocity gauge, mask outside the grid): along a short
+    split2 trajectory, d<z>/dt equals the velocity form and d<v>/dt the acceleration form (central
+    differences), which fixes the operators, their signs and the field terms; a state with a
+    frozen core is refused (its generalized-Fock corrections are not restated)."""
+    from oracle.oracle import Oracle
+    from .helpers import oracle_state
+    wl = dict(W.HE_SMALL, split_type=1, rmask=1e9)
+    o = Oracle(wl)
+    o.set_split(1)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    orb, cic = o.orth(orb, cic)
+    freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+    t0, dt = 0.5 * wl["numcyc"] * 2 * np.pi / freq, 2e-3
+    vals, w, c = [], orb, cic
+    for s in range(5):
+        vals.append(o.dipole3(w, c, o.field(t0 + s * dt)))
+        w, c, _ = o.split2(w, c, t0 + s * dt, dt, 1)
+    d = np.array([v[0][2] for v in vals])
+    v = np.array([v[1][2] for v in vals])
+    a = np.array([v[2][2] for v in vals])
+    for s in (1, 2, 3):
+        assert abs((d[s + 1] - d[s - 1]) / (2 * dt) - v[s]) < 1e-4 * abs(v[s]), (s, d, v)
+        assert abs((v[s + 1] - v[s - 1]) / (2 * dt) - a[s]) < 1e-2 * abs(a[s]), (s, v, a)
+    o2 = Oracle(dict(W.MIXED_SMALL, split_type=1))
+    orb2, cic2 = oracle_state(o2)
+    assert o2.dipole3(orb2, cic2, np.zeros(9)) is None

@@ -89,3 +89,10 @@ def test_ene_line(tmp_path):
     p.write_text(ln + wfnio.ene_line(1201, 4.804, 0.0871, -0.012, 0.2001, -128.5471))
     t = wfnio.read_ene(p)
     assert list(t["step"]) == [1200, 1201] and np.allclose(t["ene"], [-128.54712, -128.5471])
+
+
+def test_op1_line():
+    ln = wfnio.op1_line(7, 0.028, 0.0005, 1e-3, -2e-2, 0.125, -0.5, 3.25)
+    assert ln == "         7 %20.10e %20.10e %20.10e %20.10e %20.10e %20.10e %20.10e\n" % (
+        0.028, 0.0005, 1e-3, -2e-2, 0.125, -0.5, 3.25)
+    assert len(ln) == 10 + 7 * 21 + 1
