@@ -396,14 +396,22 @@ int launch_mfprod(const MfprodArgs& a, cudaStream_t st) {
       cudaFuncSetAttribute(mfprod_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       attr = true;
     }
-    static int nsm = 0;
+    // persistent: as many CTAs as are resident at once (shared memory decides; at
+    // least 2 per SM), sized once per shared-memory footprint
+    static int nsm = 0, cps = 0;
+    static size_t cps_smem = 0;
     if (!nsm) {
       int dev = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     }
+    if (cps_smem != smem) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, mfprod_dmma_kernel, MFD_NT, smem) != cudaSuccess) cps = 2;
+      cps = std::max(cps, 2);
+      cps_smem = smem;
+    }
     const int ntile = (int)((a.ngrid + MFD_TQ - 1) / MFD_TQ);
-    mfprod_dmma_kernel<<<(unsigned)std::min(ntile, 2 * nsm), MFD_NT, smem, st>>>(a);  // persistent: 2 CTAs per SM
+    mfprod_dmma_kernel<<<(unsigned)std::min(ntile, cps * nsm), MFD_NT, smem, st>>>(a);
     return (int)cudaGetLastError();
   }
   return launch_mfprod_scalar(a, st);
