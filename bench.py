@@ -39,7 +39,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-AU2FS = 0.02418884254  # fs per atomic time unit (mod_const.F90:21)
+from td1c_b200.replicas import AU2FS, job_throughput, max_over_ranks, replica_seed  # noqa: E402
 
 
 def parse():
@@ -314,7 +314,7 @@ def main():
     h = HProd(wl, rad, ang)
     d = h.dims
     tb = h.ci_tables()
-    orb = seeded_orbitals(wl, rad["xrad"], rad["wrad"], rad["mask"], seed=wl.get("seed", 0) + rank)
+    orb = seeded_orbitals(wl, rad["xrad"], rad["wrad"], rad["mask"], seed=replica_seed(wl.get("seed", 0), rank))
     cic = seeded_cic(wl, d["lcic"], tb["stra"], tb["strb"], tb["detoff"], tb["afirst"], tb["acount"])
     h.set_wfn0(orb, cic)
     dev = torch.device("cuda", local)
@@ -370,14 +370,11 @@ def main():
         torch.cuda.synchronize()
     launches = h.launch_count()
     h.sync()
-    sec = e0.elapsed_time(e1) / 1e3
+    sec = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist if world > 1 else None, dev)
     if world > 1:
-        t = torch.tensor([sec], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = float(t.item())
         dist.barrier()
     torch.cuda.synchronize()
-    value = world * args.steps * dt * AU2FS / sec
+    value = job_throughput(world, args.steps, dt, sec)
     wn = d_orb.cpu().numpy().reshape(len(wl["orbitals"]), -1)
     traj = {"t_start_au": t1, "t_end_au": t1 + args.steps * dt,
             "orbital_norm_dev": float(np.abs(np.linalg.norm(wn, axis=1) - 1.0).max()),
@@ -415,12 +412,8 @@ def main():
     e3.record(ext)
     torch.cuda.synchronize()
     wall = time.perf_counter() - w0
-    sec_e = max(e2.elapsed_time(e3) / 1e3, wall)
-    if world > 1:
-        t = torch.tensor([sec_e], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec_e = float(t.item())
-    e2e = world * ke * dt * AU2FS / sec_e
+    sec_e = max_over_ranks(max(e2.elapsed_time(e3) / 1e3, wall), dist if world > 1 else None, dev)
+    e2e = job_throughput(world, ke, dt, sec_e)
     bytes_step = (h_orb.numel() + h_cic.numel()) * 16
 
     # ---- one-body half step alone (split2's clh1itr) at the |A| peak field
