@@ -138,6 +138,12 @@ int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out);
  * ST_CONFIG with frozen-core orbitals: their generalized-Fock corrections
  * (hprod_gfock, hprod_projfc) are not built. */
 int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
+/* Drop-in for hprod_dipole_ (include/wrapper.hpp:114, called by
+ * clhprod::dipole, src/hprod/clhprod.cpp:218-222): host lfield(3,3), wfn,
+ * cic; writes dip[3], vel[3], acc[3].  With frozen-core orbitals only the
+ * length form is computed (vel, acc are NaN and the status word gets
+ * ST_CONFIG, see td1c_gpu_dipole3). */
+void hprod_dipole_(const double* lfield, const double* wfn, const double* cic, double* dip, double* vel, double* acc);
 
 /* wfn_orth_cic + wfn_orth_orb (src/wfn/wfn_orth.F90:2-110): normalise the CI
  * vector and Gram-Schmidt the non-frozen orbitals against all earlier

@@ -82,6 +82,8 @@ def load():
     lib.td1c_gpu_dipole.argtypes = [vp, vp, dp]
     lib.td1c_gpu_dipole3.restype = c_int
     lib.td1c_gpu_dipole3.argtypes = [vp, vp, dp, dp]
+    lib.hprod_dipole_.restype = None
+    lib.hprod_dipole_.argtypes = [dp, dp, dp, dp, dp, dp]
     lib.td1c_gpu_int2e_static.restype = c_int
     lib.td1c_gpu_int2e_static.argtypes = [c_int, ip, c_long, vp, vp, vp, vp]
     lib.td1c_gpu_bind_split.restype = c_int
@@ -110,7 +112,7 @@ EXPORTED = [
     "td1c_gpu_last_status", "td1c_gpu_dims", "td1c_gpu_ci_tables", "td1c_gpu_energies",
     "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
     "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset", "td1c_gpu_int2e_static", "td1c_gpu_dipole",
-    "td1c_gpu_dipole3",
+    "td1c_gpu_dipole3", "hprod_dipole_",
     "td1c_gpu_orth", "td1c_gpu_relax", "td1c_gpu_bind_split", "td1c_gpu_h1itr", "td1c_gpu_dpade",
     "td1c_gpu_split2", "td1c_gpu_etdrk2", "td1c_gpu_etdrk4", "td1c_gpu_relax_etdrk2",
     "h1itr_gen_cninv_", "h1itr_prop_", "dpade_gen_", "dpade_prod_",

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -2299,6 +2300,33 @@ int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield,
   const double r[9] = {tr[0], 0.0, tr[0], v, 0.0, v, a, 0.0, a};
   for (int k = 0; k < 9; ++k) out[k] = r[k];
   return 0;
+}
+
+// hprod_dipole_ (include/wrapper.hpp:114; clhprod::dipole, clhprod.cpp:218-222)
+// with host buffers: the state is copied in and dip, vel, acc (3 each) are
+// written back.  Without frozen-core orbitals all three forms; with them the
+// length form (which needs no correction) and NaN for the velocity and
+// acceleration forms, with ST_CONFIG in the status word.
+void hprod_dipole_(const double* lfield, const double* wfn, const double* cic, double* dip, double* vel, double* acc) {
+  Ctx& c = ctx();
+  if (!c.initialized) { c.status |= ST_CONFIG; return; }
+  cudaStream_t st = c.st;
+  cudaMemcpyAsync(c.wfn_io, wfn, c.nbas * c.nfun * sizeof(cplx), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c.cic_io, cic, c.lcic * sizeof(cplx), cudaMemcpyHostToDevice, st);
+  double out[9];
+  int rc;
+  if (c.nfcore == 0) {
+    rc = td1c_gpu_dipole3(c.wfn_io, c.cic_io, lfield, out);
+  } else {
+    double d = 0.0;
+    rc = td1c_gpu_dipole(c.wfn_io, c.cic_io, &d);
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    const double r[9] = {d, 0.0, d, nan, nan, nan, nan, nan, nan};
+    for (int k = 0; k < 9; ++k) out[k] = r[k];
+    c.status |= ST_CONFIG;
+  }
+  c.status |= rc;
+  for (int k = 0; k < 3; ++k) { dip[k] = out[k]; vel[k] = out[3 + k]; acc[k] = out[6 + k]; }
 }
 
 // wfn_orth_cic + wfn_orth_orb on a device-resident state (in place)

@@ -3,7 +3,9 @@
 Length, velocity and acceleration forms (hprod_dipole.F90:2-146) of states
 without frozen-core orbitals, at several points of a field-driven split2
 trajectory on the device, within 1e-10 of the oracle's restatement; a
-context with frozen-core orbitals refuses the call with ST_CONFIG.
+context with frozen-core orbitals refuses the call with ST_CONFIG.  The
+drop-in hprod_dipole_ (host buffers) gives the same numbers, and with a
+frozen core the length form only.
 """
 import numpy as np
 import pytest
@@ -65,5 +67,57 @@ def test_dipole_forms_refused_with_frozen_core(cuda_ok):
         d_cic = torch.from_numpy(cic.copy()).cuda()
         with pytest.raises(StatusError):
             h.dipole3_dev(d_orb.data_ptr(), d_cic.data_ptr(), np.zeros(9))
+    finally:
+        h.final()
+
+
+def _host_dipole(h, orb, cic, lf):
+    import ctypes
+    dp = ctypes.POINTER(ctypes.c_double)
+    o = np.ascontiguousarray(orb, dtype=np.complex128).reshape(-1)
+    c = np.ascontiguousarray(cic, dtype=np.complex128)
+    lf = np.ascontiguousarray(lf, dtype=np.float64)
+    dip, vel, acc = np.zeros(3), np.zeros(3), np.zeros(3)
+    h.lib.hprod_dipole_(*(a.ctypes.data_as(dp) for a in (lf, o.view(np.float64), c.view(np.float64), dip, vel, acc)))
+    return dip, vel, acc
+
+
+@pytest.mark.gpu
+def test_hprod_dipole_dropin(cuda_ok):
+    import torch
+    from oracle.oracle import Oracle
+    from td1c_b200.hprod import HProd
+    # without frozen core: all three forms, as td1c_gpu_dipole3 and the oracle
+    wl = dict(W.HE_SMALL, split_type=1)
+    o = Oracle(wl)
+    rad, ang = oracle_tables(o)
+    h = HProd(wl, rad, ang)
+    try:
+        orb, cic = oracle_state(o)
+        o.set_wfn0(orb, cic)
+        h.set_wfn0(orb, cic)
+        lf = o.field(30.0)
+        got = _host_dipole(h, orb, cic, lf)
+        ref = o.dipole3(orb, cic, lf)
+        for gv, rv in zip(got, ref):
+            assert np.abs(gv - rv).max() < 1e-10 * max(1e-3, np.abs(rv).max()), (got, ref)
+        assert h.lib.td1c_gpu_last_status() == 0
+    finally:
+        h.final()
+    # with a frozen core: the length form only, the status word flags the rest
+    wl = dict(W.MIXED_SMALL, split_type=1)
+    o = Oracle(wl)
+    rad, ang = oracle_tables(o)
+    h = HProd(wl, rad, ang)
+    try:
+        orb, cic = oracle_state(o)
+        h.set_wfn0(orb, cic)
+        dip, vel, acc = _host_dipole(h, orb, cic, o.field(30.0))
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        d_len = h.dipole_dev(d_orb.data_ptr(), d_cic.data_ptr())
+        assert dip[0] == dip[2] and dip[1] == 0.0 and abs(dip[0] - d_len) <= 1e-12 * max(1.0, abs(d_len))
+        assert np.all(np.isnan(vel)) and np.all(np.isnan(acc))
+        assert h.lib.td1c_gpu_last_status() & 16
     finally:
         h.final()
