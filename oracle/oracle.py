@@ -223,7 +223,8 @@ class Oracle:
         return self._prop("orc_etdrk4", wfn, cic, t0, dt, nstep, maxcyc, thresh)
 
     def dipole3(self, wfn, cic, lfield):
-        """hprod_dipole without frozen-core orbitals: (dip[3], vel[3], acc[3]); None with a frozen core."""
+        """hprod_dipole: (dip[3], vel[3], acc[3]); with frozen-core orbitals vel[1], acc[1] are the
+        generalized-Fock corrections and vel[2], acc[2] the totals."""
         wfn = np.ascontiguousarray(wfn, dtype=np.complex128)
         cic = np.ascontiguousarray(cic, dtype=np.complex128)
         out = np.zeros(9)

@@ -781,15 +781,20 @@ struct Oracle {
     }
   }
 
-  // hprod_mfprod2.F90:2-34 with its callees (dofc = false)
-  void mfprod2() {
+  // hprod_mfprod2.F90:2-34 (dofc = false) and hprod_mfprod2_gfock (59-84, dofc = true) with
+  // their callees.  With dofc the frozen-core rows f < nfcore also receive the exchange with the
+  // frozen cores (fcx1), the dynamic-core Coulomb and exchange (dcj, dcx) and the active-space
+  // Coulomb and exchange (actj, actx): the `_onFC` parts of each callee, the same formula on
+  // rows 0 .. nfcore - 1 (nradfc = nrad - 1).
+  void mfprod2(bool dofc) {
     const size_t NG = ngrid;
+    const int r0 = dofc ? 0 : nfcore;  // first row that receives the mean field
     auto OG = [&](int f) { return &orbg[(size_t)f * NG]; };
     auto GG = [&](int f) { return &gorbg[(size_t)f * NG]; };
     auto VG = [&](int f) { return &v2orbg[(size_t)f * NG]; };
     auto W = [&](int j, int i) { return &v2ang[ian(0, 0, j, i)]; };
     // fcx1 (hprod_mfprod2.F90:158-200): nfcore2 = 0, all frozen cores are fc1
-    for (int i = nfcore; i < nfun; ++i)
+    for (int i = r0; i < nfun; ++i)
       for (int j = 0; j < nfcore; ++j) {
         cd* g = GG(i); const cd* v = W(j, i); const cd* o = OG(j);
 #pragma omp parallel for
@@ -799,9 +804,9 @@ struct Oracle {
       // dcj (242-306)
       std::vector<cd> d2v(NG, 0.0);
       for (int j = nfcore; j < ncore; ++j) { const cd* v = W(j, j); for (size_t q = 0; q < NG; ++q) d2v[q] += v[q] * 2.0; }
-      for (int i = nfcore; i < nfun; ++i) { cd* g = GG(i); const cd* o = OG(i); for (size_t q = 0; q < NG; ++q) g[q] += d2v[q] * o[q]; }
+      for (int i = r0; i < nfun; ++i) { cd* g = GG(i); const cd* o = OG(i); for (size_t q = 0; q < NG; ++q) g[q] += d2v[q] * o[q]; }
       // dcx (308-366)
-      for (int i = nfcore; i < nfun; ++i)
+      for (int i = r0; i < nfun; ++i)
         for (int j = nfcore; j < ncore; ++j) {
           cd* g = GG(i); const cd* v = W(j, i); const cd* o = OG(j);
           for (size_t q = 0; q < NG; ++q) g[q] -= v[q] * o[q];
@@ -815,7 +820,7 @@ struct Oracle {
           cd dens = D1(den1, ka, ja); const cd* v = W(ncore + ja, ncore + ka);
           for (size_t q = 0; q < NG; ++q) d2v[q] += v[q] * dens;
         }
-      for (int i = nfcore; i < ncore; ++i) { cd* g = VG(i); const cd* o = OG(i); for (size_t q = 0; q < NG; ++q) g[q] += d2v[q] * o[q]; }
+      for (int i = r0; i < ncore; ++i) { cd* g = VG(i); const cd* o = OG(i); for (size_t q = 0; q < NG; ++q) g[q] += d2v[q] * o[q]; }
       // actx (439-514)
       std::vector<cd> wd1(NG);
       for (int ja = 0; ja < nact; ++ja) {
@@ -827,7 +832,7 @@ struct Oracle {
           cd dens = -D1(den1, ka, ja) * 0.5; const cd* o = OG(kf);
           for (size_t q = 0; q < NG; ++q) wd1[q] += o[q] * dens;
         }
-        for (int i = nfcore; i < ncore; ++i) { cd* g = VG(i); const cd* v = W(jf, i); for (size_t q = 0; q < NG; ++q) g[q] += wd1[q] * v[q]; }
+        for (int i = r0; i < ncore; ++i) { cd* g = VG(i); const cd* v = W(jf, i); for (size_t q = 0; q < NG; ++q) g[q] += wd1[q] * v[q]; }
       }
     }
     // act2 (619-694): the 2-RDM contraction
@@ -1009,9 +1014,8 @@ struct Oracle {
   // =========================================================================
   // hprod_htot / hprod_htotx (hprod_htot.F90:2-208)
   // =========================================================================
-  void htot(double dtime, const double* lfield, const cd* wfn, const cd* cic, cd* hwfn, cd* hcic) {
-    const cd zfield = lfield[2], efield = lfield[5];
-    // hprod_htot_init (hprod_htot_init.F90:2-130)
+  // hprod_htot_init (hprod_htot_init.F90:2-130): clear the scratch of one RHS
+  void htot_init() {
     for (auto* v : {&orb, &h0orb, &h1orb, &gorb, &v2orb}) std::fill(v->begin(), v->end(), cd(0.0));
     for (auto* v : {&orbg, &gorbg, &v2orbg, &torbg}) std::fill(v->begin(), v->end(), cd(0.0));
     for (auto* v : {&den1, &den2, &rden, &rrden, &int1e, &int2e, &xmat, &fmat, &bmat}) std::fill(v->begin(), v->end(), cd(0.0));
@@ -1023,6 +1027,21 @@ struct Oracle {
             rho2[isp(ir, l, j, i)] = 0.0; rho2[isp(ir, l, i, j)] = 0.0;
             v2sph[isp(ir, l, j, i)] = 0.0; v2sph[isp(ir, l, i, j)] = 0.0;
           }
+  }
+  // the pair potentials of the dynamic orbitals (hprod_mkrho2_dyn, hprod_mkv2mf_dyn) and their
+  // action (hprod_mfprod2 / hprod_mfprod2_gfock), back on the spherical basis
+  void meanfield(bool dofc) {
+    mkrho2("dyn"); mkrho2("fc1dyn");
+    poisson("dyn"); sph2ang2_herm("dyn");
+    poisson("fc1dyn"); sph2ang2_herm("fc1dyn");
+    mfprod2(dofc);
+#pragma omp parallel for
+    for (int f = dofc ? 0 : nfcore; f < nfun; ++f) { ang2sph1(gorbg, gorb, f); ang2sph1(v2orbg, v2orb, f); }
+  }
+
+  void htot(double dtime, const double* lfield, const cd* wfn, const cd* cic, cd* hwfn, cd* hcic) {
+    const cd zfield = lfield[2], efield = lfield[5];
+    htot_init();
     orbin(lfield, wfn);
     // RDMs
     mkden1(cic);
@@ -1036,14 +1055,7 @@ struct Oracle {
     else { pzprod(zfield, orb, h1orb, nfcore, nfun); pzprod(zfield, orb, h1orb, 0, nfcore); }
     if (nfcore > 0 && cfg.igauge == 1) zprod(efield, orb, h1orb, 0, nfcore);
     // mean field
-    if (neltot >= 2) {
-      mkrho2("dyn"); mkrho2("fc1dyn");
-      poisson("dyn"); sph2ang2_herm("dyn");
-      poisson("fc1dyn"); sph2ang2_herm("fc1dyn");
-      mfprod2();
-#pragma omp parallel for
-      for (int f = nfcore; f < nfun; ++f) { ang2sph1(gorbg, gorb, f); ang2sph1(v2orbg, v2orb, f); }
-    }
+    if (neltot >= 2) meanfield(false);
     // integrals: hprod_mkint1_sph.F90:2-103, hprod_mkint2_sph.F90:2-100
     for (int ia = 0; ia < nact; ++ia)
       for (int ja = 0; ja <= ia; ++ja) {
@@ -1313,22 +1325,77 @@ struct Oracle {
       }
     }
   }
-  // hprod_dipole (hprod_dipole.F90:2-146) for a state without frozen-core
-  // orbitals (no generalized-Fock corrections, no pseudopotential): the
-  // length, velocity and acceleration forms by the Ehrenfest traces,
-  // out = dip(1:3), vel(1:3), acc(1:3).  Returns -1 with a frozen core.
-  int dipole3(const cd* wfn, const cd* cic, const double* lf, double* out) {
-    if (nfcore > 0) return -1;
-    const size_t n = (size_t)nbas * nfun;
-    std::vector<cd> w(wfn, wfn + n), zo(n, 0.0), po(n, 0.0), ao(n, 0.0);
+  // hprod_gfock (hprod_gfock.F90:2-109; dft_type = 0, no pseudopotential, exact3j = false,
+  // ecs_flag = 0) and hprod_gfock_sum (hprod_gfock.F90:198-230): the generalized-Fock vectors
+  // gorb_p = (h0 + h1 + g + v2) phi_p of every orbital, the frozen cores included.  h0 is the
+  // kinetic + nuclear band with the frozen-core Coulomb folded in (jfc_implicit), h1 the laser
+  // coupling at lfield(3, 1); the frozen-core pair potentials are the ones set_wfn0 made.
+  void gfock(const double* lfield, const cd* wfn, const cd* cic) {
+    htot_init();
     mkden1(cic);
+    mkden2(cic);
+    invden();
+    orbin(lfield, wfn);
+    const cd zfield = lfield[2];
+    tprod(orb, h0orb, 0, nfun);
+    if (cfg.igauge == 0) zprod(zfield, orb, h1orb, 0, nfun);
+    else pzprod(zfield, orb, h1orb, 0, nfun);
+    if (neltot >= 2) meanfield(true);
+    for (size_t k = 0; k < (size_t)nbas * nfun; ++k) gorb[k] = v2orb[k] + gorb[k] + h1orb[k] + h0orb[k];
+  }
+  // hprod_projfc(inner = .true.) (hprod_projfc.F90:2-40, 42-76, 78-122): h <- P_fc h, the
+  // projection of every orbital's vector onto the frozen cores of equal m,
+  // h_i = sum_{j < nfcore, m_j = m_i} w_j <w_j | h_i>.
+  void projfc(const std::vector<cd>& w, std::vector<cd>& h) {
+    std::vector<cd> f((size_t)nfcore * nfun, 0.0);  // f[j + nfcore i] = <w_j | h_i>
+    for (int j = 0; j < nfcore; ++j)
+      for (int i = 0; i < nfun; ++i)
+        if (mval[i] == mval[j]) f[j + (size_t)nfcore * i] = dot_orb(w, j, h, i);
+    std::fill(h.begin(), h.end(), cd(0.0));
+    for (int i = 0; i < nfun; ++i)
+      for (int j = 0; j < nfcore; ++j) {
+        if (mval[i] != mval[j]) continue;
+        const cd x = f[j + (size_t)nfcore * i];
+        const size_t oi = (size_t)i * nbas, oj = (size_t)j * nbas;
+        for (int k = 0; k < nbas; ++k) h[oi + k] += w[oj + k] * x;
+      }
+  }
+  // hprod_dipole (hprod_dipole.F90:2-146; no pseudopotential, do_op1tr off): the length,
+  // velocity and acceleration forms by the Ehrenfest traces over the 1-RDM,
+  // out = dip(1:3), vel(1:3), acc(1:3).  With frozen-core orbitals the time derivative of the
+  // frozen cores' share is carried by the generalized-Fock corrections:
+  //   vcorr1 = -4 Im sum_{f < nfcore} <z phi_f | g_f>,  acorr1 the same with p_z phi_f,
+  //   vcorr2 = -2 Im trace1(z phi, P_fc g),            acorr2 the same with p_z phi,
+  // with g the generalized-Fock vectors (in the velocity gauge g += E_z z phi first), and
+  // vel(2) = vcorr1 + vcorr2, acc(2) = acorr1 + acorr2.
+  int dipole3(const cd* wfn, const cd* cic, const double* lf, double* out) {
+    const size_t n = (size_t)nbas * nfun;
+    std::vector<cd> w, zo(n, 0.0), po(n, 0.0), ao(n, 0.0);
+    if (nfcore > 0) {
+      gfock(lf, wfn, cic);
+      w = orb;  // the frozen cores as hprod_orbin set them (gauge phase included)
+    } else {
+      mkden1(cic);
+      w.assign(wfn, wfn + n);
+    }
     zprod(1.0, w, zo, 0, nfun);
     pzprod(1.0, w, po, 0, nfun);
     azprod(1.0, w, ao, 0, nfun);
     double d = trace1(w, zo).real(), v = trace1(w, po).real(), a = trace1(w, ao).real();
     if (cfg.igauge == 1) v += lf[8] * neltot;  // lfield(3,3): A_z
     a -= lf[5] * neltot;                       // lfield(3,2): E_z
-    const double r[9] = {d, 0.0, d, v, 0.0, v, a, 0.0, a};
+    double vc = 0.0, ac = 0.0;
+    if (nfcore > 0) {
+      std::vector<cd> g(gorb);
+      if (cfg.igauge == 1)
+        for (size_t k = 0; k < n; ++k) g[k] += lf[5] * zo[k];
+      cd v1 = 0.0, a1 = 0.0;
+      for (int f = 0; f < nfcore; ++f) { v1 += dot_orb(zo, f, g, f); a1 += dot_orb(po, f, g, f); }
+      projfc(w, g);
+      vc = -4.0 * v1.imag() - 2.0 * trace1(zo, g).imag();
+      ac = -4.0 * a1.imag() - 2.0 * trace1(po, g).imag();
+    }
+    const double r[9] = {d, 0.0, d, v, vc, v + vc, a, ac, a + ac};
     for (int k = 0; k < 9; ++k) out[k] = r[k];
     return 0;
   }

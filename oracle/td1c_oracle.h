@@ -105,8 +105,9 @@ void  orc_etdrk2(void* h, const orc_pulse* p, double t0, double dt, int nstep, i
 void  orc_etdrk4(void* h, const orc_pulse* p, double t0, double dt, int nstep, int maxcyc, double thresh,
                  double* wfn, double* cic, double* dip);
 void  orc_etd4_fun(int which, double dt, int icomp, double* out);
-/* hprod_dipole without frozen-core orbitals: out = dip(1:3), vel(1:3),
- * acc(1:3) (length, velocity, acceleration forms); -1 with a frozen core. */
+/* hprod_dipole: out = dip(1:3), vel(1:3), acc(1:3) (length, velocity,
+ * acceleration forms); with frozen-core orbitals vel(2), acc(2) carry the
+ * generalized-Fock corrections (hprod_gfock, hprod_projfc). Returns 0.     */
 int   orc_dipole3(void* h, const double* wfn, const double* cic, const double* lfield, double* out);
 /* init_prop12 with cletdrk2: per cycle ene[s], one zero-field ETD-RK2 step
  * (no mask), orc_orth (needs icomp = 0).                                     */

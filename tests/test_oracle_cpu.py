@@ -302,8 +302,7 @@ def test_etdrk4_functions_and_order():
 def test_dipole_forms_ehrenfest():
     """hprod_dipole without a frozen core (He, velocity gauge, mask outside the grid): along a short
     split2 trajectory, d<z>/dt equals the velocity form and d<v>/dt the acceleration form (central
-    differences), which fixes the operators, their signs and the field terms; a state with a
-    frozen core is refused (its generalized-Fock corrections are not restated)."""
+    differences), which fixes the operators, their signs and the field terms."""
     from oracle.oracle import Oracle
     from .helpers import oracle_state
     wl = dict(W.HE_SMALL, split_type=1, rmask=1e9)
@@ -324,6 +323,43 @@ def test_dipole_forms_ehrenfest():
     for s in (1, 2, 3):
         assert abs((d[s + 1] - d[s - 1]) / (2 * dt) - v[s]) < 1e-4 * abs(v[s]), (s, d, v)
         assert abs((v[s + 1] - v[s - 1]) / (2 * dt) - a[s]) < 1e-2 * abs(a[s]), (s, v, a)
-    o2 = Oracle(dict(W.MIXED_SMALL, split_type=1))
-    orb2, cic2 = oracle_state(o2)
-    assert o2.dipole3(orb2, cic2, np.zeros(9)) is None
+
+
+def _ehrenfest_trace(wl, nstep=3, dt=2e-3):
+    """dipole3 at nstep points of a split2 trajectory from the middle of the pulse."""
+    from oracle.oracle import Oracle
+    from .helpers import oracle_state
+    o = Oracle(wl)
+    o.set_split(1)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    orb, cic = o.orth(orb, cic)
+    freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+    t0 = 0.5 * wl["numcyc"] * 2 * np.pi / freq
+    vals, w, c = [], orb, cic
+    for s in range(nstep):
+        vals.append(o.dipole3(w, c, o.field(t0 + s * dt)))
+        w, c, _ = o.split2(w, c, t0 + s * dt, dt, 1)
+    return [np.array([v[k] for v in vals]) for k in range(3)]  # dip, vel, acc: [step][3]
+
+
+@pytest.mark.parametrize("gauge", ["length", "velocity"])
+def test_dipole_forms_frozen_core(gauge):
+    """hprod_dipole with a frozen core (hprod_gfock, hprod_projfc; C with a frozen 1s, a dynamic
+    2s and a 2s2p active space; elements of 0.875 bohr, mask outside the grid).  Along a split2
+    trajectory the corrected velocity form vel(3) is d<z>/dt while the plain trace vel(1) is far
+    from it; the corrected acceleration form acc(3) is d/dt of the plain momentum trace vel(1)
+    (the same identity with p_z in place of z) while acc(1) alone is not.  The acceleration
+    identity is checked in the length gauge: the seeded state's grid-frequency components make
+    the velocity-gauge momentum vary faster than a 2e-3 difference resolves."""
+    base = W.LENGTH_SMALL if gauge == "length" else W.MIXED_SMALL
+    dt = 2e-3
+    dip, vel, acc = _ehrenfest_trace(dict(base, split_type=1, rmask=1e9, nfe=16), dt=dt)
+    dd = (dip[2, 2] - dip[0, 2]) / (2 * dt)
+    assert abs(dd - vel[1, 2]) < 2e-4 * abs(vel[1, 2]), (dd, vel[1])
+    assert abs(dd - vel[1, 0]) > 0.2 * abs(vel[1, 2])  # the corrections are needed
+    assert dip[1, 1] == 0.0 and vel[1, 2] == vel[1, 0] + vel[1, 1] and acc[1, 2] == acc[1, 0] + acc[1, 1]
+    if gauge == "length":
+        dv1 = (vel[2, 0] - vel[0, 0]) / (2 * dt)
+        assert abs(dv1 - acc[1, 2]) < 3e-2 * abs(acc[1, 2]), (dv1, acc[1])
+        assert abs(dv1 - acc[1, 0]) > 0.1 * abs(acc[1, 2])
