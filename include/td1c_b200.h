@@ -130,19 +130,21 @@ long td1c_gpu_debug_get(const char* name, double* out, long capacity);
  * applied as the unit-field length-gauge coupling.  Uses the library stream
  * and its 1-RDM buffers; returns when the value is on the host. */
 int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out);
-/* hprod_dipole (src/hprod/hprod_dipole.F90:2-146) of a device state without
- * frozen-core orbitals: out[9] = dip(1:3), vel(1:3), acc(1:3) (length,
- * velocity and acceleration forms by the Ehrenfest traces hprod_trace1 of z,
- * p_z and the nuclear acceleration operator, plus A_z N in the velocity
- * gauge and -E_z N; the second components are 0).  lfield: host lfield(3,3).
- * ST_CONFIG with frozen-core orbitals: their generalized-Fock corrections
- * (hprod_gfock, hprod_projfc) are not built. */
+/* hprod_dipole (src/hprod/hprod_dipole.F90:2-146) of a device state:
+ * out[9] = dip(1:3), vel(1:3), acc(1:3) (length, velocity and acceleration
+ * forms by the Ehrenfest traces hprod_trace1 of z, p_z and the nuclear
+ * acceleration operator, plus A_z N in the velocity gauge and -E_z N).
+ * Without frozen-core orbitals the second components are 0; with them
+ * vel(2), acc(2) are the generalized-Fock corrections (hprod_gfock,
+ * src/hprod/hprod_gfock.F90:2-230; hprod_projfc, src/hprod/hprod_projfc.F90)
+ * and the call also runs the RHS passes (the library's RHS scratch is
+ * overwritten).  lfield: host lfield(3,3). */
 int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
 /* Drop-in for hprod_dipole_ (include/wrapper.hpp:114, called by
  * clhprod::dipole, src/hprod/clhprod.cpp:218-222): host lfield(3,3), wfn,
- * cic; writes dip[3], vel[3], acc[3].  With frozen-core orbitals only the
- * length form is computed (vel, acc are NaN and the status word gets
- * ST_CONFIG, see td1c_gpu_dipole3). */
+ * cic; writes dip[3], vel[3], acc[3] (td1c_gpu_dipole3 on the library's
+ * staging buffers; on an error all nine are NaN and the status word holds
+ * the error). */
 void hprod_dipole_(const double* lfield, const double* wfn, const double* cic, double* dip, double* vel, double* acc);
 
 /* wfn_orth_cic + wfn_orth_orb (src/wfn/wfn_orth.F90:2-110): normalise the CI

@@ -141,6 +141,13 @@ struct Ctx {
   int2* dip_ent = nullptr; int dip_nent = 0; cplx* dip_partial = nullptr;  // dipole entries and chunk sums
   double* dip_lf = nullptr;   // unit lfield(3,1) for the velocity operator
   double* dip_out = nullptr;  // [3] traces of z, p_z and the acceleration operator
+  // frozen-core dipole: z phi, p_z phi, the generalized-Fock vectors, the caller's field, and the
+  // overlaps of the generalized-Fock corrections (entries and their host-side index maps)
+  cplx *dip_z = nullptr, *dip_p = nullptr, *dip_g = nullptr, *dip_rd = nullptr;
+  double* dip_lfd = nullptr;
+  int4* dip_rd_ent = nullptr;
+  int dip_rd_n = 0;
+  std::vector<int> dip_ia, dip_ib, dip_if, dip_isz, dip_isp;
   cplx *relax_hw = nullptr, *relax_hc = nullptr;  // RHS outputs of the energy evaluation in td1c_gpu_relax
   // one-body propagators: condensed factors of 1 + c T per c, and scratch
   struct H1Slot { double cre = 0, cim = 0; H1Fac f; };
@@ -278,6 +285,86 @@ __global__ void fc_g_kernel(int Nr, int nlat, int nfcore, int nfun, const cplx* 
     v = csub(v, cmul(w, orbg[(size_t)j * ng + q]));
   }
   gorbg[(size_t)i * ng + q] = v;
+}
+
+// the mean field on the frozen-core rows of the generalized-Fock vectors
+// (hprod_mfprod2_gfock, hprod_mfprod2.F90:59-84: the dofc parts of fcx1
+// 158-200, dcj 242-306, dcx 308-366, actj 368-437 and actx 439-514; the
+// frozen-core Coulomb is in the kinetic diagonal).  For frozen core i at grid
+// point q, g + v2 =
+//   - sum_{j < nfcore} W(j,i) phi_j + sum_{j dynamic core} (2 W(j,j) phi_i - W(j,i) phi_j)
+//   + sum_{ja,ka} den1(ka,ja) W(ja,ka) phi_i - 1/2 sum_{ja} sum_{ka, m equal} den1(ka,ja) phi_ka W(ja,i)
+// written to gorbg[i]; W(j,i) is pair_of/pair_cj's pair potential (conjugated
+// for the swapped pair).
+__global__ void fc_gfock_kernel(int Nr, int nlat, int nfcore, int ncore, int nact, int nfun, const int* __restrict__ mval,
+                                const cplx* __restrict__ orbg, const cplx* __restrict__ W, const int* __restrict__ pair_of,
+                                const int* __restrict__ pair_cj, const cplx* __restrict__ den1, cplx* __restrict__ gorbg) {
+  const size_t ng = (size_t)Nr * nlat;
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ng * nfcore) return;
+  const int i = (int)(t / ng);
+  const size_t q = t % ng;
+  auto w = [&](int j, int k) {  // W(j, k) at q
+    cplx v = W[(size_t)pair_of[j * nfun + k] * ng + q];
+    return pair_cj[j * nfun + k] ? cconj(v) : v;
+  };
+  auto o = [&](int j) { return orbg[(size_t)j * ng + q]; };
+  const cplx oi = o(i);
+  cplx g = mkc(0.0, 0.0);
+  for (int j = 0; j < nfcore; ++j) g = csub(g, cmul(w(j, i), o(j)));                  // fcx1
+  for (int j = nfcore; j < ncore; ++j) g = cadd(g, csub(cscale(cmul(w(j, j), oi), 2.0), cmul(w(j, i), o(j))));  // dcj, dcx
+  if (ncore > 0 && nact > 0) {
+    cplx d2v = mkc(0.0, 0.0);
+    for (int ja = 0; ja < nact; ++ja)
+      for (int ka = 0; ka < nact; ++ka) d2v = cadd(d2v, cmul(w(ncore + ja, ncore + ka), den1[ka + nact * ja]));  // actj
+    g = cadd(g, cmul(d2v, oi));
+    for (int ja = 0; ja < nact; ++ja) {  // actx
+      cplx wd = mkc(0.0, 0.0);
+      for (int ka = 0; ka < nact; ++ka)
+        if (mval[ncore + ja] == mval[ncore + ka]) wd = cadd(wd, cmul(o(ncore + ka), cscale(den1[ka + nact * ja], -0.5)));
+      g = cadd(g, cmul(wd, w(ncore + ja, i)));
+    }
+  }
+  gorbg[(size_t)i * ng + q] = g;
+}
+
+// hprod_gfock_sum (hprod_gfock.F90:198-230) plus, in the velocity gauge, the
+// E_z z phi that hprod_dipole adds to the dynamic rows (hprod_dipole.F90:61-64).
+// The frozen-core rows' h1 already holds that term: the RHS one-body coupling
+// adds E_z z phi to them in the velocity gauge (hprod_htot.F90 via hprod_zprod).
+__global__ void gfock_sum_kernel(size_t n, size_t nfc, double ef, const cplx* __restrict__ gorb, const cplx* __restrict__ v2orb,
+                                 const cplx* __restrict__ h0orb, const cplx* __restrict__ h1orb, const cplx* __restrict__ zo,
+                                 cplx* __restrict__ g) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  cplx v = cadd(cadd(gorb[t], v2orb[t]), cadd(h1orb[t], h0orb[t]));
+  if (t >= nfc) v = cadd(v, cscale(zo[t], ef));
+  g[t] = v;
+}
+
+// out[e] = sum_k conj(A_k) B_k over one orbital (nbas values) for each entry
+// e = (buffer of A, row of A, buffer of B, row of B): one block per entry,
+// fixed summation order
+struct RowDotBufs { const cplx* b[4]; };
+__global__ void __launch_bounds__(256) rowdot_kernel(size_t nbas, RowDotBufs bufs, const int4* __restrict__ ent,
+                                                     cplx* __restrict__ out) {
+  __shared__ double re[256], im[256];
+  const int4 e = ent[blockIdx.x];
+  const cplx* A = bufs.b[e.x] + (size_t)e.y * nbas;
+  const cplx* B = bufs.b[e.z] + (size_t)e.w * nbas;
+  double sr = 0.0, si = 0.0;
+  for (size_t k = threadIdx.x; k < nbas; k += blockDim.x) {
+    cplx a = A[k], b = B[k];
+    sr += a.x * b.x + a.y * b.y;
+    si += a.x * b.y - a.y * b.x;
+  }
+  re[threadIdx.x] = sr; im[threadIdx.x] = si;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { re[threadIdx.x] += re[threadIdx.x + w]; im[threadIdx.x] += im[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = mkc(re[0], im[0]);
 }
 
 // out = Re sum conj(a) b over n complex values (one block, fixed order)
@@ -2252,61 +2339,149 @@ int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out) {
   return (rc || e != cudaSuccess) ? ST_CUDA : 0;
 }
 
-// hprod_dipole (hprod_dipole.F90:2-146) of a state without frozen-core
-// orbitals: the length, velocity and acceleration forms as 1-RDM traces of
-// z, p_z (the one-body kernel's velocity coupling at unit field) and the
-// acceleration operator, plus A_z N (velocity gauge) and -E_z N.
-// out = dip(1:3), vel(1:3), acc(1:3); ST_CONFIG with frozen-core orbitals
-// (their generalized-Fock corrections are not built).
+// the index maps of the frozen-core dipole's overlaps (rowdot entries):
+// buffers 0 orb, 1 z phi, 2 p_z phi, 3 generalized-Fock vectors
+static void dipole_fc_entries(Ctx& c) {
+  if (c.dip_rd_ent) return;
+  const int nf = c.nfun, nfc = c.nfcore;
+  std::vector<int4> ent;
+  auto add = [&](int ba, int ra, int bb, int rb) { ent.push_back(make_int4(ba, ra, bb, rb)); return (int)ent.size() - 1; };
+  c.dip_ia.assign(nfc, -1); c.dip_ib.assign(nfc, -1);
+  c.dip_if.assign((size_t)nfc * nf, -1); c.dip_isz.assign((size_t)nf * nfc, -1); c.dip_isp.assign((size_t)nf * nfc, -1);
+  for (int f = 0; f < nfc; ++f) { c.dip_ia[f] = add(1, f, 3, f); c.dip_ib[f] = add(2, f, 3, f); }
+  for (int j = 0; j < nfc; ++j)
+    for (int b = 0; b < nf; ++b)
+      if (c.mval[b] == c.mval[j]) c.dip_if[(size_t)j * nf + b] = add(0, j, 3, b);
+  for (int a = 0; a < nf; ++a)
+    for (int j = 0; j < nfc; ++j)
+      if (c.mval[a] == c.mval[j]) {
+        c.dip_isz[(size_t)a * nfc + j] = add(1, a, 0, j);
+        c.dip_isp[(size_t)a * nfc + j] = add(2, a, 0, j);
+      }
+  c.dip_rd_n = (int)ent.size();
+  c.dip_rd_ent = dupload(ent);
+  c.dip_rd = dalloc<cplx>(ent.size());
+  const size_t so = c.nbas * c.nfun;
+  c.dip_z = dalloc<cplx>(so); c.dip_p = dalloc<cplx>(so); c.dip_g = dalloc<cplx>(so);
+  c.dip_lfd = dalloc<double>(9);
+}
+
+// hprod_dipole (hprod_dipole.F90:2-146; no pseudopotential, do_op1tr off):
+// the length, velocity and acceleration forms as 1-RDM traces of z, p_z (the
+// one-body kernel's velocity coupling at unit field) and the acceleration
+// operator, plus A_z N (velocity gauge) and -E_z N.  With frozen-core
+// orbitals the velocity and acceleration forms add the generalized-Fock
+// corrections: the generalized-Fock vectors g (hprod_gfock: the RHS's
+// orbital phase, one-body and mean-field passes, then the mean field on the
+// frozen-core rows), and
+//   vel(2) = -4 Im sum_{f < nfcore} <z phi_f|g_f> - 2 Im trace1(z phi, P_fc g),
+//   acc(2) the same with p_z phi,
+// P_fc g_b = sum_{j < nfcore, m_j = m_b} phi_j <phi_j|g_b> (hprod_projfc).
+// The overlaps are reduced on the device; their few scalars are combined here.
+// out = dip(1:3), vel(1:3), acc(1:3).
 int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield, double* out) {
   Ctx& c = ctx();
   if (!c.initialized || !out || !lfield) return ST_CONFIG;
-  if (c.nfcore > 0) return ST_CONFIG;
   cudaStream_t st = c.st;
   dipole_entries(c);
   int rc = 0;
-  if (c.nact > 0) {
-    CiArgs ca{};
-    ca.t = c.cit; ca.cic = (const cplx*)d_cic; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
-    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, st));
-    rc |= chk("ci rdm", launch_ci_rdm(ca, st));
-  }
   if (!c.dip_lf) {
     const double unit[9] = {0, 0, 1, 0, 0, 0, 0, 0, 0};  // lfield(3,1) = 1: the operator at unit field
     c.dip_lf = dupload(std::vector<double>(unit, unit + 9));
     c.dip_out = dalloc<double>(3);
   }
-  // p_z phi: the velocity coupling of the one-body kernel (igauge 1, unit field) into h1orb
+  const bool fc = c.nfcore > 0;
+  const cplx* w = (const cplx*)d_wfn;
+  if (fc) {
+    // generalized-Fock vectors: the RHS passes leave the orbitals (frozen cores with their gauge
+    // phase), den1, every pair potential and the dynamic rows' g and v2 in place
+    dipole_fc_entries(c);
+    cudaMemcpyAsync(c.dip_lfd, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+    rc |= run_htot(c, c.dip_lfd, (const cplx*)d_wfn, (const cplx*)d_cic, c.hwfn_io, c.hcic_io, 1.0);
+    if (c.neltot >= 2) {
+      const size_t nfcg = c.nfcore * c.ngrid;
+      fc_gfock_kernel<<<(unsigned)((nfcg + 255) / 256), 256, 0, st>>>(c.Nr, c.nlat, c.nfcore, c.ncore, c.nact, c.nfun, c.d_mval,
+                                                                      c.orbg, c.W, c.pair_of, c.pair_cj, c.den1, c.gorbg);
+      rc |= chk("fc gorb gemm", gemm(c, c.b_gorbfc, c.nfcore, c.L1, c.nlat, false));
+    }
+    w = c.orb;
+  } else if (c.nact > 0) {
+    CiArgs ca{};
+    ca.t = c.cit; ca.cic = (const cplx*)d_cic; ca.Da = c.Da; ca.Db = c.Db; ca.T = c.T; ca.den1 = c.den1; ca.den2 = c.den2;
+    rc |= chk("ci dvec", launch_ci_dvec(ca, c.maxsec, st));
+    rc |= chk("ci rdm", launch_ci_rdm(ca, st));
+  }
+  // p_z phi: the velocity coupling of the one-body kernel (igauge 1, unit field); z phi (igauge 0)
   OneBodyArgs ob{};
   ob.Nr = c.Nr; ob.L1 = c.L1; ob.nd = c.nd; ob.nfun = c.nfun; ob.nfcore = 0; ob.mmax1 = c.mmax1; ob.igauge = 1;
   ob.radk = c.radk; ob.radk0 = c.radk0; ob.radp = c.radp; ob.tdiag = c.tdiag; ob.xrad = c.xrad; ob.alph = c.alph;
-  ob.mval = c.d_mval; ob.orb = (const cplx*)d_wfn; ob.h0orb = c.h0orb; ob.h1orb = c.h1orb; ob.lfield = c.dip_lf;
+  ob.mval = c.d_mval; ob.orb = w; ob.h0orb = fc ? c.dip_g : c.h0orb; ob.h1orb = fc ? c.dip_p : c.h1orb; ob.lfield = c.dip_lf;
   rc |= chk("onebody", launch_onebody(ob, st));
+  const cplx* po = fc ? c.dip_p : c.h1orb;
+  if (fc) {
+    ob.igauge = 0; ob.h1orb = c.dip_z;
+    rc |= chk("onebody", launch_onebody(ob, st));
+    const size_t so = c.nbas * c.nfun;
+    const double ef = c.igauge == 1 ? lfield[5] : 0.0;
+    gfock_sum_kernel<<<(unsigned)((so + 255) / 256), 256, 0, st>>>(so, c.nfcore * c.nbas, ef, c.gorb, c.v2orb, c.h0orb, c.h1orb,
+                                                                   c.dip_z, c.dip_g);
+    RowDotBufs bufs{{c.orb, c.dip_z, c.dip_p, c.dip_g}};
+    rowdot_kernel<<<c.dip_rd_n, 256, 0, st>>>(c.nbas, bufs, c.dip_rd_ent, c.dip_rd);
+    rc |= chk("gfock overlaps", (int)cudaGetLastError());
+  }
   DipoleArgs da{};
   da.Nr = c.Nr; da.L1 = c.L1; da.mmax1 = c.mmax1; da.ncore = c.ncore; da.nact = c.nact; da.nent = c.dip_nent;
-  da.xrad = c.xrad; da.alph = c.alph; da.mval = c.d_mval; da.ent = c.dip_ent; da.wfn = (const cplx*)d_wfn;
+  da.xrad = c.xrad; da.alph = c.alph; da.mval = c.d_mval; da.ent = c.dip_ent; da.wfn = w;
   da.den1 = c.den1; da.partial = c.dip_partial; da.znuc = c.znuc;
   for (int k = 0; k < 3; ++k) {  // z, p_z, acceleration
     da.mode = k == 0 ? 0 : (k == 1 ? 2 : 1);
-    da.pv = k == 1 ? c.h1orb : nullptr;
+    da.pv = k == 1 ? po : nullptr;
     da.out = c.dip_out + k;
     rc |= chk("dipole", launch_dipole(da, st));
   }
   double tr[3];
+  std::vector<std::complex<double>> rd(fc ? c.dip_rd_n : 0), den1(fc ? (size_t)c.nact * c.nact : 0);
   cudaMemcpyAsync(tr, c.dip_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (fc) {
+    cudaMemcpyAsync(rd.data(), c.dip_rd, rd.size() * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+    if (!den1.empty()) cudaMemcpyAsync(den1.data(), c.den1, den1.size() * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+  }
   cudaError_t e = cudaStreamSynchronize(st);
   if (rc || e != cudaSuccess) return ST_CUDA;
   const double v = tr[1] + (c.igauge == 1 ? lfield[8] * c.neltot : 0.0), a = tr[2] - lfield[5] * c.neltot;
-  const double r[9] = {tr[0], 0.0, tr[0], v, 0.0, v, a, 0.0, a};
+  double vc = 0.0, ac = 0.0;
+  if (fc) {
+    const int nf = c.nfun, nfc = c.nfcore;
+    // <X phi_a | P_fc g_b> = sum_{j < nfcore, m_j = m_b} <X phi_a|phi_j> <phi_j|g_b>
+    auto xpg = [&](const std::vector<int>& isx, int a_, int b_) {
+      std::complex<double> s = 0.0;
+      for (int j = 0; j < nfc; ++j) {
+        const int i1 = isx[(size_t)a_ * nfc + j], i2 = c.dip_if[(size_t)j * nf + b_];
+        if (i1 >= 0 && i2 >= 0) s += rd[i1] * rd[i2];
+      }
+      return s;
+    };
+    auto trace1 = [&](const std::vector<int>& isx) {  // hprod_trace1(.true., den1, X phi, P_fc g)
+      std::complex<double> s = 0.0;
+      for (int f = 0; f < c.ncore; ++f) s += 2.0 * xpg(isx, f, f);
+      for (int ia = 0; ia < c.nact; ++ia)
+        for (int ja = 0; ja < c.nact; ++ja)
+          if (c.mval[c.ncore + ia] == c.mval[c.ncore + ja]) s += xpg(isx, c.ncore + ia, c.ncore + ja) * den1[ja + c.nact * ia];
+      return s;
+    };
+    std::complex<double> v1 = 0.0, a1 = 0.0;
+    for (int f = 0; f < nfc; ++f) { v1 += rd[c.dip_ia[f]]; a1 += rd[c.dip_ib[f]]; }
+    vc = -4.0 * v1.imag() - 2.0 * trace1(c.dip_isz).imag();
+    ac = -4.0 * a1.imag() - 2.0 * trace1(c.dip_isp).imag();
+  }
+  const double r[9] = {tr[0], 0.0, tr[0], v, vc, v + vc, a, ac, a + ac};
   for (int k = 0; k < 9; ++k) out[k] = r[k];
   return 0;
 }
 
 // hprod_dipole_ (include/wrapper.hpp:114; clhprod::dipole, clhprod.cpp:218-222)
 // with host buffers: the state is copied in and dip, vel, acc (3 each) are
-// written back.  Without frozen-core orbitals all three forms; with them the
-// length form (which needs no correction) and NaN for the velocity and
-// acceleration forms, with ST_CONFIG in the status word.
+// written back; errors go to the status word.
 void hprod_dipole_(const double* lfield, const double* wfn, const double* cic, double* dip, double* vel, double* acc) {
   Ctx& c = ctx();
   if (!c.initialized) { c.status |= ST_CONFIG; return; }
@@ -2314,16 +2489,10 @@ void hprod_dipole_(const double* lfield, const double* wfn, const double* cic, d
   cudaMemcpyAsync(c.wfn_io, wfn, c.nbas * c.nfun * sizeof(cplx), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(c.cic_io, cic, c.lcic * sizeof(cplx), cudaMemcpyHostToDevice, st);
   double out[9];
-  int rc;
-  if (c.nfcore == 0) {
-    rc = td1c_gpu_dipole3(c.wfn_io, c.cic_io, lfield, out);
-  } else {
-    double d = 0.0;
-    rc = td1c_gpu_dipole(c.wfn_io, c.cic_io, &d);
+  const int rc = td1c_gpu_dipole3(c.wfn_io, c.cic_io, lfield, out);
+  if (rc) {
     const double nan = std::numeric_limits<double>::quiet_NaN();
-    const double r[9] = {d, 0.0, d, nan, nan, nan, nan, nan, nan};
-    for (int k = 0; k < 9; ++k) out[k] = r[k];
-    c.status |= ST_CONFIG;
+    for (int k = 0; k < 9; ++k) out[k] = nan;
   }
   c.status |= rc;
   for (int k = 0; k < 3; ++k) { dip[k] = out[k]; vel[k] = out[3 + k]; acc[k] = out[6 + k]; }

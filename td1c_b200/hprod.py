@@ -148,8 +148,9 @@ class HProd:
         return float(out[0])
 
     def dipole3_dev(self, d_wfn, d_cic, lfield):
-        """hprod_dipole of a device state without frozen-core orbitals: (dip[3], vel[3], acc[3]),
-        the length, velocity and acceleration forms."""
+        """hprod_dipole of a device state: (dip[3], vel[3], acc[3]), the length, velocity and
+        acceleration forms (with frozen-core orbitals vel[1], acc[1] are the generalized-Fock
+        corrections)."""
         out = np.zeros(9)
         lf = np.ascontiguousarray(lfield, dtype=np.float64)
         self._check(self.lib.td1c_gpu_dipole3(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(lf), _dp(out)))

@@ -1,11 +1,12 @@
 """The three forms of hprod_dipole on the device against the oracle.
 
-Length, velocity and acceleration forms (hprod_dipole.F90:2-146) of states
-without frozen-core orbitals, at several points of a field-driven split2
-trajectory on the device, within 1e-10 of the oracle's restatement; a
-context with frozen-core orbitals refuses the call with ST_CONFIG.  The
-drop-in hprod_dipole_ (host buffers) gives the same numbers, and with a
-frozen core the length form only.
+Length, velocity and acceleration forms (hprod_dipole.F90:2-146) at several
+points of a field-driven split2 trajectory on the device, within 1e-10 of the
+oracle's restatement: states without frozen-core orbitals (He, one and two
+orbitals) and with them (C with a frozen 1s, dynamic 2s and a 2s2p active
+space, in both gauges), where the velocity and acceleration forms carry the
+generalized-Fock corrections (hprod_gfock, hprod_projfc).  The drop-in
+hprod_dipole_ (host buffers) gives the same numbers.
 """
 import numpy as np
 import pytest
@@ -16,7 +17,7 @@ from .helpers import oracle_tables, oracle_state
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("base", [W.HE_SMALL, W.HE_TDHF], ids=lambda w: w["name"])
+@pytest.mark.parametrize("base", [W.HE_SMALL, W.HE_TDHF, W.MIXED_SMALL, W.LENGTH_SMALL], ids=lambda w: w["name"])
 def test_dipole_forms_match_oracle(cuda_ok, base):
     import torch
     from oracle.oracle import Oracle
@@ -45,28 +46,9 @@ def test_dipole_forms_match_oracle(cuda_ok, base):
                 scale = max(1e-3, np.abs(rv).max())
                 assert np.abs(gv - rv).max() < 1e-10 * scale, (s, g, ref)
             assert g[1][2] != 0.0 and g[2][2] != 0.0
+            assert (g[1][1] != 0.0 and g[2][1] != 0.0) == (o.dims["nfcore"] > 0)
             h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), t, dt, 2)
             h.sync()
-    finally:
-        h.final()
-
-
-@pytest.mark.gpu
-def test_dipole_forms_refused_with_frozen_core(cuda_ok):
-    import torch
-    from oracle.oracle import Oracle
-    from td1c_b200.hprod import HProd, StatusError
-    wl = dict(W.MIXED_SMALL, split_type=1)
-    o = Oracle(wl)
-    rad, ang = oracle_tables(o)
-    h = HProd(wl, rad, ang)
-    try:
-        orb, cic = oracle_state(o)
-        h.set_wfn0(orb, cic)
-        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
-        d_cic = torch.from_numpy(cic.copy()).cuda()
-        with pytest.raises(StatusError):
-            h.dipole3_dev(d_orb.data_ptr(), d_cic.data_ptr(), np.zeros(9))
     finally:
         h.final()
 
@@ -84,7 +66,6 @@ def _host_dipole(h, orb, cic, lf):
 
 @pytest.mark.gpu
 def test_hprod_dipole_dropin(cuda_ok):
-    import torch
     from oracle.oracle import Oracle
     from td1c_b200.hprod import HProd
     # without frozen core: all three forms, as td1c_gpu_dipole3 and the oracle
@@ -104,20 +85,20 @@ def test_hprod_dipole_dropin(cuda_ok):
         assert h.lib.td1c_gpu_last_status() == 0
     finally:
         h.final()
-    # with a frozen core: the length form only, the status word flags the rest
+    # with a frozen core: all three forms with their generalized-Fock corrections
     wl = dict(W.MIXED_SMALL, split_type=1)
     o = Oracle(wl)
     rad, ang = oracle_tables(o)
     h = HProd(wl, rad, ang)
     try:
         orb, cic = oracle_state(o)
+        o.set_wfn0(orb, cic)
         h.set_wfn0(orb, cic)
-        dip, vel, acc = _host_dipole(h, orb, cic, o.field(30.0))
-        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
-        d_cic = torch.from_numpy(cic.copy()).cuda()
-        d_len = h.dipole_dev(d_orb.data_ptr(), d_cic.data_ptr())
-        assert dip[0] == dip[2] and dip[1] == 0.0 and abs(dip[0] - d_len) <= 1e-12 * max(1.0, abs(d_len))
-        assert np.all(np.isnan(vel)) and np.all(np.isnan(acc))
-        assert h.lib.td1c_gpu_last_status() & 16
+        lf = o.field(30.0)
+        got = _host_dipole(h, orb, cic, lf)
+        ref = o.dipole3(orb, cic, lf)
+        for gv, rv in zip(got, ref):
+            assert np.abs(gv - rv).max() < 1e-10 * max(1e-3, np.abs(rv).max()), (got, ref)
+        assert got[1][1] != 0.0 and h.lib.td1c_gpu_last_status() == 0
     finally:
         h.final()
