@@ -140,6 +140,17 @@ int td1c_gpu_dipole(const void* d_wfn, const void* d_cic, double* out);
  * and the call also runs the RHS passes (the library's RHS scratch is
  * overwritten).  lfield: host lfield(3,3). */
 int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
+/* The mixed-precision form of the RHS (no counterpart in the reference; the
+ * precision variant of hprod_htot, src/hprod/hprod_htot.F90:2-208): on = 1
+ * runs the mean field's pair-density multipoles (bas_ang2sph2.F90:330-482)
+ * and pair potentials on the grid (bas_sph2ang2.F90:334-463) in split TF32
+ * on the tensor cores with FP32 accumulation, FP64 everywhere else; 0 restores
+ * the plain FP64 path.  Every later RHS and step uses the mode. */
+int td1c_gpu_set_mixed(int on);
+/* Deviation of the mixed form from FP64 on one RHS of a device state:
+ * out[0..2] = max |delta| / max |FP64 value| of the pair-density multipoles,
+ * the pair potentials on the grid and hwfn.  lfield: host lfield(3,3). */
+int td1c_gpu_mixed_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
 /* Drop-in for hprod_dipole_ (include/wrapper.hpp:114, called by
  * clhprod::dipole, src/hprod/clhprod.cpp:218-222): host lfield(3,3), wfn,
  * cic; writes dip[3], vel[3], acc[3] (td1c_gpu_dipole3 on the library's

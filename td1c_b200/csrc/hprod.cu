@@ -162,6 +162,7 @@ struct Ctx {
   cudaStream_t st4 = nullptr;  // stream on which graph-loop bodies are captured
   // phase timing (off during graph capture)
   bool profile = false;
+  int mixed = 0;  // 1: the mean field's pair-density and pair-potential transforms in split TF32 (tcgen05)
   cudaEvent_t ev[16] = {};
   cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1270,6 +1271,13 @@ int gemm(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
   c.launches++;
   return launch_legendre_gemm(b, nb, M, K, 2 * c.Nr, pair, c.st);
 }
+// the mean field's transforms (pair densities theta -> l, pair potentials l -> theta):
+// FP64 DMMA, or split TF32 on tcgen05 in the mixed-precision form
+int gemm_mf(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
+  if (!c.mixed) return gemm(c, b, nb, M, K, pair);
+  c.launches++;
+  return launch_legendre_gemm_tf32(b, nb, M, K, 2 * c.Nr, pair, c.d_status, c.st);
+}
 
 // report the first failing launcher of an RHS (status ST_CUDA is set by the caller)
 int chk(const char* what, int rc) {
@@ -1345,7 +1353,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   bool i2_forked = false;
   // mean field
   if (c.neltot >= 2 && c.npair > 0) {
-    rc |= chk("rho gemm", gemm(c, c.b_rho, c.npair, c.L2, c.nlat, true));
+    rc |= chk("rho gemm", gemm_mf(c, c.b_rho, c.npair, c.L2, c.nlat, true));
     mark();  // end rho_gemm
     rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
     c.launches += 3;
@@ -1364,7 +1372,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
       i2_forked = true;
     }
     mark();  // end poisson
-    rc |= chk("W gemm", gemm(c, c.b_W, c.npair, c.nlat, c.L2, false));
+    rc |= chk("W gemm", gemm_mf(c, c.b_W, c.npair, c.nlat, c.L2, false));
     mark();  // end w_gemm
     join();
     rc |= chk("mfprod", launch_mfprod(c.mf, st));
@@ -2027,7 +2035,7 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
     int s0 = 0;
     cudaGraphExec_t& ge = c.graph_exec[kind];
     bool cached;
-    const int ctl = c.icomp * 2 + c.igauge;
+    const int ctl = c.icomp * 2 + c.igauge + 4 * c.mixed;
     if (kind == 0) {
       cached = ge && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt && b.g_ro == b.reset_orb &&
                b.g_ctl == ctl;
@@ -2363,7 +2371,7 @@ static void dipole_fc_entries(Ctx& c) {
   c.dip_rd = dalloc<cplx>(ent.size());
   const size_t so = c.nbas * c.nfun;
   c.dip_z = dalloc<cplx>(so); c.dip_p = dalloc<cplx>(so); c.dip_g = dalloc<cplx>(so);
-  c.dip_lfd = dalloc<double>(9);
+  if (!c.dip_lfd) c.dip_lfd = dalloc<double>(9);
 }
 
 // hprod_dipole (hprod_dipole.F90:2-146; no pseudopotential, do_op1tr off):
@@ -2697,6 +2705,56 @@ int td1c_gpu_rk4_reset(const void* d_wfn0, const void* d_cic0) {
 }
 
 void* td1c_gpu_stream(void) { return g ? (void*)g->st : nullptr; }
+
+// the mixed-precision form of the RHS: on = 1 runs the mean field's pair-density
+// multipoles and pair potentials on the grid (the two theta <-> l transforms of
+// the pair fields) in split TF32 on the tensor cores, FP32 accumulation, FP64
+// everywhere else; on = 0 restores the plain FP64 path.  Captured step graphs
+// are recaptured on their next use.
+int td1c_gpu_set_mixed(int on) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  c.mixed = on ? 1 : 0;
+  return 0;
+}
+
+// the deviation of the mixed-precision form from FP64 on one RHS of a device
+// state: out[0] = max |d rho2| / max |rho2| (pair-density multipoles),
+// out[1] = the same for the pair potentials on the grid W, out[2] for hwfn.
+// Runs the RHS twice (lfield: host lfield(3,3)); the mode is restored.
+int td1c_gpu_mixed_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out || !lfield) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  if (!c.dip_lfd) c.dip_lfd = dalloc<double>(9);
+  cudaMemcpyAsync(c.dip_lfd, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+  const size_t nr = c.nbas2 * c.npair, nw = c.ngrid * c.npair, nh = c.nbas * c.nfun;
+  std::vector<std::complex<double>> r[2], w[2], h[2];
+  const int keep = c.mixed;
+  int rc = 0;
+  for (int mode = 0; mode < 2; ++mode) {
+    c.mixed = mode;
+    rc |= run_htot(c, c.dip_lfd, (const cplx*)d_wfn, (const cplx*)d_cic, c.hwfn_io, c.hcic_io, 1.0);
+    r[mode].resize(nr); w[mode].resize(nw); h[mode].resize(nh);
+    cudaMemcpyAsync(r[mode].data(), c.rho2, nr * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(w[mode].data(), c.W, nw * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h[mode].data(), c.hwfn_io, nh * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc |= ST_CUDA;
+  }
+  c.mixed = keep;
+  if (rc) return ST_CUDA;
+  int dst = 0;
+  cudaMemcpy(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  c.status |= dst;
+  if (dst & ST_TIMEOUT) return ST_TIMEOUT;
+  auto rel = [](const std::vector<std::complex<double>>& a, const std::vector<std::complex<double>>& b) {
+    double d = 0.0, m = 0.0;
+    for (size_t k = 0; k < a.size(); ++k) { d = std::max(d, std::abs(b[k] - a[k])); m = std::max(m, std::abs(a[k])); }
+    return m > 0.0 ? d / m : d;
+  };
+  out[0] = rel(r[0], r[1]); out[1] = rel(w[0], w[1]); out[2] = rel(h[0], h[1]);
+  return 0;
+}
 
 int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d_wfn, const void* d_cic, void* d_hwfn,
                      void* d_hcic, double* ms, char* names, int names_cap) {

@@ -28,6 +28,10 @@ struct LegGemmBatch {
 __host__ __device__ inline int legendre_lda(int k) { return (k + 31) / 32 * 32; }
 int launch_legendre_gemm(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair,
                          cudaStream_t st);
+// the same transform in split TF32 on tcgen05 (FP32 accumulation, FP64 in and out);
+// a bounded wait that runs out sets ST_TIMEOUT in *status
+int launch_legendre_gemm_tf32(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair, int* status,
+                              cudaStream_t st);
 
 // ---- one-body: tprod + zprod/pzprod (hprod_tprod.F90, hprod_zprod.F90, hprod_pzprod.F90)
 struct OneBodyArgs {

@@ -156,6 +156,19 @@ class HProd:
         self._check(self.lib.td1c_gpu_dipole3(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(lf), _dp(out)))
         return out[0:3], out[3:6], out[6:9]
 
+    def set_mixed(self, on):
+        """Mixed-precision form of every later RHS: the mean field's pair-density multipoles and pair
+        potentials in split TF32 on the tensor cores (on=True), or plain FP64 (on=False)."""
+        self._check(self.lib.td1c_gpu_set_mixed(1 if on else 0))
+
+    def mixed_selftest(self, d_wfn, d_cic, lfield):
+        """Relative deviation of the mixed form from FP64 on one RHS: (pair-density multipoles,
+        pair potentials on the grid, hwfn)."""
+        out = np.zeros(3)
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        self._check(self.lib.td1c_gpu_mixed_selftest(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(lf), _dp(out)))
+        return out
+
     def orth_dev(self, d_wfn, d_cic):
         """wfn_orth_cic + wfn_orth_orb in place on device buffers."""
         self._check(self.lib.td1c_gpu_orth(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic)))

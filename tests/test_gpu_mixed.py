@@ -1,0 +1,79 @@
+"""The mixed-precision form of the RHS against the plain FP64 path on the device.
+
+The mean field's pair-density multipoles and pair potentials on the grid run in
+split TF32 on the tensor cores (FP32 accumulation); everything else stays
+FP64.  One RHS: the two transformed fields deviate from FP64 by FP32-class
+amounts, and so does hwfn.  A field-driven split2 trajectory: the
+length-form dipole stays within 1e-5 a.u. and the CI and orbital norms (the
+absorbing mask acts on the orbitals) within 1e-8 of the
+FP64 trajectory (the FP64 device path itself matches the oracle to 1e-10 in
+the other GPU tests).
+"""
+import numpy as np
+import pytest
+
+from td1c_b200 import workloads as W
+
+from .helpers import oracle_tables, oracle_state
+
+
+def _setup(base):
+    from oracle.oracle import Oracle
+    from td1c_b200.hprod import HProd
+    wl = dict(base, split_type=1)
+    o = Oracle(wl)
+    o.set_split(1)
+    rad, ang = oracle_tables(o)
+    h = HProd(wl, rad, ang)
+    orb, cic = oracle_state(o)
+    o.set_wfn0(orb, cic)
+    h.set_wfn0(orb, cic)
+    orb, cic = o.orth(orb, cic)
+    return o, h, wl, orb, cic
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.NE_SMALL, W.MIXED_SMALL], ids=lambda w: w["name"])
+def test_mixed_rhs_deviation(cuda_ok, base):
+    import torch
+    o, h, wl, orb, cic = _setup(base)
+    try:
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        dev = h.mixed_selftest(d_orb.data_ptr(), d_cic.data_ptr(), o.field(30.0))
+        assert np.all(dev > 0.0), dev            # the tensor-core path ran and rounds differently
+        assert dev[0] < 2e-6 and dev[1] < 2e-6, dev
+        assert dev[2] < 1e-5, dev
+        assert h.lib.td1c_gpu_last_status() == 0
+    finally:
+        h.final()
+
+
+@pytest.mark.gpu
+def test_mixed_trajectory_dipole_and_norm(cuda_ok):
+    import torch
+    o, h, wl, orb, cic = _setup(W.MIXED_SMALL)
+    try:
+        freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+        t0, dt, nseg, per = 0.4 * wl["numcyc"] * 2 * np.pi / freq, 0.004, 10, 5
+        res = {}
+        for mixed in (False, True):
+            h.set_mixed(mixed)
+            h.rk4_reset(None, None)
+            d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+            d_cic = torch.from_numpy(cic.copy()).cuda()
+            dip, norm = [], []
+            for s in range(nseg):
+                h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), t0 + s * per * dt, dt, per)
+                h.sync()
+                dip.append(h.dipole_dev(d_orb.data_ptr(), d_cic.data_ptr()))
+                norm.append([float(torch.linalg.vector_norm(d_cic).item()), float(torch.linalg.vector_norm(d_orb).item())])
+            res[mixed] = (np.array(dip), np.array(norm))
+        h.set_mixed(False)
+        ddip = np.abs(res[True][0] - res[False][0]).max()
+        dnorm = np.abs(res[True][1] - res[False][1]).max()
+        assert 0.0 < ddip <= 1e-5, ddip
+        assert dnorm <= 1e-8, dnorm
+        assert h.lib.td1c_gpu_last_status() == 0
+    finally:
+        h.final()
