@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--workload", default="ne", choices=["ne", "he"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--prop", default="split2", choices=["split2", "etdrk2", "rk4"])
     # imaginary time tau = 3 au: the energy is within 0.07 au of its limit and
     # the smallest natural occupation stays ~1e-3.  Relaxed further, the 3d0
@@ -376,6 +377,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     value = job_throughput(world, args.steps, dt, sec)
+    d_orb_end, d_cic_end = d_orb.clone(), d_cic.clone()  # the FP64 state at the end of the window
     wn = d_orb.cpu().numpy().reshape(len(wl["orbitals"]), -1)
     traj = {"t_start_au": t1, "t_end_au": t1 + args.steps * dt,
             "orbital_norm_dev": float(np.abs(np.linalg.norm(wn, axis=1) - 1.0).max()),
@@ -459,6 +461,45 @@ def main():
         roof = {"bound": "hbm", "achieved": by / t_dom / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": by / t_dom / 1e9 / hbm, "traffic": traffic, "kernel": dom, "peak_source": hbm_src}
 
+    # ---- the mixed-precision form (pair-density multipoles and pair potentials in split TF32 on the
+    # tensor cores) over the same window: same start state, warm-up and timed steps; its deviation
+    # from the FP64 trajectory at the end of the window, and of one RHS at the window's start
+    mixed = None
+    if not args.no_mixed:
+        d_orb.copy_(d_orb0)
+        d_cic.copy_(d_cic0)
+        torch.cuda.synchronize()
+        rhs_dev = h.mixed_selftest(d_orb.data_ptr(), d_cic.data_ptr(), gauge_field(wl, t0))
+        h.set_mixed(True)
+        if args.prop == "rk4":
+            h.rk4_reset(d_orb0.data_ptr(), d_cic0.data_ptr())
+        else:
+            h.rk4_reset(None, None)
+        steps(t0, args.warmup)
+        h.sync()
+        torch.cuda.synchronize()
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(ext)
+        steps(t1, args.steps)
+        e5.record(ext)
+        torch.cuda.synchronize()
+        h.sync()
+        sec_m = max_over_ranks(e4.elapsed_time(e5) / 1e3, dist if world > 1 else None, dev)
+        h.set_mixed(False)
+        dip_m = h.dipole_dev(d_orb.data_ptr(), d_cic.data_ptr())
+        dip_p = h.dipole_dev(d_orb_end.data_ptr(), d_cic_end.data_ptr())
+        nf = len(wl["orbitals"])
+        nm = np.linalg.norm(d_orb.cpu().numpy().reshape(nf, -1), axis=1)
+        npl = np.linalg.norm(d_orb_end.cpu().numpy().reshape(nf, -1), axis=1)
+        vm = job_throughput(world, args.steps, dt, sec_m)
+        mixed = {"value": vm, "unit": "fs/s", "ms_per_step": sec_m / args.steps * 1e3, "speedup_vs_fp64": vm / value,
+                 "precision": "pair-density multipoles and pair potentials in split TF32 (tcgen05, FP32 accumulation); "
+                              "all else FP64",
+                 "dipole_dev_end_au": abs(dip_m - dip_p), "orbital_norm_dev_end": float(np.abs(nm - npl).max()),
+                 "rhs_rel_dev": {"rho2": float(rhs_dev[0]), "W": float(rhs_dev[1]), "hwfn": float(rhs_dev[2])},
+                 "window": "t0 + warm-up, then the timed steps (as the FP64 value); deviations at the window's end "
+                           "against the FP64 trajectory"}
+
     h.final()
     if rank != 0:
         if world > 1:
@@ -482,6 +523,7 @@ def main():
         "phases_ms_per_rhs": {k: round(v, 4) for k, v in phases.items()},
         "one_body_half_step": h1_ms,
         "clocks": clk.summary(),
+        "mixed": mixed,
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, dt, args.prop)
