@@ -49,6 +49,8 @@ def _load():
     lib.orc_dpade_prod.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_double, dp]
     lib.orc_etd4_fun.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+    lib.orc_v2sph.restype = ctypes.c_int
+    lib.orc_v2sph.argtypes = [vp, dp]
     lib.orc_dipole3.restype = ctypes.c_int
     lib.orc_dipole3.argtypes = [vp, dp, dp, dp, dp]
     for name in ("orc_split2", "orc_etdrk2", "orc_etdrk4"):
@@ -139,6 +141,16 @@ class Oracle:
         self.lib.orc_htot(self.h, float(dtime), _dp(lf), _dp(wfn.view(np.float64)), _dp(cic.view(np.float64)),
                           _dp(hw.view(np.float64)), _dp(hc.view(np.float64)))
         return hw, hc
+
+    def v2sph(self):
+        """Pair potentials v2sph of the last RHS for the 'dyn' pairs (j >= i, both dynamic):
+        [npair][lmax2 + 1][nrad - 1] complex."""
+        ndyn = len(self.wl["orbitals"]) - self.dims["nfcore"]
+        shape = (ndyn * (ndyn + 1) // 2, self.wl["lmax2"] + 1, self.dims["nrad"] - 1)
+        out = np.zeros(shape, dtype=np.complex128)
+        n = self.lib.orc_v2sph(self.h, _dp(out.view(np.float64)))
+        assert n == shape[0]
+        return out
 
     def energies(self):
         e = np.zeros(5)

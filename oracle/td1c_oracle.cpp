@@ -1654,6 +1654,19 @@ void orc_htot(void* h, double dtime, const double* lfield, const double* wfn, co
   static_cast<Oracle*>(h)->htot(dtime, lfield, reinterpret_cast<const cd*>(wfn), reinterpret_cast<const cd*>(cic),
                                 reinterpret_cast<cd*>(hwfn), reinterpret_cast<cd*>(hcic));
 }
+// the pair potentials v2sph(r, l, j, i) of the last RHS for the 'dyn' pairs (j >= i, both dynamic),
+// pair-major in the order of the pair list, then l, then r: [npair][L2][Nr] complex
+int orc_v2sph(void* h, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::vector<std::pair<int, int>> P;
+  o->pairs("dyn", P);
+  cd* z = reinterpret_cast<cd*>(out);
+  size_t k = 0;
+  for (auto& pr : P)
+    for (int l = 0; l <= o->lmax2; ++l)
+      for (int ir = 0; ir < o->Nr; ++ir) z[k++] = o->v2sph[o->isp(ir, l, pr.first, pr.second)];
+  return (int)P.size();
+}
 void orc_energies(void* h, double* e) {
   Oracle* o = static_cast<Oracle*>(h);
   e[0] = o->ene_fcore; e[1] = o->ene_dcore; e[2] = o->ene_core; e[3] = o->ene_act; e[4] = o->ene_tot;

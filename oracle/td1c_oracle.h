@@ -116,6 +116,9 @@ void  orc_relax_etdrk2(void* h, double dt, int ncyc, int maxcyc, double thresh, 
 /* Observable: length-form dipole <z> of the full state (orbitals + CI)      */
 double orc_dipole(void* h, const double* wfn, const double* cic);
 int   orc_num_threads(void);
+/* v2sph of the last RHS for the 'dyn' pairs: out [npair][lmax2 + 1][nrad - 1]
+ * complex; returns npair (test data for the learned mean-field predictor).  */
+int   orc_v2sph(void* h, double* out);
 
 #ifdef __cplusplus
 }

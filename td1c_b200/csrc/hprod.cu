@@ -418,7 +418,7 @@ __device__ void herm_reg_inverse_warp(int n, double thr, const cplx* a, cplx* in
     // converged at the rounding floor of a cyclic Jacobi, |off|^2 ~ (n eps)^2 |diag|^2
     if (off <= 1e-30 * fmax(dg, 1e-300)) { conv = true; break; }
     for (int rnd = 0; rnd < N - 1; ++rnd) {
-      // rotation parameters of this round's disjoint pairs
+      // rotation parameters of this sweep stage's disjoint pairs
       if (lane < N / 2) {
         const int i = lane;
         auto player = [&](int pos) { return pos == 0 ? 0 : ((pos - 1 + rnd) % (N - 1)) + 1; };
