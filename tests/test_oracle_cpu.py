@@ -56,6 +56,31 @@ def test_legendre_orthonormal(he):
         assert np.abs(G[np.ix_(nz, nz)] - np.eye(nz.sum())).max() < 1e-12
 
 
+def test_legendre_tables_against_scipy():
+    """The theta tables against an independent associated-Legendre evaluation (scipy's lpmv, with
+    the Condon-Shortley phase): legf(theta, l, m) = sqrt((2l+1)/2 (l-|m|)!/(l+|m|)!) P_l^|m|(cos theta),
+    zero below |m|; legb = w_theta legf^T; the theta nodes and weights are the Gauss-Legendre rule."""
+    from scipy.special import gammaln, lpmv
+    o = Oracle(dict(W.MIXED_SMALL))
+    d = o.dims
+    nlat = d["nlat"]
+    cost, wlat = o.get("cost"), o.get("wlat")
+    x, w = np.polynomial.legendre.leggauss(nlat)
+    assert np.abs(np.sort(cost) - x).max() < 1e-14 and np.abs(wlat[np.argsort(cost)] - w).max() < 1e-14
+    for nf, nb, L in (("legf1", "legb1", d["lmax1"] + 1), ("legf2", "legb2", d["lmax2"] + 1)):
+        lf = o.get(nf).reshape(-1, nlat, L)
+        lb = o.get(nb).reshape(-1, L, nlat)
+        mm = (lf.shape[0] - 1) // 2
+        assert mm >= 1
+        for m in range(-mm, mm + 1):
+            am = abs(m)
+            ref = np.zeros((nlat, L))
+            for l in range(am, L):
+                ref[:, l] = np.sqrt((2 * l + 1) / 2.0 * np.exp(gammaln(l - am + 1) - gammaln(l + am + 1))) * lpmv(am, l, cost)
+            assert np.abs(lf[m + mm] - ref).max() < 1e-13 * max(1.0, np.abs(ref).max()), (nf, m)
+            assert np.abs(lb[m + mm] - (lf[m + mm] * wlat[:, None]).T).max() < 1e-15, (nb, m)
+
+
 def test_gauss_lobatto_against_dsyev():
     """Lobatto interior nodes = eigenvalues of the cldvr.cpp:82-139 Jacobi matrix."""
     from td1c_b200.basis import lobatto
