@@ -24,6 +24,13 @@
  *   lfield    : lfield(1:3, 1:3) column-major (gauge field, E, A)
  * Errors: the void drop-in calls record a status readable with
  * td1c_gpu_last_status() (0 = ok); the td1c_gpu_* calls return it directly.
+ * Status bits: 1 Poisson band factor not positive definite, 2 Jacobi
+ * eigensolver not converged, 4 non-finite value in an output (hprod_htot_'s
+ * hwfn, hcic and energies; the state at the end of every propagation call),
+ * 8 CUDA call failed, 16 unsupported configuration, 32 a bounded device
+ * wait ran out, 64 singular one-body factor.  The reference stops the
+ * program in these cases (e.g. src/hprod/hprod_mkv2mf.F90:167-170,
+ * src/bas/bas_gen_d2ll.F90:120-123).
  */
 #ifndef TD1C_B200_H
 #define TD1C_B200_H
@@ -60,6 +67,13 @@ int td1c_gpu_bind_sph(int lmax1, int lmax2, int mmax1, int mmax2, int nlat,
  * frozen, dynamic core, active.  lval is the nominal l of each orbital. */
 int td1c_gpu_bind_bas(double znuc, int smul, int mtot, int nfun, const int* otype,
                       const int* mval, const int* lval, int nela, int nelb);
+
+/* ormas_bind_'s subspace count nsub (src/ormas/ormas_bind.F90:2-75).  Only
+ * CAS (nsub = 1) is supported: other values are recorded and hprod_init_
+ * then fails with ST_CONFIG (16), where the reference would run the
+ * active-active rotation solve of ormas_xact2 (src/ormas/ormas_xact2.F90:
+ * 46,82).  Returns 16 for nsub != 1.  Default 1. */
+int td1c_gpu_bind_ormas(int nsub);
 
 /* control_bind_ (src/control/control_bind.F90:2-61): icomp 1 real time,
  * 0 imaginary time; igauge 0 length, 1 velocity. */
@@ -123,6 +137,26 @@ int td1c_gpu_htot_dev(double dtime, const double* lfield, const void* d_wfn, con
 /* Copy a named device intermediate of the last htot to host memory
  * (complex arrays as interleaved doubles); returns doubles copied or -1. */
 long td1c_gpu_debug_get(const char* name, double* out, long capacity);
+
+/* Device address of a named buffer of the context: "W" (pair potentials on
+ * the grid, [pair][nlat][Nr] complex), "int2e" ([nact^4] complex), "rho2",
+ * "v2sph" ([pair][lmax2+1][Nr] complex); NULL for other names. */
+void* td1c_gpu_debug_ptr(const char* name);
+/* Queue a device copy of a named buffer (names as above) to (to_ctx = 0) or
+ * from (to_ctx = 1) the device buffer d_other on the library stream; returns
+ * the bytes copied or -1. */
+long td1c_gpu_debug_xfer(const char* name, void* d_other, int to_ctx);
+/* on = 1: every following RHS takes the pair potentials W and int2e as they
+ * stand in the context instead of forming them from the stage's orbitals
+ * (no pair densities, Poisson solve, l -> theta transform or int2e); the
+ * rest of hprod_htot (src/hprod/hprod_htot.F90:44-208) is unchanged.  This
+ * is the stage RHS of the learned form, whose predictor writes W and int2e;
+ * 0 restores the full RHS. */
+int td1c_gpu_set_mf_external(int on);
+/* lfield(3,3) (9 doubles, host) of the sin^2 pulse at time t in the bound
+ * gauge, as the propagators stage it (clfield1 velocity1 / length1,
+ * src/field/clfield1.cpp:253-300,472-500,573-620). */
+int td1c_gpu_pulse_lfield(double t, double fint, double wlen, double numcyc, double cep, double* out9);
 
 /* Length-form dipole <z> of a device-resident state, written to *out (host):
  * dip(1) of hprod_dipole (src/hprod/hprod_dipole.F90:2-70), i.e.
@@ -211,6 +245,14 @@ int td1c_gpu_relax_etdrk2(void* d_wfn, void* d_cic, double dt, int ncyc, int max
  * (NULL, NULL to switch off): each step then performs the complete update on
  * the same input, for throughput measurement of a fixed synthetic state. */
 int td1c_gpu_rk4_reset(const void* d_wfn0, const void* d_cic0);
+/* Self-test of the bounded wait that every staged kernel uses on its
+ * mbarriers (a copy or tensor-core commit that never completes): one kernel
+ * waits on a barrier that nothing arrives on, gives up after the bound (1 s)
+ * and records ST_TIMEOUT in a word of its own (not the context's status).
+ * Returns the bits that word holds, ST_TIMEOUT (32) when the bound works;
+ * no copy or MMA is in flight, and the context stays usable.  No counterpart
+ * in the reference, which has no device waits. */
+int td1c_gpu_wait_selftest(void);
 /* Synchronise the library stream. */
 int td1c_gpu_sync(void);
 /* Number of kernel launches issued by the last td1c_gpu_rk4 call. */
@@ -247,15 +289,24 @@ int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d
  *   stream      cudaStream_t the work is queued on (NULL: legacy stream)
  *
  * Scratch (block tables and split-K partial sums) lives in one 8 MiB device
- * array built into the library, held by every GPU that loads it until the
- * process exits.  All calls on a device share that array, and it keeps the
- * last call's contents: calls whose GPU work overlaps (different streams or
- * unordered host threads) race and give wrong results.  The first call on
- * each device looks up the array's device address (with that device
- * current); make that first call before any stream capture.  Returns 0 on
- * success, 16 with a message on stderr when a size exceeds these limits or
- * an argument is null, 8 when a CUDA call fails.  The work is asynchronous
- * on the stream. */
+ * array built into the library.  The call uses the current device and its
+ * primary context: make it with the device that owns d_rho2, d_v2sph and
+ * d_int2e current.  The array is reserved when CUDA loads this file's
+ * module on a device: at the first call on that device under CUDA's default
+ * lazy module loading (CUDA_MODULE_LOADING=EAGER reserves it when the
+ * library is loaded), after which the device holds it until the process
+ * exits.  So make the first call on each device during set-up, before a
+ * pool allocator takes the device's memory and before any stream capture;
+ * that first call also looks up the array's device address, which later
+ * calls reuse (after cudaDeviceReset on that device, do not call it again
+ * in the same process).  All calls on a device share the array, and it
+ * keeps the last call's contents: calls whose GPU work overlaps (different
+ * streams or unordered host threads) race and give wrong results, and so do
+ * replays of a CUDA graph that holds the call, whichever graph or stream
+ * they run on: order every direct call and replay like calls on one stream.
+ * Returns 0 on success, 16 with a message on stderr when a size exceeds
+ * these limits or an argument is null, 8 when a CUDA call fails.  The work
+ * is asynchronous on the stream. */
 int td1c_gpu_int2e_static(int nact, const int* mval, long K, const double* d_rho2, const double* d_v2sph,
                           double* d_int2e, void* stream);
 

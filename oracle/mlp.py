@@ -15,6 +15,10 @@ Nothing in the product imports this module.
 """
 import numpy as np
 
+# Lagrange weights of the cubic through the step offsets tau = 0, -1, -2, -3 (latest history value
+# first), evaluated at tau = c: the extrapolation the predictor's weights start from
+CUBIC = {1.0: np.array([4.0, -6.0, 4.0, -1.0]), 0.5: np.array([2.1875, -2.1875, 1.3125, -0.3125])}
+
 
 def bf16_round(a):
     """Round float32 values to the nearest bfloat16 (ties to even), returned as float32."""

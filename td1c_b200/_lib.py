@@ -23,12 +23,28 @@ _lib = None
 
 
 def build(verbose=False):
-    """Compile every CUDA source into td1c_b200/_lib/libtd1c_b200.so."""
+    """Compile every CUDA source into td1c_b200/_lib/libtd1c_b200.so (one object per
+    source, compiled in parallel, then linked)."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [NVCC] + NVCC_FLAGS + ["-o", LIB_PATH] + [os.path.join(CSRC, s) for s in SOURCES]
+    obj_dir = os.path.join(LIB_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    objs, cmds = [], []
+    for s in SOURCES:
+        o = os.path.join(obj_dir, s.replace(".cu", ".o"))
+        objs.append(o)
+        cmds.append([NVCC] + compile_flags + ["-c", "-o", o, os.path.join(CSRC, s)])
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd, r in zip(cmds, ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            if verbose:
+                print(" ".join(cmd))
+            if r.returncode != 0:
+                raise RuntimeError("nvcc failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    link = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB_PATH] + objs
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return LIB_PATH
 
 
@@ -107,6 +123,18 @@ def load():
     lib.h1itr_prop_.argtypes = [ip, ip, ip, ip, dp, dp, ip, dp, ip, dp, dp]
     lib.dpade_gen_.argtypes = [ip, dp, dp, dp, ip]
     lib.dpade_prod_.argtypes = [ip, ip, ip, ip, dp, dp, dp, ip, dp, ip, dp, dp]
+    lib.td1c_gpu_debug_ptr.restype = vp
+    lib.td1c_gpu_debug_ptr.argtypes = [ctypes.c_char_p]
+    lib.td1c_gpu_debug_xfer.restype = c_long
+    lib.td1c_gpu_debug_xfer.argtypes = [ctypes.c_char_p, vp, c_int]
+    lib.td1c_gpu_set_mf_external.restype = c_int
+    lib.td1c_gpu_set_mf_external.argtypes = [c_int]
+    lib.td1c_gpu_bind_ormas.restype = c_int
+    lib.td1c_gpu_bind_ormas.argtypes = [c_int]
+    lib.td1c_gpu_wait_selftest.restype = c_int
+    lib.td1c_gpu_wait_selftest.argtypes = []
+    lib.td1c_gpu_pulse_lfield.restype = c_int
+    lib.td1c_gpu_pulse_lfield.argtypes = [c_double, c_double, c_double, c_double, c_double, dp]
     _lib = lib
     return lib
 
@@ -121,4 +149,6 @@ EXPORTED = [
     "td1c_gpu_orth", "td1c_gpu_relax", "td1c_gpu_bind_split", "td1c_gpu_h1itr", "td1c_gpu_dpade",
     "td1c_gpu_split2", "td1c_gpu_etdrk2", "td1c_gpu_etdrk4", "td1c_gpu_relax_etdrk2",
     "h1itr_gen_cninv_", "h1itr_prop_", "dpade_gen_", "dpade_prod_",
+    "td1c_gpu_debug_ptr", "td1c_gpu_debug_xfer", "td1c_gpu_set_mf_external", "td1c_gpu_pulse_lfield",
+    "td1c_gpu_bind_ormas", "td1c_gpu_wait_selftest",
 ]

@@ -32,6 +32,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "reductions.cuh"
+#include "tma.cuh"
 #include "../../include/td1c_b200.h"
 
 using namespace td1c;
@@ -78,6 +79,7 @@ struct Ctx {
   int icomp = 1, igauge = 0;
   int isplit = 0;  // split_type (clcontrol.cpp:98): one-body terms left out of the orbital RHS
   int nfcore = 0, ndcore = 0, nact = 0, ncore = 0, nelact = 0, neltot = 0;
+  int nsub = 1;  // ORMAS subspaces of the active space (ormas_bind_ nsub); 1 = CAS
   // ---- hprod_bind_ outputs
   double *p_ene_fcore = nullptr, *p_ene_dcore = nullptr, *p_ene_core = nullptr, *p_ene_act = nullptr, *p_ene_tot = nullptr;
   // ---- device tables
@@ -163,6 +165,7 @@ struct Ctx {
   // phase timing (off during graph capture)
   bool profile = false;
   int mixed = 0;  // 1: the mean field's pair-density and pair-potential transforms in split TF32 (tcgen05)
+  int mf_external = 0;  // 1: the RHS takes W and int2e as they stand (the learned form's predicted stages)
   cudaEvent_t ev[16] = {};
   cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1351,8 +1354,18 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   c.launches++;
   mark();  // end onebody (the stencil itself overlaps the next phases)
   bool i2_forked = false;
-  // mean field
-  if (c.neltot >= 2 && c.npair > 0) {
+  // mean field: computed from the stage's own orbitals, or (mf_external) taken
+  // as it stands in W and int2e, where the mean-field predictor of the
+  // learned form has written its stage values
+  if (c.neltot >= 2 && c.npair > 0 && c.mf_external) {
+    mark(); mark();  // no rho_gemm, no poisson
+    mark();          // no w_gemm
+    join();
+    rc |= chk("mfprod", launch_mfprod(c.mf, st));
+    c.launches += 2;
+    mark();  // end mfprod
+    rc |= chk("gorb gemm", gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false));
+  } else if (c.neltot >= 2 && c.npair > 0) {
     rc |= chk("rho gemm", gemm_mf(c, c.b_rho, c.npair, c.L2, c.nlat, true));
     mark();  // end rho_gemm
     rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
@@ -1392,10 +1405,13 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   if (i2_forked) {
     cudaStreamWaitEvent(st, c.ev_i2_join, 0);
   } else if (c.nact > 0) {
-    if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
-    else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
+    if (!c.mf_external || c.npair == 0) {
+      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
+      else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
+      c.launches += 3;
+    }
     rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, st));  // the CI chain joined before mfprod
-    c.launches += 4;
+    c.launches += 1;
   }
   mark();  // end int2e (its wait for the third stream)
   SmallArgs sa{};
@@ -1490,6 +1506,35 @@ __global__ void zaxpby_kernel(size_t n, cplx* z, const cplx* x, const cplx* y, c
   z[t] = cadd(cmul(a, x[t]), cmul(b, y[t]));
 }
 __global__ void counter_inc_kernel(int* counter) { if (threadIdx.x == 0) *counter += 1; }
+
+// ST_NONFINITE in *status when any of the n doubles is not finite (the output
+// check of the drop-in RHS and of every propagation call)
+__global__ void nonfinite_kernel(const double* __restrict__ a, size_t n, int* __restrict__ status) {
+  bool bad = false;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(a[i])) bad = true;
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, ST_NONFINITE);
+}
+void check_finite(Ctx& c, const void* p, size_t ndouble, cudaStream_t st) {
+  if (!ndouble) return;
+  const unsigned grid = (unsigned)std::min<size_t>((ndouble + 255) / 256, 148 * 4);
+  nonfinite_kernel<<<grid, 256, 0, st>>>((const double*)p, ndouble, c.d_status);
+  c.launches++;
+}
+
+// The bounded wait of the staged kernels (mbar_wait: an mbarrier phase, given
+// up after TMA_WAIT_NS) on a barrier that nothing arrives on: the wait runs
+// out and the kernel records ST_TIMEOUT, as the kernels do when a copy or an
+// MMA commit never completes.  No copy or MMA is in flight.
+__global__ void wait_selftest_kernel(int* __restrict__ status) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0)) atomicOr(status, ST_TIMEOUT);
+}
 
 // sin^2 pulse (clfield1.cpp:15-115 set-up, 253-300 E explicit, 472-500
 // A explicit, 573-620 E as the 6-point derivative of A in velocity1)
@@ -2035,7 +2080,7 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
     int s0 = 0;
     cudaGraphExec_t& ge = c.graph_exec[kind];
     bool cached;
-    const int ctl = c.icomp * 2 + c.igauge + 4 * c.mixed;
+    const int ctl = c.icomp * 2 + c.igauge + 4 * c.mixed + 8 * c.mf_external;
     if (kind == 0) {
       cached = ge && b.g_y == y && b.g_yc == yc && b.g_tab == c.field_tab && b.g_dt == dt && b.g_ro == b.reset_orb &&
                b.g_ctl == ctl;
@@ -2074,6 +2119,8 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
       c.launches += per_step;
     }
   }
+  check_finite(c, y, 2 * no, st);
+  check_finite(c, yc, 2 * nc, st);
   rc |= (int)cudaGetLastError();
   return rc ? ST_CUDA : 0;
 }
@@ -2128,6 +2175,12 @@ int td1c_gpu_bind_bas(double znuc, int smul, int mtot, int nfun, const int* otyp
   return 0;
 }
 
+int td1c_gpu_bind_ormas(int nsub) {
+  Ctx& c = ctx();
+  c.nsub = nsub;
+  return nsub == 1 ? 0 : ST_CONFIG;
+}
+
 int td1c_gpu_bind_control(int icomp, int igauge) {
   Ctx& c = ctx();
   c.icomp = icomp; c.igauge = igauge;
@@ -2151,6 +2204,9 @@ void hprod_init_(void) {
   Ctx& c = ctx();
   if (!c.have_rad || !c.have_sph || !c.have_bas) { c.status |= ST_CONFIG; return; }
   if (c.nfun > 16) { c.status |= ST_CONFIG; return; }
+  // the active-active rotations of ORMAS with several subspaces
+  // (ormas_xact2.F90:46,82) are not built: only CAS (nsub = 1) is accepted
+  if (c.nsub != 1) { c.status |= ST_CONFIG; return; }
   // one library stream for the process lifetime: callers may hold it
   // (td1c_gpu_stream) beyond hprod_final_
   static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr, lib_stream3 = nullptr, lib_stream4 = nullptr;
@@ -2240,6 +2296,12 @@ void hprod_htot_(const double* dtime, const double* lfield, const double* wfn, c
   cudaMemcpyAsync(c.wfn_io, wfn, so * sizeof(cplx), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(c.cic_io, cic, c.lcic * sizeof(cplx), cudaMemcpyHostToDevice, st);
   int rc = run_htot(c, c.lfield, c.wfn_io, c.cic_io, c.hwfn_io, c.hcic_io, *dtime);
+  // the reference stops on a failed solve (hprod_mkv2mf.F90:167-170); here a
+  // non-finite output (a NaN in the input, a diverged state) is reported in
+  // the status word instead
+  check_finite(c, c.hwfn_io, 2 * so, st);
+  check_finite(c, c.hcic_io, 2 * (size_t)c.lcic, st);
+  check_finite(c, c.ene, 5, st);
   cudaMemcpyAsync(hwfn, c.hwfn_io, so * sizeof(cplx), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(hcic, c.hcic_io, c.lcic * sizeof(cplx), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(c.h_ene, c.ene, 5 * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -2789,10 +2851,74 @@ int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d
   return rc ? -ST_CUDA : kNumPhases;
 }
 
+int td1c_gpu_wait_selftest(void) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  static int* d_word = nullptr;
+  if (!d_word && cudaMalloc(&d_word, sizeof(int)) != cudaSuccess) return ST_CUDA;
+  int word = 0;
+  cudaMemsetAsync(d_word, 0, sizeof(int), c.st);
+  wait_selftest_kernel<<<1, 32, 0, c.st>>>(d_word);
+  cudaMemcpyAsync(&word, d_word, sizeof(int), cudaMemcpyDeviceToHost, c.st);
+  if (cudaStreamSynchronize(c.st) != cudaSuccess) return ST_CUDA;
+  return word;
+}
+
 int td1c_gpu_sync(void) {
   Ctx& c = ctx();
   cudaError_t e = cudaStreamSynchronize(c.st);
   return e == cudaSuccess ? 0 : (int)e;
+}
+
+// device address of a named buffer of the context (for callers that stage
+// their own mean field with td1c_gpu_set_mf_external), or NULL
+void* td1c_gpu_debug_ptr(const char* name) {
+  Ctx& c = ctx();
+  std::string n(name);
+  if (n == "W") return c.W;
+  if (n == "int2e") return c.int2e;
+  if (n == "rho2") return c.rho2;
+  if (n == "v2sph") return c.v2sph;
+  return nullptr;
+}
+
+// copy a named buffer of the context to (to_ctx = 0) or from (to_ctx = 1) the
+// device buffer d_other, queued on the library stream; returns the bytes or -1
+long td1c_gpu_debug_xfer(const char* name, void* d_other, int to_ctx) {
+  Ctx& c = ctx();
+  std::string n(name);
+  void* p = nullptr;
+  size_t bytes = 0;
+  if (n == "W") { p = c.W; bytes = c.ngrid * c.npair * sizeof(cplx); }
+  else if (n == "int2e") { p = c.int2e; bytes = (size_t)c.nact * c.nact * c.nact * c.nact * sizeof(cplx); }
+  else if (n == "rho2") { p = c.rho2; bytes = c.nbas2 * c.npair * sizeof(cplx); }
+  else if (n == "v2sph") { p = c.v2sph; bytes = c.nbas2 * c.npair * sizeof(cplx); }
+  else return -1;
+  if (!d_other || !p) return -1;
+  if (cudaMemcpyAsync(to_ctx ? p : d_other, to_ctx ? d_other : p, bytes, cudaMemcpyDeviceToDevice, c.st) != cudaSuccess)
+    return -1;
+  return (long)bytes;
+}
+
+// on = 1: every following RHS skips the pair densities, the Poisson solve, the
+// l -> theta transform of the pair potentials and int2e, and uses W and int2e
+// as they stand in the context's buffers; 0 restores the full RHS
+int td1c_gpu_set_mf_external(int on) {
+  Ctx& c = ctx();
+  if (!c.initialized) return ST_CONFIG;
+  c.mf_external = on ? 1 : 0;
+  return 0;
+}
+
+// lfield(3,3) of the sin^2 pulse at time t in the bound gauge, as the
+// propagators stage it (clfield1 velocity1 / length1)
+int td1c_gpu_pulse_lfield(double t, double fint, double wlen, double numcyc, double cep, double* out9) {
+  Ctx& c = ctx();
+  Pulse p;
+  p.famp = std::sqrt(fint / 3.50944506E+16); p.freq = 1239.84190 / (wlen * 27.2113845);
+  p.period = 2 * PI / p.freq; p.numcyc = numcyc; p.cep = cep / 180.0 * PI; p.igauge = c.igauge;
+  pulse_lfield(p, t, out9);
+  return 0;
 }
 
 long td1c_gpu_debug_get(const char* name, double* out, long cap) {

@@ -58,6 +58,7 @@ class HProd:
         self._keep += [ot, mv, lv]
         self._check(lib.td1c_gpu_bind_bas(float(wl["znuc"]), int(wl.get("smul", 1)), int(wl.get("mtot", 0)),
                                           self.nfun, _ip(ot), _ip(mv), _ip(lv), int(wl["nela"]), int(wl["nelb"])))
+        self._check(lib.td1c_gpu_bind_ormas(int(wl.get("nsub", 1))))
         self._check(lib.td1c_gpu_bind_control(int(wl.get("icomp", 1)), int(wl["igauge"])))
         self._check(lib.td1c_gpu_bind_split(int(wl.get("split_type", 0))))
         self.ene = np.zeros(8)
@@ -284,6 +285,41 @@ class HProd:
         if n <= 0 or n > 16:
             raise StatusError("td1c_gpu_profile failed (%d)" % n)
         return dict(zip(names.value.decode().split(","), ms[:n].tolist()))
+
+    def debug_ptr(self, name):
+        """Device address of a named context buffer ("W", "int2e", "rho2", "v2sph")."""
+        p = self.lib.td1c_gpu_debug_ptr(name.encode())
+        if not p:
+            raise KeyError(name)
+        return int(p)
+
+    def debug_xfer(self, name, d_other, to_ctx):
+        """Queue a device copy of a named context buffer to (to_ctx=False) or from (to_ctx=True) the
+        device buffer d_other on the library stream; returns the bytes copied."""
+        n = self.lib.td1c_gpu_debug_xfer(name.encode(), ctypes.c_void_p(d_other), 1 if to_ctx else 0)
+        if n < 0:
+            raise KeyError(name)
+        return n
+
+    def set_mf_external(self, on):
+        """on=True: later RHS evaluations take the pair potentials W and int2e as they stand in the
+        context (see debug_ptr) instead of computing them from the stage's orbitals."""
+        self._check(self.lib.td1c_gpu_set_mf_external(1 if on else 0))
+
+    def pulse_lfield(self, t):
+        """lfield(3,3) of the workload's sin^2 pulse at time t, as the propagators stage it."""
+        wl = self.wl
+        out = np.zeros(9)
+        self._check(self.lib.td1c_gpu_pulse_lfield(float(t), float(wl["fint"]), float(wl["wlen"]), float(wl["numcyc"]),
+                                                   float(wl.get("cep", 0.0)), _dp(out)))
+        return out
+
+    def wait_selftest(self):
+        """Status bits of the bounded-wait self-test (ST_TIMEOUT = 32 when the wait bound works)."""
+        return int(self.lib.td1c_gpu_wait_selftest())
+
+    def last_status(self):
+        return int(self.lib.td1c_gpu_last_status())
 
     def sync(self):
         self._check(self.lib.td1c_gpu_sync())

@@ -1,4 +1,4 @@
-"""CPU reference of the learned mean-field predictor (oracle/mlp.py, oracle/predictor_study.py).
+"""CPU reference of the learned mean-field predictor (oracle/mlp.py).
 
 The network's hand-written backward pass agrees with central differences,
 bfloat16 rounding is round-to-nearest-even, Adam fits a small map, the cubic
@@ -43,7 +43,7 @@ def test_adam_fits_a_small_map():
 
 
 def test_cubic_extrapolation_weights():
-    from oracle.predictor_study import CUBIC
+    from oracle.mlp import CUBIC
     p = np.poly1d([0.3, -1.2, 0.7, 2.0])
     hist = np.array([p(-k) for k in range(4)])
     for c, w in CUBIC.items():

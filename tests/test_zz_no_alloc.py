@@ -12,7 +12,8 @@ with its own allocated scratch (read back with td1c_gpu_debug_get). It does
 this on two calls in a row, so the second call meets the array as the first
 left it. The tolerance is 1e-10 relative, the parity tolerance of the other
 GPU tests. The output buffer is filled with NaN before each call, to show
-that the call writes every entry. The file is named to be collected last.
+that the call writes every entry, and checks that the second call leaves the
+device's free memory unchanged. The file is named to be collected last.
 """
 import ctypes
 
@@ -72,9 +73,14 @@ def test_int2e_static_matches_htot(cuda_ok, wl):
         for call in range(2):
             t_out.fill_(float("nan"))
             torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info(dev)[0]
             rc = _run(lib, nact, mval, K, t_rho.data_ptr(), t_v2.data_ptr(), t_out.data_ptr(), stream)
             assert rc == 0, (call, rc)
             torch.cuda.synchronize()
+            if call == 1:
+                # the first call may have had CUDA load the module (and with it the array); the
+                # second reserves nothing: the device's free memory is unchanged
+                assert torch.cuda.mem_get_info(dev)[0] == free0
             got = t_out.cpu().numpy().view(np.complex128)
             assert np.isfinite(got).all(), call
             assert rel_err(got, ref) < TOL, (call, rel_err(got, ref))
