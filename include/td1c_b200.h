@@ -179,7 +179,9 @@ int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield,
  * runs the mean field's pair-density multipoles (bas_ang2sph2.F90:330-482)
  * and pair potentials on the grid (bas_sph2ang2.F90:334-463) in split TF32
  * on the tensor cores with FP32 accumulation, FP64 everywhere else; 0 restores
- * the plain FP64 path.  Every later RHS and step uses the mode. */
+ * the plain FP64 path.  Every later RHS and step uses the mode.  on = 2 is the
+ * same arithmetic on the per-tile split-TF32 kernel instead of the persistent
+ * one (for comparisons); other values return 16. */
 int td1c_gpu_set_mixed(int on);
 /* Deviation of the mixed form from FP64 on one RHS of a device state:
  * out[0..2] = max |delta| / max |FP64 value| of the pair-density multipoles,

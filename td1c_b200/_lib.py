@@ -14,7 +14,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtd1c_b200.so")
 SOURCES = ["hprod.cu", "legendre_gemm.cu", "onebody.cu", "poisson.cu", "mfprod.cu", "reductions.cu", "ci.cu",
            "int2e_static.cu", "int2e_dmma.cu", "observables.cu", "h1prop.cu", "poisson_cond.cu",
-           "legendre_tf32.cu"]
+           "legendre_tf32.cu", "legendre_tc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]

@@ -37,6 +37,12 @@
 
 using namespace td1c;
 
+namespace td1c {
+int legendre_tc_plan(const std::vector<LegGemmBatch>& h_batches, const LegGemmBatch* d_batches, int M, int K, int N, bool pair,
+                     const double* slab_base, int slab_count, int nsm, LegTcPlan* out, std::vector<void*>& allocs,
+                     cudaStream_t st);
+}
+
 namespace {
 
 const double PI = 3.14159265358979323846264338327950288;
@@ -165,6 +171,10 @@ struct Ctx {
   // phase timing (off during graph capture)
   bool profile = false;
   int mixed = 0;  // 1: the mean field's pair-density and pair-potential transforms in split TF32 (tcgen05)
+  // persistent split-TF32 plans of the two pair-field transforms (built on the first switch to mixed)
+  std::vector<LegGemmBatch> h_b_rho, h_b_W;
+  LegTcPlan tc_rho, tc_W;
+  bool tc_built = false, tc_ok_rho = false, tc_ok_W = false;
   int mf_external = 0;  // 1: the RHS takes W and int2e as they stand (the learned form's predicted stages)
   cudaEvent_t ev[16] = {};
   cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
@@ -852,7 +862,7 @@ int build_batches(Ctx& c) {
     v.push_back({lb2(c.mval[b] - c.mval[a]), (const double*)(c.orbg + a * c.ngrid), (const double*)(c.orbg + b * c.ngrid),
                  (double*)(c.rho2 + (size_t)p * c.nbas2), N, N, ldn, 0});
   }
-  batch_upload(c.b_rho, v); v.clear();
+  batch_upload(c.b_rho, v); c.h_b_rho = v; v.clear();
   for (int p = c.npair; p < c.npair_all; ++p) {
     int a = c.pa[p], b = c.pb[p];
     v.push_back({lb2(c.mval[b] - c.mval[a]), (const double*)(c.orbg + a * c.ngrid), (const double*)(c.orbg + b * c.ngrid),
@@ -868,6 +878,7 @@ int build_batches(Ctx& c) {
   {
     std::vector<LegGemmBatch> v1(v.begin(), v.begin() + c.npair), v2(v.begin() + c.npair, v.end());
     batch_upload(c.b_W, v1); batch_upload(c.b_W_fcfc, v2);
+    c.h_b_W = v1;
   }
   v.clear();
   // ang2sph1 of g and v2 for dynamic orbitals (M = L1, K = nlat)
@@ -1279,7 +1290,26 @@ int gemm(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
 int gemm_mf(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
   if (!c.mixed) return gemm(c, b, nb, M, K, pair);
   c.launches++;
+  if (c.mixed == 1 && b == c.b_rho && c.tc_ok_rho) return launch_legendre_tc(c.tc_rho, c.d_status, c.st);
+  if (c.mixed == 1 && b == c.b_W && c.tc_ok_W) return launch_legendre_tc(c.tc_W, c.d_status, c.st);
   return launch_legendre_gemm_tf32(b, nb, M, K, 2 * c.Nr, pair, c.d_status, c.st);
+}
+
+// the persistent split-TF32 plans of the pair-density (theta -> l) and
+// pair-potential (l -> theta) transforms; shapes outside the persistent
+// kernel's range keep the per-tile split-TF32 kernel
+void build_tc_plans(Ctx& c) {
+  if (c.tc_built) return;
+  c.tc_built = true;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (c.npair > 0 && !c.h_b_rho.empty())
+    c.tc_ok_rho = legendre_tc_plan(c.h_b_rho, c.b_rho, c.L2, c.nlat, 2 * c.Nr, true, (const double*)c.orbg, c.nfun, nsm, &c.tc_rho,
+                                   g_allocs, c.st) == 0;
+  if (c.npair > 0 && !c.h_b_W.empty())
+    c.tc_ok_W = legendre_tc_plan(c.h_b_W, c.b_W, c.nlat, c.L2, 2 * c.Nr, false, (const double*)c.v2sph, c.npair_all, nsm,
+                                 &c.tc_W, g_allocs, c.st) == 0;
 }
 
 // report the first failing launcher of an RHS (status ST_CUDA is set by the caller)
@@ -2776,7 +2806,9 @@ void* td1c_gpu_stream(void) { return g ? (void*)g->st : nullptr; }
 int td1c_gpu_set_mixed(int on) {
   Ctx& c = ctx();
   if (!c.initialized) return ST_CONFIG;
-  c.mixed = on ? 1 : 0;
+  if (on < 0 || on > 2) return ST_CONFIG;
+  c.mixed = on;
+  if (c.mixed) build_tc_plans(c);
   return 0;
 }
 
@@ -2793,9 +2825,10 @@ int td1c_gpu_mixed_selftest(const void* d_wfn, const void* d_cic, const double* 
   const size_t nr = c.nbas2 * c.npair, nw = c.ngrid * c.npair, nh = c.nbas * c.nfun;
   std::vector<std::complex<double>> r[2], w[2], h[2];
   const int keep = c.mixed;
+  build_tc_plans(c);
   int rc = 0;
   for (int mode = 0; mode < 2; ++mode) {
-    c.mixed = mode;
+    c.mixed = mode ? std::max(keep, 1) : 0;
     rc |= run_htot(c, c.dip_lfd, (const cplx*)d_wfn, (const cplx*)d_cic, c.hwfn_io, c.hcic_io, 1.0);
     r[mode].resize(nr); w[mode].resize(nw); h[mode].resize(nh);
     cudaMemcpyAsync(r[mode].data(), c.rho2, nr * sizeof(cplx), cudaMemcpyDeviceToHost, st);

@@ -33,6 +33,39 @@ int launch_legendre_gemm(const LegGemmBatch* d_batches, int nbatch, int M, int K
 int launch_legendre_gemm_tf32(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair, int* status,
                               cudaStream_t st);
 
+// the same transform in split TF32 as a persistent warp-specialised kernel
+// (legendre_tc.cu): tables split once at set-up and resident per CTA, a ring
+// of staged slab chunks, two TMEM accumulators; for M <= 128
+struct LegTcArgs {
+  const LegGemmBatch* batches;
+  const int* order;        // batch of each group-ordered batch slot
+  const int4* work;        // per CTA: (table, first tile, end tile, -)
+  const uint32_t* tables;  // per table: hi then lo plane, np x kp each, tensor-core layout
+  const int2* zc;          // per batch: tensor-map slab index of B0 and B1
+  int* status;
+  int M, K, N, np, kp, ntn, stages, raw_slots, tmem_cols;
+};
+struct LegTcPlan {
+  CUtensorMap tmap;        // the slab array (3-d: N doubles x K rows x slabs), boxes of 128 x 16
+  LegTcArgs args{};
+  int ncta = 0, smem = 0;
+  bool pair = false;
+};
+int launch_legendre_tc(const LegTcPlan& p, int* status, cudaStream_t st);
+
+// ---- the learned predictor's network (mlp.cu)
+constexpr int MLP_MAXDEPTH = 8;
+struct MlpInferArgs {
+  int depth, rows, nin, ldx, ldy;
+  const float* x;
+  float* y;
+  int* status;
+  int n[MLP_MAXDEPTH], np[MLP_MAXDEPTH], kp[MLP_MAXDEPTH];  // width, padded width, padded depth of each layer
+  const float* b[MLP_MAXDEPTH];
+  const unsigned short* wbf16[MLP_MAXDEPTH];  // BF16 weight planes (tensor-core layout)
+};
+int launch_mlp_infer_bf16(const MlpInferArgs& a, cudaStream_t st);
+
 // ---- one-body: tprod + zprod/pzprod (hprod_tprod.F90, hprod_zprod.F90, hprod_pzprod.F90)
 struct OneBodyArgs {
   int Nr, L1, nd, nfun, nfcore, mmax1, igauge;

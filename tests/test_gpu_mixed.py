@@ -77,3 +77,47 @@ def test_mixed_trajectory_dipole_and_norm(cuda_ok):
         assert h.lib.td1c_gpu_last_status() == 0
     finally:
         h.final()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.NE_SMALL, W.MIXED_SMALL, W.NE_CAS], ids=lambda w: w["name"])
+def test_persistent_and_per_tile_kernels_agree(cuda_ok, base):
+    """The persistent split-TF32 kernel (mode 1) and the per-tile one (mode 2) give the same
+    pair-density multipoles and pair potentials to FP32 rounding, both within 2e-6 of FP64; on the
+    full-size Ne configuration as well (the persistent kernel's tables resident per CTA)."""
+    import torch
+    from td1c_b200 import basis
+    from td1c_b200.hprod import HProd
+    from td1c_b200.wfn import seeded_orbitals, seeded_cic
+    from .helpers import rel_err
+    if base is W.NE_CAS:
+        wl = dict(base, split_type=1)
+        rad, ang = basis.build(wl)
+        h = HProd(wl, rad, ang)
+        tb = h.ci_tables()
+        orb = seeded_orbitals(wl, rad["xrad"], rad["wrad"], rad["mask"])
+        cic = seeded_cic(wl, h.dims["lcic"], tb["stra"], tb["strb"], tb["detoff"], tb["afirst"], tb["acount"])
+        h.set_wfn0(orb, cic)
+        lf = h.pulse_lfield(100.0)
+    else:
+        o, h, wl, orb, cic = _setup(base)
+        lf = o.field(30.0)
+    try:
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        d_hw, d_hc = torch.empty_like(d_orb), torch.empty_like(d_cic)
+        out = {}
+        for mode in (0, 1, 2):
+            h.set_mixed(mode)
+            h.htot_dev(1.0, lf, d_orb.data_ptr(), d_cic.data_ptr(), d_hw.data_ptr(), d_hc.data_ptr())
+            h.sync()
+            out[mode] = (h.debug("rho2"), h.debug("W"), d_hw.cpu().numpy())
+        h.set_mixed(False)
+        for mode in (1, 2):
+            assert rel_err(out[mode][0], out[0][0]) < 2e-6, (mode, rel_err(out[mode][0], out[0][0]))
+            assert rel_err(out[mode][1], out[0][1]) < 2e-6, (mode, rel_err(out[mode][1], out[0][1]))
+            assert rel_err(out[mode][2], out[0][2]) < 1e-5
+        assert rel_err(out[1][0], out[2][0]) < 1e-6 and rel_err(out[1][1], out[2][1]) < 1e-6
+        assert h.lib.td1c_gpu_last_status() == 0
+    finally:
+        h.final()
