@@ -312,6 +312,84 @@ int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d
 int td1c_gpu_int2e_static(int nact, const int* mval, long K, const double* d_rho2, const double* d_v2sph,
                           double* d_int2e, void* stream);
 
+/* ---- the learned form of the propagation -------------------------------
+ * No counterpart in the reference.  td1c_gpu_split2 (tdse_split2) with the
+ * mean field of the RK4 stages predicted instead of formed from the stage
+ * orbitals: once per step the exact pair potentials W and integrals int2e of
+ * the step's start state are formed (the pair densities, Poisson, the
+ * l -> theta transform) and kept in a history of five; the stages take
+ * W(c) at c = 0 (the exact value), 1/2 and 1 from it, per unit (a stored
+ * pair and one FEDVR element) with weights = the cubic extrapolation through
+ * the last four steps + a correction from the registered network.  The exact
+ * value of every step judges the previous step's prediction (relative error
+ * over all units); after a window of 8 predicted steps the window stands if
+ * its largest judge value is at most the bound, else the state returns to
+ * the window's start and the window is recomputed exactly, after which
+ * exact steps run for a back-off of 1, 3, 7, ... (at most 63) windows.
+ * Needs a context bound with split_type 1 (the RHS without h0 and laser). */
+/* Register the network (device pointers, FP32 weights as td1c_mlp_forward
+ * takes them, widths 32 .. 8; pack: td1c_mlp_pack_size bytes, the BF16
+ * copy the steps read: pack it with td1c_mlp_infer_bf16(repack = 1) after
+ * every weight update); use_net = 0 runs the cubic weights alone (the
+ * method without the network); depth = 0 unregisters.  bound: the judge's
+ * largest accepted relative error (1e-6 by default). */
+int td1c_gpu_set_learned(int depth, const int* sizes, const float* const* W, const float* const* b, void* pack, int use_net,
+                         double bound);
+/* learned split2 steps on device buffers (arguments as td1c_gpu_split2);
+ * stats (host, 10 doubles, may be NULL): windows accepted, rejected, exact
+ * (back-off), history fills; largest judge value of an accepted window;
+ * smallest and largest window judge value; predicted steps kept; the last
+ * window's judge value; steps run. */
+int td1c_gpu_split2_learned(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                            double cep, int maxcyc, double thresh, double* stats);
+/* exact split2 steps that write the predictor's training records into
+ * d_record (device, (nstep + 1) * nunit * 41 doubles): per step and unit the
+ * Gram matrix of the previous four history values (4 x 4 complex), their
+ * products with the new value (4 complex) and its squared norm; the first
+ * four steps' records precede a full history. */
+int td1c_gpu_learned_record(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                            double cep, int maxcyc, double thresh, double* d_record);
+/* out4 = units, FEDVR elements, stored pairs, doubles per record */
+int td1c_gpu_learned_dims(int* out4);
+/* the kind of each stored pair (0 diagonal, 1 off-diagonal, 2 with the frozen core) */
+int td1c_gpu_learned_pair_kind(int* out);
+/* network inputs (n x 32 floats) of training records (idx: record index of
+ * each sample, NULL: 0..n-1; unit = record index mod nu), computed as the
+ * steps compute them */
+int td1c_lp_features(int n, const double* rec, const int* idx, int nu, int nfe, const int* pair_kind, float* x, void* stream);
+/* relative squared error of each sample's prediction with weights cubic +
+ * out (n x 8: re, im of the four corrections) into loss[n] (FP64), and the
+ * gradient of their mean with respect to out into dy (NULL: none); use_net = 0
+ * evaluates the cubic alone */
+int td1c_lp_loss(int n, const double* rec, const int* idx, const float* out, float* dy, double* loss, int use_net, void* stream);
+
+/* ---- the learned mean-field predictor's network ------------------------
+ * No counterpart in the reference (td1c has no learned component).  A stack
+ * of depth linear layers with tanh between them, widths sizes[0] (input) ..
+ * sizes[depth] (output), depth <= 8; W[k], b[k] device pointers to layer
+ * k+1's FP32 weights [sizes[k+1] x sizes[k]] (row-major) and bias.  All
+ * buffers are device pointers; work is queued on stream (NULL: legacy).
+ * Return 0, 16 for bad arguments, 8 when a launch fails. */
+/* forward in FP32: acts receives every layer's output (sum_k rows * sizes[k]
+ * floats, k = 1..depth; the network output is the last block) */
+int td1c_mlp_forward(int depth, const int* sizes, const float* const* W, const float* const* b, const float* x, int rows,
+                     float* acts, void* stream);
+/* the hand-written backward pass for the output gradient dy [rows x
+ * sizes[depth]]: dW[k], db[k] overwritten; work: 2 * rows * max(sizes) floats */
+int td1c_mlp_backward(int depth, const int* sizes, const float* const* W, const float* x, int rows, const float* acts,
+                      const float* dy, float* const* dW, float* const* db, float* work, void* stream);
+/* one Adam step (Kingma and Ba) on n parameters; step = 1-based step count */
+int td1c_mlp_adam(long n, float* p, const float* g, float* m, float* v, float lr, float beta1, float beta2, float eps, int step,
+                  void* stream);
+/* BF16 inference on the tensor cores (tcgen05.mma kind::f16, FP32
+ * accumulation): widths <= 256; pack is a device buffer of
+ * td1c_mlp_pack_size bytes that holds the BF16 weights, rebuilt from W when
+ * repack != 0; y [rows x sizes[depth]] FP32; a bounded wait that runs out
+ * sets ST_TIMEOUT (32) in *status (device). */
+long td1c_mlp_pack_size(int depth, const int* sizes);
+int td1c_mlp_infer_bf16(int depth, const int* sizes, const float* const* W, const float* const* b, void* pack, int repack,
+                        const float* x, int rows, float* y, int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,7 +14,8 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtd1c_b200.so")
 SOURCES = ["hprod.cu", "legendre_gemm.cu", "onebody.cu", "poisson.cu", "mfprod.cu", "reductions.cu", "ci.cu",
            "int2e_static.cu", "int2e_dmma.cu", "observables.cu", "h1prop.cu", "poisson_cond.cu",
-           "legendre_tf32.cu", "legendre_tc.cu"]
+           "legendre_tf32.cu", "legendre_tc.cu", "mlp.cu",
+           "predictor.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -129,6 +130,34 @@ def load():
     lib.td1c_gpu_debug_xfer.argtypes = [ctypes.c_char_p, vp, c_int]
     lib.td1c_gpu_set_mf_external.restype = c_int
     lib.td1c_gpu_set_mf_external.argtypes = [c_int]
+    fpp = ctypes.POINTER(ctypes.c_void_p)
+    lib.td1c_mlp_forward.restype = c_int
+    lib.td1c_mlp_forward.argtypes = [c_int, ip, fpp, fpp, vp, c_int, vp, vp]
+    lib.td1c_mlp_backward.restype = c_int
+    lib.td1c_mlp_backward.argtypes = [c_int, ip, fpp, vp, c_int, vp, vp, fpp, fpp, vp, vp]
+    lib.td1c_mlp_adam.restype = c_int
+    lib.td1c_mlp_adam.argtypes = [c_long, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                  c_int, vp]
+    lib.td1c_mlp_pack_size.restype = c_long
+    lib.td1c_mlp_pack_size.argtypes = [c_int, ip]
+    lib.td1c_mlp_infer_bf16.restype = c_int
+    lib.td1c_mlp_infer_bf16.argtypes = [c_int, ip, fpp, fpp, vp, c_int, vp, c_int, vp, vp, vp]
+    lib.td1c_gpu_set_learned.restype = c_int
+    lib.td1c_gpu_set_learned.argtypes = [c_int, ip, fpp, fpp, vp, c_int, c_double]
+    lib.td1c_gpu_split2_learned.restype = c_int
+    lib.td1c_gpu_split2_learned.argtypes = [vp, vp, c_double, c_double, c_int, c_double, c_double, c_double, c_double, c_int,
+                                            c_double, dp]
+    lib.td1c_gpu_learned_record.restype = c_int
+    lib.td1c_gpu_learned_record.argtypes = [vp, vp, c_double, c_double, c_int, c_double, c_double, c_double, c_double, c_int,
+                                            c_double, vp]
+    lib.td1c_gpu_learned_dims.restype = c_int
+    lib.td1c_gpu_learned_dims.argtypes = [ip]
+    lib.td1c_gpu_learned_pair_kind.restype = c_int
+    lib.td1c_gpu_learned_pair_kind.argtypes = [ip]
+    lib.td1c_lp_features.restype = c_int
+    lib.td1c_lp_features.argtypes = [c_int, vp, vp, c_int, c_int, vp, vp, vp]
+    lib.td1c_lp_loss.restype = c_int
+    lib.td1c_lp_loss.argtypes = [c_int, vp, vp, vp, vp, vp, c_int, vp]
     lib.td1c_gpu_bind_ormas.restype = c_int
     lib.td1c_gpu_bind_ormas.argtypes = [c_int]
     lib.td1c_gpu_wait_selftest.restype = c_int
@@ -151,4 +180,7 @@ EXPORTED = [
     "h1itr_gen_cninv_", "h1itr_prop_", "dpade_gen_", "dpade_prod_",
     "td1c_gpu_debug_ptr", "td1c_gpu_debug_xfer", "td1c_gpu_set_mf_external", "td1c_gpu_pulse_lfield",
     "td1c_gpu_bind_ormas", "td1c_gpu_wait_selftest",
+    "td1c_mlp_forward", "td1c_mlp_backward", "td1c_mlp_adam", "td1c_mlp_pack_size", "td1c_mlp_infer_bf16",
+    "td1c_gpu_set_learned", "td1c_gpu_split2_learned", "td1c_gpu_learned_record", "td1c_gpu_learned_dims",
+    "td1c_gpu_learned_pair_kind", "td1c_lp_features", "td1c_lp_loss",
 ]

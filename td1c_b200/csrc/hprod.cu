@@ -176,6 +176,17 @@ struct Ctx {
   LegTcPlan tc_rho, tc_W;
   bool tc_built = false, tc_ok_rho = false, tc_ok_W = false;
   int mf_external = 0;  // 1: the RHS takes W and int2e as they stand (the learned form's predicted stages)
+  // learned form: predictor data path (predictor.cu), the caller's network, and the captured steps
+  LpArgs lp{};
+  bool lp_alloc = false;
+  MlpInferArgs lp_mi{};
+  bool lp_has_net = false;
+  float* lp_out = nullptr;
+  int* lp_mi_status = nullptr;
+  int lp_use_net = 0;
+  double lp_bound = 1e-6;
+  cplx* lp_save = nullptr;  // the state at the start of a judged window (orbitals, then CI)
+  cudaGraphExec_t lp_exec[3] = {nullptr, nullptr, nullptr};  // E, H, P steps (captured per call)
   cudaEvent_t ev[16] = {};
   cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -2048,6 +2059,139 @@ int etdrk4_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double 
   return rc;
 }
 
+// ---------------------------------------------------------------------------
+// the learned form: split2 with the stage mean fields predicted from the
+// history of exact step-start mean fields (predictor.cu)
+// ---------------------------------------------------------------------------
+int lp_setup(Ctx& c) {
+  if (c.lp_alloc) return 0;
+  if (c.npair < 1 || c.nfe < 1) return ST_CONFIG;
+  LpArgs& a = c.lp;
+  a.nfe = c.nfe; a.nd = c.nd; a.Nr = c.Nr; a.nlat = c.nlat; a.npair = c.npair; a.nu = c.npair * c.nfe;
+  a.ni = c.nact * c.nact * c.nact * c.nact;
+  a.nw = c.ngrid * c.npair;
+  a.W = c.W; a.int2e = c.int2e;
+  a.ring = dalloc<cplx>(5 * a.nw);
+  a.iring = dalloc<cplx>(5 * (size_t)std::max(a.ni, 1));
+  a.gram = dalloc<cplx>((size_t)a.nu * 16);
+  a.weights = dalloc<cplx>((size_t)a.nu * 4);
+  a.err = dalloc<double>(a.nu); a.tnorm = dalloc<double>(a.nu);
+  a.judge = dalloc<double>(2);
+  a.counter = dalloc<int>(1);
+  a.feat = dalloc<float>((size_t)a.nu * 32);
+  c.lp_out = dalloc<float>((size_t)a.nu * 8);
+  a.net_out = c.lp_out;
+  c.lp_mi_status = dalloc<int>(1);
+  std::vector<int> kind(c.npair);
+  for (int p = 0; p < c.npair; ++p) kind[p] = c.pb[p] < c.nfcore ? 2 : (c.pa[p] == c.pb[p] ? 0 : 1);
+  a.pair_kind = dupload(kind);
+  a.record = nullptr; a.rec_count = dalloc<int>(1);
+  c.lp_save = dalloc<cplx>(c.nbas * c.nfun + c.lcic);
+  if (!a.ring || !a.iring || !c.lp_save) return ST_CUDA;
+  c.lp_alloc = true;
+  return 0;
+}
+
+// the exact mean field (W, int2e) of the orbitals wfn: the orbital transform
+// with the frozen core's gauge phase of d_lf, the pair densities, Poisson,
+// the l -> theta transform and int2e (hprod_htot.F90:44-140's mean-field part)
+int run_meanfield(Ctx& c, const cplx* wfn, const double* d_lf) {
+  cudaStream_t st = c.st;
+  const size_t so = c.nbas * c.nfun;
+  int rc = 0;
+  cudaMemcpyAsync(c.orb + c.nfcore * c.nbas, wfn + c.nfcore * c.nbas, (so - c.nfcore * c.nbas) * sizeof(cplx),
+                  cudaMemcpyDeviceToDevice, st);
+  if (c.n_orbg) rc |= chk("orbg gemm", gemm(c, c.b_orbg, c.n_orbg, c.nlat, c.L1, false));
+  if (c.nfcore > 0) {
+    if (c.igauge == 0) {
+      cudaMemcpyAsync(c.orbg, c.orbg0, c.nfcore * c.ngrid * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+    } else {
+      size_t nfc = c.ngrid * c.nfcore;
+      fc_phase_kernel<<<(unsigned)((nfc + 255) / 256), 256, 0, st>>>(c.Nr, c.nlat, c.nfcore, c.xrad, c.cost, d_lf, c.orbg0, c.orbg);
+      c.launches++;
+    }
+  }
+  rc |= chk("rho gemm", gemm_mf(c, c.b_rho, c.npair, c.L2, c.nlat, true));
+  rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
+  c.launches += 3;
+  rc |= chk("W gemm", gemm_mf(c, c.b_W, c.npair, c.nlat, c.L2, false));
+  if (c.nact > 0) {
+    if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
+    else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
+    c.launches += 3;
+  }
+  return rc;
+}
+
+// J: exact mean field of the step-start state y, pushed into the history; the
+// judge of the last prediction; the network's weights for the next prediction
+int lp_j(Ctx& c, const cplx* y, const double* d_lf) {
+  cudaStream_t st = c.st;
+  int rc = run_meanfield(c, y, d_lf);
+  LpArgs a = c.lp;
+  a.use_net = c.lp_use_net && c.lp_has_net;
+  rc |= chk("lp push", launch_lp_push_judge(a, st));
+  c.launches += 3;
+  if (a.use_net) {
+    rc |= chk("lp features", launch_lp_features(a, st));
+    MlpInferArgs mi = c.lp_mi;
+    rc |= chk("lp network", launch_mlp_infer_bf16(mi, st));
+    c.launches += 2;
+  }
+  rc |= chk("lp weights", launch_lp_weights(a, st));
+  c.launches++;
+  return rc;
+}
+
+// RK4 of the two-body RHS with the predicted stage mean fields: stage 1 the
+// exact W_n, int2e_n (the last J), stages 2 and 3 the c = 1/2 values, stage 4
+// the c = 1 values
+int lp_rk4_pred(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, const double* lf) {
+  cudaStream_t st = c.st;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic;
+  RkBufs& b = g_rk;
+  const double wts[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+  const double anext[4] = {0.5, 0.5, 1.0, 0.0};
+  cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(b.y0 + no, y_cic, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+  int rc = 0;
+  c.mf_external = 1;
+  for (int is = 0; is < 4; ++is) {
+    if (is == 1 || is == 3) {
+      rc |= chk("lp stage", launch_lp_stage(c.lp, is == 1 ? 1 : 0, st));
+      c.launches += 2;
+    }
+    const cplx* in = (is == 0) ? b.y0 : b.yt;
+    rc |= run_htot(c, lf + 9 * is, in, in + no, b.k, b.k + no, 1.0);
+    const int nxt = is < 3 ? 1 : 0;
+    rk_combine_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(no, y_orb, b.y0, b.k, b.yt, dt * wts[is], dt * anext[is], nxt);
+    rk_combine_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(nc, y_cic, b.y0 + no, b.k + no, b.yt + no, dt * wts[is],
+                                                                  dt * anext[is], nxt);
+    c.launches += 2;
+  }
+  c.mf_external = 0;
+  return rc;
+}
+
+// the three step kinds of the learned driver: E plain split2; H split2 then J
+// of the new state; P split2 with predicted stage mean fields, then J
+int lp_step(Ctx& c, int kind, cplx* y, cplx* yc, double dt, int maxcyc, double thresh) {
+  if (kind == 0) return split2_step(c, y, yc, dt, maxcyc, thresh, true);
+  int rc = 0;
+  if (kind == 1) {
+    rc |= split2_step(c, y, yc, dt, maxcyc, thresh, true);
+  } else {
+    step_begin(c, y, yc, 54);
+    const double* lf = g_rk.lf_cur;
+    rc |= h1_apply(c, false, lf + 36, y, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
+    rc |= lp_rk4_pred(c, y, yc, dt, lf);
+    rc |= h1_apply(c, false, lf + 45, y, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
+    rc |= step_end(c, y, true);
+  }
+  rc |= lp_j(c, y, g_rk.lf_cur + 27);  // the field at t + dt (the step's last stage field)
+  return rc;
+}
+
 // Propagation driver of td1c_gpu_rk4 / _split2 / _etdrk2 / _etdrk4 (kind 0 / 1 / 2 / 3):
 // stages the fields of every step, then runs the steps eagerly or as one
 // CUDA graph per step (captured after one eager step that does the first-call
@@ -2151,6 +2295,159 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
   }
   check_finite(c, y, 2 * no, st);
   check_finite(c, yc, 2 * nc, st);
+  rc |= (int)cudaGetLastError();
+  return rc ? ST_CUDA : 0;
+}
+
+// The learned split2 driver.  Windows of LP_WIN steps:
+//   FILL  the exact mean field of the window's start state, then exact steps
+//         that push the history (H), so predictions have four history values;
+//   TRY   predicted steps (P); every step's J judges the prediction the last
+//         one made; after the window the largest judge value decides: at or
+//         below the bound the window stands, above it the state goes back to
+//         the window's start and the window is recomputed with exact steps (H);
+//   PLAIN exact steps without history (E), the back-off after a rejection
+//         (1, 3, 7, ... up to 63 windows), followed by a FILL.
+// With record != null only exact steps run (J0 then H), and every J writes its
+// training records (nstep + 1 of them, the first four before the history is full).
+// stats (10 doubles): windows accepted, rejected, plain, fill; largest judge
+// value of an accepted window; smallest and largest window judge value seen;
+// predicted steps kept; last window judge value; steps run.
+constexpr int LP_WIN = 8;
+int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc, double cep,
+                int maxcyc, double thresh, double* record, double* stats) {
+  Ctx& c = ctx();
+  if (!c.initialized || c.isplit != 1 || c.npair < 1 || nstep < 0 || maxcyc < 0 || !(thresh >= 0.0)) return ST_CONFIG;
+  int rc = lp_setup(c);
+  if (rc) return rc;
+  cudaStream_t st = c.st;
+  const size_t no = c.nbas * c.nfun, nc = c.lcic;
+  RkBufs& b = g_rk;
+  if (b.cap < no + nc) {
+    b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc); b.k2 = dalloc<cplx>(no + nc);
+    if (!b.lf_cur) { b.lf_cur = dalloc<double>(54); b.counter = dalloc<int>(2); }
+    b.cap = no + nc;
+  }
+  b.reset_orb = nullptr; b.reset_cic = nullptr;
+  Pulse pl;
+  pl.famp = std::sqrt(fint / 3.50944506E+16); pl.freq = 1239.84190 / (wlen * 27.2113845);
+  pl.period = 2 * PI / pl.freq; pl.numcyc = numcyc; pl.cep = cep / 180.0 * PI; pl.igauge = c.igauge;
+  static const double nodes[6] = {0.0, 0.5, 0.5, 1.0, 0.25, 0.75};
+  const int per = 54;
+  std::vector<double> tab((size_t)std::max(nstep, 1) * per);
+  for (int s = 0; s < nstep; ++s)
+    for (int is = 0; is < 6; ++is) pulse_lfield(pl, t0 + dt * s + dt * nodes[is], &tab[(size_t)s * per + 9 * is]);
+  if ((size_t)c.field_cap < tab.size()) {
+    const size_t cap = std::max(tab.size(), (size_t)65536 * 54);
+    c.field_tab = dalloc<double>(cap);
+    c.field_cap = (long)cap;
+  }
+  cudaMemcpyAsync(c.field_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  auto set_step = [&](int s) {
+    b.h_counter[0] = s; b.h_counter[1] = nstep;
+    cudaMemcpyAsync(b.counter, b.h_counter, 2 * sizeof(int), cudaMemcpyHostToDevice, st);
+  };
+  set_step(0);
+  c.launches = 0;
+  cplx* y = (cplx*)d_wfn;
+  cplx* yc = (cplx*)d_cic;
+  c.lp.record = record;
+  cudaMemsetAsync(c.lp.rec_count, 0, sizeof(int), st);
+  cudaMemsetAsync(c.lp.gram, 0, (size_t)c.lp.nu * 16 * sizeof(cplx), st);
+  // J of the state at step s (the window's start state)
+  auto j0 = [&](int s) -> int {
+    double lf[9];
+    pulse_lfield(pl, t0 + dt * s, lf);
+    cudaMemcpyAsync(c.lfield, lf, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);  // lf lives on this frame
+    return lp_j(c, y, c.lfield);
+  };
+  // one step of the given kind: eager the first time in this call (factor
+  // set-up), then a graph captured in this call
+  for (auto& ge : c.lp_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  long per_launch[3] = {0, 0, 0};
+  bool warm[3] = {false, false, false};
+  auto step = [&](int kind) -> int {
+    cudaGraphExec_t& ge = c.lp_exec[kind];
+    if (!warm[kind]) {
+      warm[kind] = true;
+      return lp_step(c, kind, y, yc, dt, maxcyc, thresh);  // eager: first-call set-up happens here
+    }
+    if (!ge) {
+      const long l0 = c.launches;
+      cudaGraph_t graph;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
+      int r = lp_step(c, kind, y, yc, dt, maxcyc, thresh);
+      if (cudaStreamEndCapture(st, &graph) != cudaSuccess || r) return ST_CUDA;
+      if (cudaGraphInstantiate(&ge, graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
+      cudaGraphDestroy(graph);
+      per_launch[kind] = c.launches - l0;
+      c.launches = l0;
+    }
+    if (cudaGraphLaunch(ge, st) != cudaSuccess) return ST_CUDA;
+    c.launches += per_launch[kind];
+    return 0;
+  };
+  double stt[10] = {0, 0, 0, 0, 0, 1e300, 0, 0, 0, 0};
+  int s = 0;
+  if (record) {
+    rc |= j0(0);
+    for (; s < nstep && !rc; ++s) rc |= step(1);
+  } else {
+    int mode = 0;  // 0 FILL, 1 TRY, 2 PLAIN
+    int backoff = 0, plain_left = 0;
+    const bool can_predict = true;
+    while (s < nstep && !rc) {
+      const int w = std::min(LP_WIN, nstep - s);
+      if (mode == 0) {
+        rc |= j0(s);
+        for (int k = 0; k < w && !rc; ++k) rc |= step(1);
+        s += w;
+        stt[3] += 1;
+        mode = (w >= 4 && can_predict) ? 1 : 0;
+      } else if (mode == 1) {
+        cudaMemcpyAsync(c.lp_save, y, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(c.lp_save + no, yc, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+        cudaMemsetAsync(c.lp.judge, 0, 2 * sizeof(double), st);
+        for (int k = 0; k < w && !rc; ++k) rc |= step(2);
+        double jd[2] = {0, 0};
+        cudaMemcpyAsync(jd, c.lp.judge, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) { rc |= ST_CUDA; break; }
+        const double wj = jd[1];
+        stt[8] = wj;
+        stt[5] = std::min(stt[5], wj);
+        stt[6] = std::max(stt[6], wj);
+        if (wj <= c.lp_bound && std::isfinite(wj)) {
+          stt[0] += 1; stt[4] = std::max(stt[4], wj); stt[7] += w;
+          s += w;
+          backoff = 0;
+        } else {
+          // the window's predictions are rejected: back to its start, recompute it exactly
+          stt[1] += 1;
+          cudaMemcpyAsync(y, c.lp_save, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+          cudaMemcpyAsync(yc, c.lp_save + no, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+          set_step(s);
+          rc |= j0(s);
+          for (int k = 0; k < w && !rc; ++k) rc |= step(1);
+          s += w;
+          backoff = std::min(2 * backoff + 1, 63);
+          plain_left = backoff;
+          mode = 2;
+        }
+      } else {
+        for (int k = 0; k < w && !rc; ++k) rc |= step(0);
+        s += w;
+        stt[2] += 1;
+        if (--plain_left <= 0) mode = 0;
+      }
+    }
+  }
+  stt[9] = s;
+  check_finite(c, y, 2 * no, st);
+  check_finite(c, yc, 2 * nc, st);
+  c.lp.record = nullptr;
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc |= ST_CUDA;
+  if (stats) for (int i = 0; i < 10; ++i) stats[i] = stt[i];
   rc |= (int)cudaGetLastError();
   return rc ? ST_CUDA : 0;
 }
@@ -2351,6 +2648,7 @@ void hprod_final_(void) {
   if (!g) return;
   Ctx& c = *g;
   for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  for (auto& ge : c.lp_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
   if (c.st) cudaStreamSynchronize(c.st);
   if (c.st2) cudaStreamSynchronize(c.st2);
   if (c.st3) cudaStreamSynchronize(c.st3);
@@ -2882,6 +3180,58 @@ int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d
     names[names_cap - 1] = 0;
   }
   return rc ? -ST_CUDA : kNumPhases;
+}
+
+int td1c_gpu_set_learned(int depth, const int* sizes, const float* const* W, const float* const* b, void* pack, int use_net,
+                         double bound) {
+  Ctx& c = ctx();
+  if (!c.initialized || bound < 0.0) return ST_CONFIG;
+  int rc = lp_setup(c);
+  if (rc) return rc;
+  c.lp_bound = bound;
+  c.lp_use_net = use_net ? 1 : 0;
+  if (depth <= 0) { c.lp_has_net = false; return 0; }
+  if (depth > MLP_MAXDEPTH || !sizes || !W || !b || !pack || sizes[0] != 32 || sizes[depth] != 8) return ST_CONFIG;
+  MlpInferArgs& a = c.lp_mi;
+  a = MlpInferArgs{};
+  a.depth = depth; a.rows = c.lp.nu; a.nin = sizes[0]; a.x = c.lp.feat; a.ldx = 32; a.y = c.lp_out; a.ldy = 8;
+  a.status = c.lp_mi_status;
+  unsigned short* p = (unsigned short*)pack;
+  for (int k = 0; k < depth; ++k) {
+    if (sizes[k + 1] < 1 || sizes[k + 1] > 256) return ST_CONFIG;
+    const int np = (sizes[k + 1] + 15) / 16 * 16, kp = (sizes[k] + 15) / 16 * 16;
+    a.n[k] = sizes[k + 1]; a.np[k] = np; a.kp[k] = kp; a.b[k] = b[k]; a.wbf16[k] = p;
+    p += (long)np * kp;
+  }
+  c.lp_has_net = true;
+  for (auto& ge : c.lp_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  return 0;
+}
+
+int td1c_gpu_split2_learned(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                            double cep, int maxcyc, double thresh, double* stats) {
+  return learned_run(d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, maxcyc, thresh, nullptr, stats);
+}
+
+int td1c_gpu_learned_record(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc,
+                            double cep, int maxcyc, double thresh, double* d_record) {
+  if (!d_record) return ST_CONFIG;
+  return learned_run(d_wfn, d_cic, t0, dt, nstep, fint, wlen, numcyc, cep, maxcyc, thresh, d_record, nullptr);
+}
+
+int td1c_gpu_learned_dims(int* out4) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out4) return ST_CONFIG;
+  out4[0] = c.npair * c.nfe; out4[1] = c.nfe; out4[2] = c.npair; out4[3] = LP_REC;
+  return 0;
+}
+
+// pair kind of each stored pair (0 diagonal, 1 off-diagonal, 2 with the frozen core) as the predictor uses it
+int td1c_gpu_learned_pair_kind(int* out) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out) return ST_CONFIG;
+  for (int p = 0; p < c.npair; ++p) out[p] = c.pb[p] < c.nfcore ? 2 : (c.pa[p] == c.pb[p] ? 0 : 1);
+  return 0;
 }
 
 int td1c_gpu_wait_selftest(void) {

@@ -53,6 +53,32 @@ struct LegTcPlan {
 };
 int launch_legendre_tc(const LegTcPlan& p, int* status, cudaStream_t st);
 
+// ---- the learned predictor's data path (predictor.cu)
+constexpr int LP_REC = 41;  // doubles per training record: Gram matrix (16 complex), targets (4 complex), |W_n|^2
+struct LpArgs {
+  int nu, nfe, nd, Nr, nlat, npair, ni;  // units (pair x element), grid, pairs, int2e entries
+  size_t nw;                             // complex values of one W field
+  cplx* W;                               // the context's pair potentials (exact value in, stage value out)
+  cplx* ring;                            // [5][nw] history of W at the step start states
+  cplx* int2e;                           // the context's int2e
+  cplx* iring;                           // [5][ni]
+  cplx* gram;                            // [nu][4][4] Gram matrix of each unit's last four history values
+  cplx* weights;                         // [nu][4] weights of the c = 1 prediction
+  double *err, *tnorm;                   // [nu] judge terms
+  double* judge;                         // [0] this step's relative error, [1] running maximum
+  int* counter;                          // history index of the newest value
+  float* feat;                           // [nu][32] network inputs
+  const float* net_out;                  // [nu][8] network outputs
+  int use_net;
+  const int* pair_kind;                  // [npair] 0 diagonal, 1 off-diagonal, 2 with the frozen core
+  double* record;                        // training records [steps][nu][LP_REC] (null: none)
+  int* rec_count;
+};
+int launch_lp_push_judge(const LpArgs& a, cudaStream_t st);
+int launch_lp_features(const LpArgs& a, cudaStream_t st);
+int launch_lp_weights(const LpArgs& a, cudaStream_t st);
+int launch_lp_stage(const LpArgs& a, int half, cudaStream_t st);
+
 // ---- the learned predictor's network (mlp.cu)
 constexpr int MLP_MAXDEPTH = 8;
 struct MlpInferArgs {

@@ -315,6 +315,53 @@ class HProd:
                                                    float(wl.get("cep", 0.0)), _dp(out)))
         return out
 
+    # ---- the learned form (predicted stage mean fields, judge and fallback)
+    def learned_dims(self):
+        d = (ctypes.c_int * 4)()
+        self._check(self.lib.td1c_gpu_learned_dims(d))
+        return dict(nu=d[0], nfe=d[1], npair=d[2], rec=d[3])
+
+    def learned_pair_kind(self):
+        n = self.learned_dims()["npair"]
+        out = np.zeros(n, dtype=np.int32)
+        self._check(self.lib.td1c_gpu_learned_pair_kind(_ip(out)))
+        return out
+
+    def set_learned(self, net=None, use_net=True, bound=1e-6):
+        """Register a learned.DeviceMLP (widths 32 .. 8) for the predicted steps, or none (cubic weights)."""
+        if net is None:
+            self._check(self.lib.td1c_gpu_set_learned(0, None, None, None, None, 0, float(bound)))
+            self._net = None
+            return
+        net.pack()
+        net.torch.cuda.synchronize()  # the BF16 copy is written on torch's stream; the steps read it on the library's
+        self._net = net
+        self._check(self.lib.td1c_gpu_set_learned(net.depth, net._sizes, net._ptrs(net.W), net._ptrs(net.b),
+                                                  ctypes.c_void_p(net._pack.data_ptr()), 1 if use_net else 0, float(bound)))
+
+    def split2_learned_dev(self, d_wfn, d_cic, t0, dt, nstep, maxcyc=20, thresh=1e-10):
+        """Learned split2 steps in place; returns the judge statistics."""
+        wl = self.wl
+        st = np.zeros(10)
+        self._check(self.lib.td1c_gpu_split2_learned(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(t0), float(dt),
+                                                     int(nstep), float(wl["fint"]), float(wl["wlen"]), float(wl["numcyc"]),
+                                                     float(wl.get("cep", 0.0)), int(maxcyc), float(thresh), _dp(st)))
+        keys = ["accepted", "rejected", "exact_windows", "fills", "max_accepted_judge", "min_judge", "max_judge",
+                "predicted_steps", "last_judge", "steps"]
+        out = dict(zip(keys, st.tolist()))
+        if out["min_judge"] > 1e299:
+            out["min_judge"] = None
+        return out
+
+    def learned_record_dev(self, d_wfn, d_cic, t0, dt, nstep, d_record, fint=None, wlen=None, maxcyc=20, thresh=1e-10):
+        """Exact split2 steps writing (nstep + 1) x units training records into the device buffer d_record."""
+        wl = self.wl
+        self._check(self.lib.td1c_gpu_learned_record(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), float(t0), float(dt),
+                                                     int(nstep), float(fint if fint is not None else wl["fint"]),
+                                                     float(wlen if wlen is not None else wl["wlen"]), float(wl["numcyc"]),
+                                                     float(wl.get("cep", 0.0)), int(maxcyc), float(thresh),
+                                                     ctypes.c_void_p(d_record)))
+
     def wait_selftest(self):
         """Status bits of the bounded-wait self-test (ST_TIMEOUT = 32 when the wait bound works)."""
         return int(self.lib.td1c_gpu_wait_selftest())

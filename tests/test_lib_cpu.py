@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def header_symbols():
     src = open(os.path.join(ROOT, "include", "td1c_b200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(td1c_gpu_\w+|hprod_\w+_|h1itr_\w+_|dpade_\w+_)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(td1c_gpu_\w+|td1c_mlp_\w+|td1c_lp_\w+|hprod_\w+_|h1itr_\w+_|dpade_\w+_)\s*\(", src)))
 
 
 def test_header_symbols_exported():
