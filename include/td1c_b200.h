@@ -312,6 +312,33 @@ int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d
 int td1c_gpu_int2e_static(int nact, const int* mval, long K, const double* d_rho2, const double* d_v2sph,
                           double* d_int2e, void* stream);
 
+/* ---- ensembles of independent jobs --------------------------------------
+ * No counterpart in the reference, whose clhprod is a process singleton
+ * (src/hprod/clhprod.cpp:32-34).  Every entry point above acts on the
+ * current context; context 0 is the default one (the drop-in calls' context,
+ * also current after loading).  A new context holds one job: bind, init and
+ * set_wfn0 it like the default one; it gets streams of its own. */
+int td1c_gpu_ctx_create(void);   /* new context, made current; returns its id (>= 1) */
+int td1c_gpu_ctx_select(int id); /* make context id current; 16 for an unknown id */
+int td1c_gpu_ctx_current(void);
+int td1c_gpu_ctx_destroy(int id); /* hprod_final_ of context id (>= 1); the default context becomes current */
+/* launch shapes of the current context (0 = the built-in choice): mt the
+ * FP64 Legendre GEMM's m-tiles per CTA (3 or 6), mf_cap the cap of the
+ * persistent mean-field action grid, i2_split the K split of int2e (at most
+ * the allocated split, get_tuning's out4[3]) */
+int td1c_gpu_set_tuning(int mt, int mf_cap, int i2_split);
+int td1c_gpu_get_tuning(int* out4);
+/* nstep split2 steps (td1c_gpu_split2 with its mask) of njob jobs at once:
+ * job j is context ids[j] (bound with split_type 1) with state d_wfn[j],
+ * d_cic[j] and its own pulse (t0, dt, fint, wlen, numcyc, cep per job).  One
+ * CUDA graph holds one step of every job, each job's kernels on its own
+ * streams forked from one stream, so the jobs run side by side; it is
+ * replayed nstep times.  *ms (host, may be NULL) = device time of the
+ * replays.  Returns 0 or the status bits of the jobs. */
+int td1c_gpu_ensemble_split2(int njob, const int* ids, void* const* d_wfn, void* const* d_cic, const double* t0,
+                             const double* dt, int nstep, const double* fint, const double* wlen, const double* numcyc,
+                             const double* cep, int maxcyc, double thresh, double* ms);
+
 /* ---- the learned form of the propagation -------------------------------
  * No counterpart in the reference.  td1c_gpu_split2 (tdse_split2) with the
  * mean field of the RK4 stages predicted instead of formed from the stage
@@ -322,10 +349,13 @@ int td1c_gpu_int2e_static(int nact, const int* mval, long K, const double* d_rho
  * pair and one FEDVR element) with weights = the cubic extrapolation through
  * the last four steps + a correction from the registered network.  The exact
  * value of every step judges the previous step's prediction (relative error
- * over all units); after a window of 8 predicted steps the window stands if
- * its largest judge value is at most the bound, else the state returns to
- * the window's start and the window is recomputed exactly, after which
- * exact steps run for a back-off of 1, 3, 7, ... (at most 63) windows.
+ * over all units).  Windows of 8 steps: a window of exact steps that fills
+ * the history also judges the predictions it would have made; only when
+ * their largest judge value is at most the bound are predicted steps tried.
+ * A window of predicted steps stands if its largest judge value is at most
+ * the bound, else the state returns to the window's start and the window
+ * is recomputed exactly.  After a judge value above the bound, exact steps
+ * without history run for a back-off of 1, 3, 7, ... (at most 63) windows.
  * Needs a context bound with split_type 1 (the RHS without h0 and laser). */
 /* Register the network (device pointers, FP32 weights as td1c_mlp_forward
  * takes them, widths 32 .. 8; pack: td1c_mlp_pack_size bytes, the BF16
@@ -335,6 +365,10 @@ int td1c_gpu_int2e_static(int nact, const int* mval, long K, const double* d_rho
  * largest accepted relative error (1e-6 by default). */
 int td1c_gpu_set_learned(int depth, const int* sizes, const float* const* W, const float* const* b, void* pack, int use_net,
                          double bound);
+/* screen = 1 (default): predicted windows only after a history-filling window
+ * whose judge values pass the bound; 0: after every history-filling window
+ * (each predicted window is then judged and, above the bound, rolled back). */
+int td1c_gpu_set_learned_policy(int screen);
 /* learned split2 steps on device buffers (arguments as td1c_gpu_split2);
  * stats (host, 10 doubles, may be NULL): windows accepted, rejected, exact
  * (back-off), history fills; largest judge value of an accepted window;

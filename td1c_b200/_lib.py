@@ -144,6 +144,8 @@ def load():
     lib.td1c_mlp_infer_bf16.argtypes = [c_int, ip, fpp, fpp, vp, c_int, vp, c_int, vp, vp, vp]
     lib.td1c_gpu_set_learned.restype = c_int
     lib.td1c_gpu_set_learned.argtypes = [c_int, ip, fpp, fpp, vp, c_int, c_double]
+    lib.td1c_gpu_set_learned_policy.restype = c_int
+    lib.td1c_gpu_set_learned_policy.argtypes = [c_int]
     lib.td1c_gpu_split2_learned.restype = c_int
     lib.td1c_gpu_split2_learned.argtypes = [vp, vp, c_double, c_double, c_int, c_double, c_double, c_double, c_double, c_int,
                                             c_double, dp]
@@ -158,6 +160,18 @@ def load():
     lib.td1c_lp_features.argtypes = [c_int, vp, vp, c_int, c_int, vp, vp, vp]
     lib.td1c_lp_loss.restype = c_int
     lib.td1c_lp_loss.argtypes = [c_int, vp, vp, vp, vp, vp, c_int, vp]
+    for name in ("td1c_gpu_ctx_create", "td1c_gpu_ctx_current"):
+        getattr(lib, name).restype = c_int
+        getattr(lib, name).argtypes = []
+    for name in ("td1c_gpu_ctx_select", "td1c_gpu_ctx_destroy"):
+        getattr(lib, name).restype = c_int
+        getattr(lib, name).argtypes = [c_int]
+    lib.td1c_gpu_set_tuning.restype = c_int
+    lib.td1c_gpu_set_tuning.argtypes = [c_int, c_int, c_int]
+    lib.td1c_gpu_get_tuning.restype = c_int
+    lib.td1c_gpu_get_tuning.argtypes = [ip]
+    lib.td1c_gpu_ensemble_split2.restype = c_int
+    lib.td1c_gpu_ensemble_split2.argtypes = [c_int, ip, fpp, fpp, dp, dp, c_int, dp, dp, dp, dp, c_int, c_double, dp]
     lib.td1c_gpu_bind_ormas.restype = c_int
     lib.td1c_gpu_bind_ormas.argtypes = [c_int]
     lib.td1c_gpu_wait_selftest.restype = c_int
@@ -181,6 +195,8 @@ EXPORTED = [
     "td1c_gpu_debug_ptr", "td1c_gpu_debug_xfer", "td1c_gpu_set_mf_external", "td1c_gpu_pulse_lfield",
     "td1c_gpu_bind_ormas", "td1c_gpu_wait_selftest",
     "td1c_mlp_forward", "td1c_mlp_backward", "td1c_mlp_adam", "td1c_mlp_pack_size", "td1c_mlp_infer_bf16",
-    "td1c_gpu_set_learned", "td1c_gpu_split2_learned", "td1c_gpu_learned_record", "td1c_gpu_learned_dims",
+    "td1c_gpu_set_learned", "td1c_gpu_set_learned_policy", "td1c_gpu_split2_learned", "td1c_gpu_learned_record", "td1c_gpu_learned_dims",
     "td1c_gpu_learned_pair_kind", "td1c_lp_features", "td1c_lp_loss",
+    "td1c_gpu_ctx_create", "td1c_gpu_ctx_select", "td1c_gpu_ctx_current", "td1c_gpu_ctx_destroy",
+    "td1c_gpu_set_tuning", "td1c_gpu_get_tuning", "td1c_gpu_ensemble_split2",
 ]

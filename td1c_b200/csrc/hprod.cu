@@ -47,7 +47,7 @@ namespace {
 
 const double PI = 3.14159265358979323846264338327950288;
 
-std::vector<void*> g_allocs;  // every device allocation of the context, freed by hprod_final_
+std::vector<void*>& cur_allocs();  // every device allocation of the current context, freed by hprod_final_
 
 template <class T>
 T* dalloc(size_t n) {
@@ -62,7 +62,7 @@ T* dalloc(size_t n) {
   // allocation must not race the clearing
   cudaMemset(p, 0, n * sizeof(T));
   cudaStreamSynchronize(cudaStreamLegacy);
-  g_allocs.push_back(p);
+  cur_allocs().push_back(p);
   return p;
 }
 template <class T>
@@ -72,7 +72,34 @@ T* dupload(const std::vector<T>& v) {
   return p;
 }
 
+struct RkBufs {
+  cplx *y0 = nullptr, *yt = nullptr, *k = nullptr, *k2 = nullptr;  // orbitals then CI, contiguous
+  double* lf_cur = nullptr;
+  int* counter = nullptr;
+  size_t cap = 0;
+  const cplx* reset_orb = nullptr;  // optional: every step starts from this state
+  const cplx* reset_cic = nullptr;
+  // cached graph of one step and what it was captured with
+  const void* g_y = nullptr; const void* g_yc = nullptr; const void* g_tab = nullptr;
+  const void* g_ro = nullptr; double g_dt = 0; long g_per = 0;
+  int h_counter[2] = {0, 0};
+  // cached graphs of one split2 / ETD-RK2 / ETD-RK4 step
+  const void* s_y[3] = {nullptr, nullptr, nullptr}; const void* s_yc[3] = {nullptr, nullptr, nullptr};
+  const void* s_tab[3] = {nullptr, nullptr, nullptr}; double s_dt[3] = {0, 0, 0}; int s_cyc[3] = {0, 0, 0};
+  double s_thr[3] = {0, 0, 0}; int s_split[3] = {-1, -1, -1}; int s_mask[3] = {-1, -1, -1}; long s_per[3] = {0, 0, 0};
+  const void* s_ro[3] = {nullptr, nullptr, nullptr};
+  int g_ctl = -1, s_ctl[3] = {-1, -1, -1};  // control flags (icomp, igauge) the graphs were captured with
+};
+struct Etd4Bufs {
+  cplx *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *h2 = nullptr, *h3 = nullptr, *tmp = nullptr;
+  size_t cap = 0;
+};
 struct Ctx {
+  std::vector<void*> allocs;  // device allocations of this context
+  RkBufs rk;                  // propagation buffers and cached step graphs
+  Etd4Bufs e4;
+  bool own_streams = false;   // contexts other than the default one own their streams
+  int tune_mt = 0, tune_mf_cap = 0, tune_i2_split = 0;  // launch shapes (0: the built-in choice)
   // ---- bound inputs
   bool have_rad = false, have_sph = false, have_bas = false, initialized = false;
   int nfe = 0, nd = 0, nrad = 0, Nr = 0;
@@ -186,7 +213,15 @@ struct Ctx {
   int lp_use_net = 0;
   double lp_bound = 1e-6;
   cplx* lp_save = nullptr;  // the state at the start of a judged window (orbitals, then CI)
-  cudaGraphExec_t lp_exec[3] = {nullptr, nullptr, nullptr};  // E, H, P steps (captured per call)
+  cudaGraphExec_t lp_exec[3] = {nullptr, nullptr, nullptr};  // E, H, P steps
+  long lp_exec_launch[3] = {0, 0, 0};
+  // what the captured steps and the window schedule belong to: a call that starts where the last
+  // one ended (same state buffers, field and step) continues its history and schedule
+  const void* lp_key_y = nullptr; const void* lp_key_yc = nullptr; const void* lp_key_tab = nullptr;
+  double lp_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double lp_t_end = -1e300;
+  int lp_mode = 0, lp_backoff = 0, lp_plain_left = 0;
+  int lp_screen = 1;  // 1: predicted windows only after a fill window whose judge values pass
   cudaEvent_t ev[16] = {};
   cudaStream_t st2 = nullptr;  // side stream of the CI RDM chain (process lifetime, like st)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -201,11 +236,16 @@ const char* kPhaseNames[] = {"orbin", "ci_rdm", "onebody", "rho_gemm", "poisson"
                              "gorb_gemm", "orbdots", "int2e", "smallmat", "ci_sigma", "dtorb"};
 const int kNumPhases = 13;
 
-Ctx* g = nullptr;
+// contexts: [0] is the default one the drop-in entry points use; further
+// contexts (td1c_gpu_ctx_create) hold independent jobs of an ensemble
+std::vector<Ctx*> g_ctxs(1, nullptr);
+int g_cur = 0;
+Ctx* g = nullptr;  // the current context, g_ctxs[g_cur]
 Ctx& ctx() {
-  if (!g) g = new Ctx();
+  if (!g) { g = new Ctx(); g_ctxs[g_cur] = g; }
   return *g;
 }
+std::vector<void*>& cur_allocs() { return ctx().allocs; }
 
 // ===========================================================================
 // set-up kernels
@@ -1294,7 +1334,14 @@ int build_ci(Ctx& c) {
 // ===========================================================================
 int gemm(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
   c.launches++;
-  return launch_legendre_gemm(b, nb, M, K, 2 * c.Nr, pair, c.st);
+  return launch_legendre_gemm_mt(b, nb, M, K, 2 * c.Nr, pair, c.tune_mt, c.st);
+}
+// the int2e K split: the tuned value where one is set (at most the allocated split)
+int i2_split(const Ctx& c) { return c.tune_i2_split > 0 ? std::min(c.tune_i2_split, c.i2_nsplit) : c.i2_nsplit; }
+int mfprod_run(Ctx& c, cudaStream_t st) {
+  MfprodArgs m = c.mf;
+  m.max_cta = c.tune_mf_cap;
+  return launch_mfprod(m, st);
 }
 // the mean field's transforms (pair densities theta -> l, pair potentials l -> theta):
 // FP64 DMMA, or split TF32 on tcgen05 in the mixed-precision form
@@ -1317,10 +1364,10 @@ void build_tc_plans(Ctx& c) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (c.npair > 0 && !c.h_b_rho.empty())
     c.tc_ok_rho = legendre_tc_plan(c.h_b_rho, c.b_rho, c.L2, c.nlat, 2 * c.Nr, true, (const double*)c.orbg, c.nfun, nsm, &c.tc_rho,
-                                   g_allocs, c.st) == 0;
+                                   c.allocs, c.st) == 0;
   if (c.npair > 0 && !c.h_b_W.empty())
     c.tc_ok_W = legendre_tc_plan(c.h_b_W, c.b_W, c.nlat, c.L2, 2 * c.Nr, false, (const double*)c.v2sph, c.npair_all, nsm,
-                                 &c.tc_W, g_allocs, c.st) == 0;
+                                 &c.tc_W, c.allocs, c.st) == 0;
 }
 
 // report the first failing launcher of an RHS (status ST_CUDA is set by the caller)
@@ -1402,7 +1449,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     mark(); mark();  // no rho_gemm, no poisson
     mark();          // no w_gemm
     join();
-    rc |= chk("mfprod", launch_mfprod(c.mf, st));
+    rc |= chk("mfprod", mfprod_run(c, st));
     c.launches += 2;
     mark();  // end mfprod
     rc |= chk("gorb gemm", gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false));
@@ -1417,8 +1464,8 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     if (c.nact > 0) {
       cudaEventRecord(c.ev_i2_fork, st);
       cudaStreamWaitEvent(c.st3, c.ev_i2_fork, 0);
-      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, c.st3));
-      else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, c.st3));
+      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, i2_split(c), c.st3));
+      else rc |= chk("int2e", launch_int2e(c.i2, i2_split(c), c.st3));
       cudaStreamWaitEvent(c.st3, c.ev_join, 0);
       rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, c.st3));
       cudaEventRecord(c.ev_i2_join, c.st3);
@@ -1429,7 +1476,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     rc |= chk("W gemm", gemm_mf(c, c.b_W, c.npair, c.nlat, c.L2, false));
     mark();  // end w_gemm
     join();
-    rc |= chk("mfprod", launch_mfprod(c.mf, st));
+    rc |= chk("mfprod", mfprod_run(c, st));
     c.launches += 2;
     mark();  // end mfprod
     rc |= chk("gorb gemm", gemm(c, c.b_gorb, c.n_gorb, c.L1, c.nlat, false));
@@ -1447,8 +1494,8 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     cudaStreamWaitEvent(st, c.ev_i2_join, 0);
   } else if (c.nact > 0) {
     if (!c.mf_external || c.npair == 0) {
-      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
-      else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
+      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, i2_split(c), st));
+      else rc |= chk("int2e", launch_int2e(c.i2, i2_split(c), st));
       c.launches += 3;
     }
     rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, st));  // the CI chain joined before mfprod
@@ -1611,25 +1658,6 @@ void pulse_lfield(const Pulse& p, double t, double* lf) {
   }
 }
 
-struct RkBufs {
-  cplx *y0 = nullptr, *yt = nullptr, *k = nullptr, *k2 = nullptr;  // orbitals then CI, contiguous
-  double* lf_cur = nullptr;
-  int* counter = nullptr;
-  size_t cap = 0;
-  const cplx* reset_orb = nullptr;  // optional: every step starts from this state
-  const cplx* reset_cic = nullptr;
-  // cached graph of one step and what it was captured with
-  const void* g_y = nullptr; const void* g_yc = nullptr; const void* g_tab = nullptr;
-  const void* g_ro = nullptr; double g_dt = 0; long g_per = 0;
-  int h_counter[2] = {0, 0};
-  // cached graphs of one split2 / ETD-RK2 / ETD-RK4 step
-  const void* s_y[3] = {nullptr, nullptr, nullptr}; const void* s_yc[3] = {nullptr, nullptr, nullptr};
-  const void* s_tab[3] = {nullptr, nullptr, nullptr}; double s_dt[3] = {0, 0, 0}; int s_cyc[3] = {0, 0, 0};
-  double s_thr[3] = {0, 0, 0}; int s_split[3] = {-1, -1, -1}; int s_mask[3] = {-1, -1, -1}; long s_per[3] = {0, 0, 0};
-  const void* s_ro[3] = {nullptr, nullptr, nullptr};
-  int g_ctl = -1, s_ctl[3] = {-1, -1, -1};  // control flags (icomp, igauge) the graphs were captured with
-};
-RkBufs g_rk;
 
 // ---------------------------------------------------------------------------
 // one-body propagators (h1prop.cu): factor cache and the application of
@@ -1810,7 +1838,7 @@ int h1_run(Ctx& c, bool pade, cplx fac, cplx zf0, bool allow_cycles, const doubl
 int rk4_stages(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, const double* lf) {
   cudaStream_t st = c.st;
   const size_t no = c.nbas * c.nfun, nc = c.lcic;
-  RkBufs& b = g_rk;
+  RkBufs& b = c.rk;
   const double wts[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
   const double anext[4] = {0.5, 0.5, 1.0, 0.0};
   cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
@@ -1832,7 +1860,7 @@ int rk4_stages(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, const double* lf) {
 // (wfn_mask, step counter)
 void step_begin(Ctx& c, cplx* y_orb, cplx* y_cic, int per) {
   cudaStream_t st = c.st;
-  RkBufs& b = g_rk;
+  RkBufs& b = c.rk;
   field_select_kernel<<<1, 64, 0, st>>>(c.field_tab, b.counter, per, b.lf_cur);
   c.launches++;
   if (b.reset_orb) {
@@ -1849,14 +1877,14 @@ int step_end(Ctx& c, cplx* y_orb, bool do_mask) {
     mask_kernel<<<(unsigned)((no + 255) / 256), 256, 0, st>>>(c.Nr, c.L1, c.nfun, c.nfcore, min_irad, c.d_mval, c.mask, y_orb);
     c.launches++;
   }
-  counter_inc_kernel<<<1, 32, 0, st>>>(g_rk.counter);
+  counter_inc_kernel<<<1, 32, 0, st>>>(c.rk.counter);
   c.launches++;
   return (int)cudaGetLastError();
 }
 
 int rk_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt) {
   step_begin(c, y_orb, y_cic, 36);
-  int rc = rk4_stages(c, y_orb, y_cic, dt, g_rk.lf_cur);
+  int rc = rk4_stages(c, y_orb, y_cic, dt, c.rk.lf_cur);
   rc |= step_end(c, y_orb, true);
   return rc;
 }
@@ -1868,7 +1896,7 @@ int rk_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt) {
 int split2_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double thresh, bool do_mask) {
   step_begin(c, y_orb, y_cic, 54);
   const bool doh1 = c.isplit != 0, doh2 = c.neltot > 1 || c.isplit != 1;
-  const double* lf = g_rk.lf_cur;
+  const double* lf = c.rk.lf_cur;
   int rc = 0;
   if (doh1) rc |= h1_apply(c, false, lf + 36, y_orb, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
   if (doh2) rc |= rk4_stages(c, y_orb, y_cic, dt, lf);
@@ -1883,7 +1911,7 @@ int split2_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double 
 int etdrk2_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double thresh, bool do_mask) {
   cudaStream_t st = c.st;
   step_begin(c, y_orb, y_cic, 18);
-  RkBufs& b = g_rk;
+  RkBufs& b = c.rk;
   const size_t no = c.nbas * c.nfun, nc = c.lcic, n = no + nc;
   const double* lf = b.lf_cur;
   const unsigned gn = (unsigned)((n + 255) / 256), go = (unsigned)((no + 255) / 256), gc = (unsigned)((nc + 255) / 256);
@@ -1953,11 +1981,6 @@ Etd4Fun etd4_fun(int which, double dt, int icomp) {
   return F;
 }
 
-struct Etd4Bufs {
-  cplx *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *h2 = nullptr, *h3 = nullptr, *tmp = nullptr;
-  size_t cap = 0;
-};
-Etd4Bufs g_e4;
 
 void zaxpby(Ctx& c, size_t n, cplx* z, const cplx* x, const cplx* y, cplx a, cplx b) {
   if (!n) return;
@@ -1983,7 +2006,7 @@ int h1rat_run(Ctx& c, const Etd4Fun& F, const double* d_lf, cplx* w, int maxcyc,
     return 0;
   }
   int rc = 0;
-  cplx* t = g_e4.tmp;
+  cplx* t = c.e4.tmp;
   cudaMemcpyAsync(t, w, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
   zaxpby(c, nd, w + nf, w + nf, w + nf, F.n[0], mkc(0, 0));
   OneBodyArgs ob{};
@@ -2012,8 +2035,8 @@ int h1rat_run(Ctx& c, const Etd4Fun& F, const double* d_lf, cplx* w, int maxcyc,
 int etdrk4_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double thresh, bool do_mask) {
   cudaStream_t st = c.st;
   step_begin(c, y_orb, y_cic, 27);
-  RkBufs& b = g_rk;
-  Etd4Bufs& e = g_e4;
+  RkBufs& b = c.rk;
+  Etd4Bufs& e = c.e4;
   const size_t no = c.nbas * c.nfun, nc = c.lcic, n = no + nc;
   const double* lf = b.lf_cur;
   const double* lh = lf + 9;
@@ -2116,8 +2139,8 @@ int run_meanfield(Ctx& c, const cplx* wfn, const double* d_lf) {
   c.launches += 3;
   rc |= chk("W gemm", gemm_mf(c, c.b_W, c.npair, c.nlat, c.L2, false));
   if (c.nact > 0) {
-    if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, c.i2_nsplit, st));
-    else rc |= chk("int2e", launch_int2e(c.i2, c.i2_nsplit, st));
+    if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, i2_split(c), st));
+    else rc |= chk("int2e", launch_int2e(c.i2, i2_split(c), st));
     c.launches += 3;
   }
   return rc;
@@ -2149,7 +2172,7 @@ int lp_j(Ctx& c, const cplx* y, const double* d_lf) {
 int lp_rk4_pred(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, const double* lf) {
   cudaStream_t st = c.st;
   const size_t no = c.nbas * c.nfun, nc = c.lcic;
-  RkBufs& b = g_rk;
+  RkBufs& b = c.rk;
   const double wts[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
   const double anext[4] = {0.5, 0.5, 1.0, 0.0};
   cudaMemcpyAsync(b.y0, y_orb, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
@@ -2182,13 +2205,13 @@ int lp_step(Ctx& c, int kind, cplx* y, cplx* yc, double dt, int maxcyc, double t
     rc |= split2_step(c, y, yc, dt, maxcyc, thresh, true);
   } else {
     step_begin(c, y, yc, 54);
-    const double* lf = g_rk.lf_cur;
+    const double* lf = c.rk.lf_cur;
     rc |= h1_apply(c, false, lf + 36, y, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
     rc |= lp_rk4_pred(c, y, yc, dt, lf);
     rc |= h1_apply(c, false, lf + 45, y, 0.5 * dt, mkc(0, 0), maxcyc, thresh);
     rc |= step_end(c, y, true);
   }
-  rc |= lp_j(c, y, g_rk.lf_cur + 27);  // the field at t + dt (the step's last stage field)
+  rc |= lp_j(c, y, c.rk.lf_cur + 27);  // the field at t + dt (the step's last stage field)
   return rc;
 }
 
@@ -2204,14 +2227,14 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
   if (kind != 0 && (maxcyc < 0 || !(thresh >= 0.0))) return ST_CONFIG;
   cudaStream_t st = c.st;
   const size_t no = c.nbas * c.nfun, nc = c.lcic;
-  RkBufs& b = g_rk;
+  RkBufs& b = c.rk;
   if (b.cap < no + nc) {
     b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc); b.k2 = dalloc<cplx>(no + nc);
     if (!b.lf_cur) { b.lf_cur = dalloc<double>(54); b.counter = dalloc<int>(2); }
     b.cap = no + nc;
   }
-  if (kind == 3 && g_e4.cap < no + nc) {
-    Etd4Bufs& e = g_e4;
+  if (kind == 3 && c.e4.cap < no + nc) {
+    Etd4Bufs& e = c.e4;
     for (cplx** q : {&e.w1, &e.w2, &e.w3, &e.h2, &e.h3, &e.tmp}) *q = dalloc<cplx>(no + nc);
     e.cap = no + nc;
   }
@@ -2322,7 +2345,7 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
   if (rc) return rc;
   cudaStream_t st = c.st;
   const size_t no = c.nbas * c.nfun, nc = c.lcic;
-  RkBufs& b = g_rk;
+  RkBufs& b = c.rk;
   if (b.cap < no + nc) {
     b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc); b.k2 = dalloc<cplx>(no + nc);
     if (!b.lf_cur) { b.lf_cur = dalloc<double>(54); b.counter = dalloc<int>(2); }
@@ -2353,7 +2376,22 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
   cplx* yc = (cplx*)d_cic;
   c.lp.record = record;
   cudaMemsetAsync(c.lp.rec_count, 0, sizeof(int), st);
-  cudaMemsetAsync(c.lp.gram, 0, (size_t)c.lp.nu * 16 * sizeof(cplx), st);
+  // captured steps are reused while their inputs are the same; a call that continues the last one
+  // (same buffers and pulse, t0 = its end time) keeps the history and the window schedule
+  const double key[8] = {dt, fint, wlen, numcyc, cep, (double)maxcyc, thresh,
+                         (double)(c.icomp * 2 + c.igauge + 4 * c.mixed + 16 * (c.lp_use_net && c.lp_has_net))};
+  bool same = c.lp_key_y == y && c.lp_key_yc == yc && c.lp_key_tab == c.field_tab && !record;
+  for (int i = 0; i < 8 && same; ++i) same = c.lp_key[i] == key[i];
+  const bool cont = same && std::fabs(t0 - c.lp_t_end) <= 1e-9 * std::max(1.0, std::fabs(t0));
+  if (!same || record) {
+    for (auto& ge : c.lp_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+    c.lp_key_y = record ? nullptr : y; c.lp_key_yc = record ? nullptr : yc; c.lp_key_tab = c.field_tab;
+    for (int i = 0; i < 8; ++i) c.lp_key[i] = key[i];
+  }
+  if (!cont) {
+    cudaMemsetAsync(c.lp.gram, 0, (size_t)c.lp.nu * 16 * sizeof(cplx), st);
+    c.lp_mode = 0; c.lp_backoff = 0; c.lp_plain_left = 0;
+  }
   // J of the state at step s (the window's start state)
   auto j0 = [&](int s) -> int {
     double lf[9];
@@ -2362,14 +2400,12 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
     cudaStreamSynchronize(st);  // lf lives on this frame
     return lp_j(c, y, c.lfield);
   };
-  // one step of the given kind: eager the first time in this call (factor
-  // set-up), then a graph captured in this call
-  for (auto& ge : c.lp_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
-  long per_launch[3] = {0, 0, 0};
+  // one step of the given kind: eager the first time (factor set-up), then a
+  // captured graph, kept for later calls with the same inputs
   bool warm[3] = {false, false, false};
   auto step = [&](int kind) -> int {
     cudaGraphExec_t& ge = c.lp_exec[kind];
-    if (!warm[kind]) {
+    if (!ge && !warm[kind]) {
       warm[kind] = true;
       return lp_step(c, kind, y, yc, dt, maxcyc, thresh);  // eager: first-call set-up happens here
     }
@@ -2381,11 +2417,11 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
       if (cudaStreamEndCapture(st, &graph) != cudaSuccess || r) return ST_CUDA;
       if (cudaGraphInstantiate(&ge, graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
       cudaGraphDestroy(graph);
-      per_launch[kind] = c.launches - l0;
+      c.lp_exec_launch[kind] = c.launches - l0;
       c.launches = l0;
     }
     if (cudaGraphLaunch(ge, st) != cudaSuccess) return ST_CUDA;
-    c.launches += per_launch[kind];
+    c.launches += c.lp_exec_launch[kind];
     return 0;
   };
   double stt[10] = {0, 0, 0, 0, 0, 1e300, 0, 0, 0, 0};
@@ -2394,17 +2430,32 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
     rc |= j0(0);
     for (; s < nstep && !rc; ++s) rc |= step(1);
   } else {
-    int mode = 0;  // 0 FILL, 1 TRY, 2 PLAIN
-    int backoff = 0, plain_left = 0;
+    int mode = c.lp_mode;  // 0 FILL, 1 TRY, 2 PLAIN (continued from the last call when it continues it)
+    int backoff = c.lp_backoff, plain_left = c.lp_plain_left;
     const bool can_predict = true;
     while (s < nstep && !rc) {
       const int w = std::min(LP_WIN, nstep - s);
       if (mode == 0) {
+        // the exact steps judge every step's prediction as well (their J): once the history
+        // is full, the window's judge values decide whether predicted steps are tried at all
         rc |= j0(s);
-        for (int k = 0; k < w && !rc; ++k) rc |= step(1);
+        for (int k = 0; k < w && !rc; ++k) {
+          if (k == 4) cudaMemsetAsync(c.lp.judge, 0, 2 * sizeof(double), st);
+          rc |= step(1);
+        }
         s += w;
         stt[3] += 1;
-        mode = (w >= 4 && can_predict) ? 1 : 0;
+        double jd[2] = {0, 0};
+        cudaMemcpyAsync(jd, c.lp.judge, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) { rc |= ST_CUDA; break; }
+        if (w > 4) { stt[5] = std::min(stt[5], jd[1]); stt[6] = std::max(stt[6], jd[1]); stt[8] = jd[1]; }
+        if (w > 4 && can_predict && (!c.lp_screen || (jd[1] <= c.lp_bound && std::isfinite(jd[1])))) {
+          mode = 1;
+        } else {
+          backoff = std::min(2 * backoff + 1, 63);
+          plain_left = backoff;
+          mode = w > 4 ? 2 : 0;
+        }
       } else if (mode == 1) {
         cudaMemcpyAsync(c.lp_save, y, no * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
         cudaMemcpyAsync(c.lp_save + no, yc, nc * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
@@ -2441,7 +2492,9 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
         if (--plain_left <= 0) mode = 0;
       }
     }
+    c.lp_mode = mode; c.lp_backoff = backoff; c.lp_plain_left = plain_left;
   }
+  c.lp_t_end = t0 + dt * s;
   stt[9] = s;
   check_finite(c, y, 2 * no, st);
   check_finite(c, yc, 2 * nc, st);
@@ -2537,14 +2590,18 @@ void hprod_init_(void) {
   // one library stream for the process lifetime: callers may hold it
   // (td1c_gpu_stream) beyond hprod_final_
   static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr, lib_stream3 = nullptr, lib_stream4 = nullptr;
-  if (!lib_stream4) cudaStreamCreateWithFlags(&lib_stream4, cudaStreamNonBlocking);
-  c.st4 = lib_stream4;
-  if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
-  if (!lib_stream2) cudaStreamCreateWithFlags(&lib_stream2, cudaStreamNonBlocking);
-  if (!lib_stream3) cudaStreamCreateWithFlags(&lib_stream3, cudaStreamNonBlocking);
-  c.st = lib_stream;
-  c.st2 = lib_stream2;
-  c.st3 = lib_stream3;
+  if (g_cur == 0) {
+    if (!lib_stream4) cudaStreamCreateWithFlags(&lib_stream4, cudaStreamNonBlocking);
+    if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
+    if (!lib_stream2) cudaStreamCreateWithFlags(&lib_stream2, cudaStreamNonBlocking);
+    if (!lib_stream3) cudaStreamCreateWithFlags(&lib_stream3, cudaStreamNonBlocking);
+    c.st = lib_stream; c.st2 = lib_stream2; c.st3 = lib_stream3; c.st4 = lib_stream4;
+  } else if (!c.st) {
+    // an ensemble job: its own streams, so that a graph captured over several
+    // jobs (forked from one stream) has no edges between them
+    for (cudaStream_t* q : {&c.st, &c.st2, &c.st3, &c.st4}) cudaStreamCreateWithFlags(q, cudaStreamNonBlocking);
+    c.own_streams = true;
+  }
   for (cudaEvent_t* e : {&c.ev_fork, &c.ev_join, &c.ev_ob_fork, &c.ev_ob_join, &c.ev_i2_fork, &c.ev_i2_join,
                          &c.ev_sig_fork, &c.ev_sig_join})
     cudaEventCreateWithFlags(e, cudaEventDisableTiming);
@@ -2656,12 +2713,13 @@ void hprod_final_(void) {
                         c.ev_sig_join})
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t& e : c.ev) if (e) { cudaEventDestroy(e); e = nullptr; }
-  for (void* p : g_allocs) cudaFree(p);
-  g_allocs.clear();
-  g_rk = RkBufs();
-  g_e4 = Etd4Bufs();
+  for (void* p : c.allocs) cudaFree(p);
+  c.allocs.clear();
+  if (c.own_streams)
+    for (cudaStream_t q : {c.st, c.st2, c.st3, c.st4}) if (q) cudaStreamDestroy(q);
   delete g;
   g = nullptr;
+  g_ctxs[g_cur] = nullptr;
 }
 
 int td1c_gpu_last_status(void) { return g ? g->status : 0; }
@@ -3089,8 +3147,8 @@ void dpade_prod_(const int* isplit, const int* igauge, const int* icomp, const i
 long td1c_gpu_launch_count(void) { return g ? g->launches : 0; }
 
 int td1c_gpu_rk4_reset(const void* d_wfn0, const void* d_cic0) {
-  g_rk.reset_orb = (const cplx*)d_wfn0;
-  g_rk.reset_cic = (const cplx*)d_cic0;
+  ctx().rk.reset_orb = (const cplx*)d_wfn0;
+  ctx().rk.reset_cic = (const cplx*)d_cic0;
   return 0;
 }
 
@@ -3190,6 +3248,7 @@ int td1c_gpu_set_learned(int depth, const int* sizes, const float* const* W, con
   if (rc) return rc;
   c.lp_bound = bound;
   c.lp_use_net = use_net ? 1 : 0;
+  c.lp_key_y = nullptr;
   if (depth <= 0) { c.lp_has_net = false; return 0; }
   if (depth > MLP_MAXDEPTH || !sizes || !W || !b || !pack || sizes[0] != 32 || sizes[depth] != 8) return ST_CONFIG;
   MlpInferArgs& a = c.lp_mi;
@@ -3205,6 +3264,14 @@ int td1c_gpu_set_learned(int depth, const int* sizes, const float* const* W, con
   }
   c.lp_has_net = true;
   for (auto& ge : c.lp_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  c.lp_key_y = nullptr;  // the next call starts afresh
+  return 0;
+}
+
+int td1c_gpu_set_learned_policy(int screen) {
+  Ctx& c = ctx();
+  c.lp_screen = screen ? 1 : 0;
+  c.lp_key_y = nullptr;
   return 0;
 }
 
@@ -3232,6 +3299,155 @@ int td1c_gpu_learned_pair_kind(int* out) {
   if (!c.initialized || !out) return ST_CONFIG;
   for (int p = 0; p < c.npair; ++p) out[p] = c.pb[p] < c.nfcore ? 2 : (c.pa[p] == c.pb[p] ? 0 : 1);
   return 0;
+}
+
+// ---- contexts of an ensemble and their launch shapes ------------------------
+int td1c_gpu_ctx_create(void) {
+  int id = -1;
+  for (int i = 1; i < (int)g_ctxs.size(); ++i)
+    if (!g_ctxs[i]) { id = i; break; }
+  if (id < 0) { id = (int)g_ctxs.size(); g_ctxs.push_back(nullptr); }
+  g_cur = id;
+  g = new Ctx();
+  g_ctxs[id] = g;
+  return id;
+}
+
+int td1c_gpu_ctx_select(int id) {
+  if (id < 0 || id >= (int)g_ctxs.size()) return ST_CONFIG;
+  g_cur = id;
+  g = g_ctxs[id];
+  return 0;
+}
+
+int td1c_gpu_ctx_current(void) { return g_cur; }
+
+int td1c_gpu_ctx_destroy(int id) {
+  if (id <= 0 || id >= (int)g_ctxs.size()) return ST_CONFIG;
+  const int keep = g_cur;
+  td1c_gpu_ctx_select(id);
+  hprod_final_();
+  td1c_gpu_ctx_select(keep == id ? 0 : keep);
+  return 0;
+}
+
+int td1c_gpu_set_tuning(int mt, int mf_cap, int i2_split_) {
+  Ctx& c = ctx();
+  if ((mt != 0 && mt != 3 && mt != 6) || mf_cap < 0 || i2_split_ < 0) return ST_CONFIG;
+  c.tune_mt = mt; c.tune_mf_cap = mf_cap; c.tune_i2_split = i2_split_;
+  for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }  // recaptured with the new shapes
+  return 0;
+}
+
+int td1c_gpu_get_tuning(int* out4) {
+  Ctx& c = ctx();
+  if (!out4) return ST_CONFIG;
+  out4[0] = c.tune_mt; out4[1] = c.tune_mf_cap; out4[2] = c.tune_i2_split; out4[3] = c.i2_nsplit;
+  return 0;
+}
+
+// nstep split2 steps of every job of an ensemble in one CUDA graph per step:
+// the step of job j is captured on job j's own streams, forked from one
+// stream and joined back, so the jobs' kernels have no order between them and
+// the GPU runs them side by side.  *ms = device time of the nstep replays.
+int td1c_gpu_ensemble_split2(int njob, const int* ids, void* const* d_wfn, void* const* d_cic, const double* t0,
+                             const double* dt, int nstep, const double* fint, const double* wlen, const double* numcyc,
+                             const double* cep, int maxcyc, double thresh, double* ms) {
+  if (njob < 1 || !ids || !d_wfn || !d_cic || !t0 || !dt || !fint || !wlen || !numcyc || !cep || nstep < 0 || maxcyc < 0)
+    return ST_CONFIG;
+  const int keep = g_cur;
+  static cudaStream_t master = nullptr;
+  static std::vector<cudaEvent_t> evs;
+  if (!master) cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking);
+  while ((int)evs.size() < 2 * njob + 2) {
+    cudaEvent_t e;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    evs.push_back(e);
+  }
+  int rc = 0;
+  // per job: the field table, buffers and first-call set-up (outside any capture)
+  for (int j = 0; j < njob && !rc; ++j) {
+    if (td1c_gpu_ctx_select(ids[j]) || !g || !g->initialized || g->isplit != 1) { rc = ST_CONFIG; break; }
+    Ctx& c = *g;
+    const size_t no = c.nbas * c.nfun, nc = c.lcic;
+    RkBufs& b = c.rk;
+    if (b.cap < no + nc) {
+      b.y0 = dalloc<cplx>(no + nc); b.yt = dalloc<cplx>(no + nc); b.k = dalloc<cplx>(no + nc); b.k2 = dalloc<cplx>(no + nc);
+      if (!b.lf_cur) { b.lf_cur = dalloc<double>(54); b.counter = dalloc<int>(2); }
+      b.cap = no + nc;
+    }
+    b.reset_orb = nullptr; b.reset_cic = nullptr;
+    Pulse pl;
+    pl.famp = std::sqrt(fint[j] / 3.50944506E+16); pl.freq = 1239.84190 / (wlen[j] * 27.2113845);
+    pl.period = 2 * PI / pl.freq; pl.numcyc = numcyc[j]; pl.cep = cep[j] / 180.0 * PI; pl.igauge = c.igauge;
+    static const double nodes[6] = {0.0, 0.5, 0.5, 1.0, 0.25, 0.75};
+    std::vector<double> tab((size_t)std::max(nstep, 1) * 54);
+    for (int s = 0; s < nstep; ++s)
+      for (int is = 0; is < 6; ++is) pulse_lfield(pl, t0[j] + dt[j] * s + dt[j] * nodes[is], &tab[(size_t)s * 54 + 9 * is]);
+    if ((size_t)c.field_cap < tab.size()) {
+      const size_t cap = std::max(tab.size(), (size_t)4096 * 54);
+      c.field_tab = dalloc<double>(cap);
+      c.field_cap = (long)cap;
+    }
+    cudaMemcpyAsync(c.field_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, c.st);
+    b.h_counter[0] = 0; b.h_counter[1] = nstep;
+    cudaMemcpyAsync(b.counter, b.h_counter, 2 * sizeof(int), cudaMemcpyHostToDevice, c.st);
+    // warm-up on a copy of the state: the one-body factors, scratch and kernel attributes
+    cudaMemcpyAsync(b.yt, d_wfn[j], no * sizeof(cplx), cudaMemcpyDeviceToDevice, c.st);
+    cudaMemcpyAsync(b.yt + no, d_cic[j], nc * sizeof(cplx), cudaMemcpyDeviceToDevice, c.st);
+    cudaMemcpyAsync(c.lfield, tab.data(), 9 * sizeof(double), cudaMemcpyHostToDevice, c.st);
+    rc |= h1_apply(c, false, c.lfield, b.yt, 0.5 * dt[j], mkc(0, 0), maxcyc, thresh);
+    rc |= run_htot(c, c.lfield, b.yt, b.yt + no, b.k, b.k + no, 1.0);
+    if (cudaStreamSynchronize(c.st) != cudaSuccess) rc |= ST_CUDA;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (!rc && nstep > 0) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(master, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = ST_CUDA;
+    for (int j = 0; j < njob && !rc; ++j) {
+      td1c_gpu_ctx_select(ids[j]);
+      Ctx& c = *g;
+      cudaEventRecord(evs[2 * j], master);
+      cudaStreamWaitEvent(c.st, evs[2 * j], 0);
+      rc |= split2_step(c, (cplx*)d_wfn[j], (cplx*)d_cic[j], dt[j], maxcyc, thresh, true);
+      cudaEventRecord(evs[2 * j + 1], c.st);
+      cudaStreamWaitEvent(master, evs[2 * j + 1], 0);
+    }
+    if (cudaStreamEndCapture(master, &graph) != cudaSuccess) rc |= ST_CUDA;
+    if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc |= ST_CUDA;
+    if (graph) cudaGraphDestroy(graph);
+  }
+  if (!rc && exec) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, master);
+    for (int s = 0; s < nstep && !rc; ++s)
+      if (cudaGraphLaunch(exec, master) != cudaSuccess) rc |= ST_CUDA;
+    cudaEventRecord(e1, master);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc |= ST_CUDA;
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  for (int j = 0; j < njob; ++j) {
+    td1c_gpu_ctx_select(ids[j]);
+    if (!g) continue;
+    Ctx& c = *g;
+    const size_t no = c.nbas * c.nfun, nc = c.lcic;
+    check_finite(c, d_wfn[j], 2 * no, c.st);
+    check_finite(c, d_cic[j], 2 * nc, c.st);
+    int dst = 0;
+    cudaMemcpyAsync(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.st);
+    if (cudaStreamSynchronize(c.st) != cudaSuccess) rc |= ST_CUDA;
+    c.status |= dst;
+    rc |= dst;
+  }
+  td1c_gpu_ctx_select(keep);
+  return rc;
 }
 
 int td1c_gpu_wait_selftest(void) {

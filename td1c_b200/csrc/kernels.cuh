@@ -28,6 +28,8 @@ struct LegGemmBatch {
 __host__ __device__ inline int legendre_lda(int k) { return (k + 31) / 32 * 32; }
 int launch_legendre_gemm(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair,
                          cudaStream_t st);
+int launch_legendre_gemm_mt(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair, int mt,
+                            cudaStream_t st);
 // the same transform in split TF32 on tcgen05 (FP32 accumulation, FP64 in and out);
 // a bounded wait that runs out sets ST_TIMEOUT in *status
 int launch_legendre_gemm_tf32(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair, int* status,
@@ -205,6 +207,7 @@ struct MfprodArgs {
   // tensor-core form of act2 (used when dmma != 0): its own padded
   // coefficient layout and map, per-target epilogue lists
   int dmma, nblk_d, ndcol, ncoef_d, nelist;
+  int max_cta;          // cap of the persistent DMMA grid (0: as many CTAs as are resident)
   const MfdBlock* dblk;
   const int2* dcol;       // (pair, conj) of every padded column
   const Act2Coef* dmap;   // den2 element -> padded coefficient slot

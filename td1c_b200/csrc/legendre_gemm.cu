@@ -154,9 +154,15 @@ static void lg_launch(const LegGemmBatch* d_batches, int nbatch, int M, int K, i
 
 int launch_legendre_gemm(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair,
                          cudaStream_t st) {
+  return launch_legendre_gemm_mt(d_batches, nbatch, M, K, N, pair, 0, st);
+}
+
+// mt: the CTA's m-tiles (3: 48 rows, 6: 96 rows); 0 chooses by M
+int launch_legendre_gemm_mt(const LegGemmBatch* d_batches, int nbatch, int M, int K, int N, bool pair, int mt,
+                            cudaStream_t st) {
   if (nbatch <= 0) return 0;
   if (N % 2) return (int)cudaErrorInvalidValue;  // slabs are complex: 16-byte pairs
-  if (M <= 48) {
+  if (mt == 3 || (mt != 6 && M <= 48)) {
     if (pair) lg_launch<3, true>(d_batches, nbatch, M, K, N, st);
     else lg_launch<3, false>(d_batches, nbatch, M, K, N, st);
   } else {

@@ -411,7 +411,9 @@ int launch_mfprod(const MfprodArgs& a, cudaStream_t st) {
       cps_smem = smem;
     }
     const int ntile = (int)((a.ngrid + MFD_TQ - 1) / MFD_TQ);
-    mfprod_dmma_kernel<<<(unsigned)std::min(ntile, cps * nsm), MFD_NT, smem, st>>>(a);
+    int grid = std::min(ntile, cps * nsm);
+    if (a.max_cta > 0) grid = std::min(grid, a.max_cta);
+    mfprod_dmma_kernel<<<(unsigned)grid, MFD_NT, smem, st>>>(a);
     return (int)cudaGetLastError();
   }
   return launch_mfprod_scalar(a, st);

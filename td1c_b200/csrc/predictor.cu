@@ -10,7 +10,7 @@
 // 1/2, 1/2, 1) from the history W_n, W_{n-1}, ...:
 //   c = 1:    W = sum_h w_h(u) W_{n-h}, h = 0..3, per unit u,
 //             w = (4, -6, 4, -1) (the cubic through the last four steps) + dw(u),
-//             dw from the network (per unit, from its Gram matrix);
+//             dw = 1e-3 x the network's output (per unit, from its Gram matrix);
 //   c = 1/2:  the cubic interpolant through n-2, n-1, n and the c = 1 value:
 //             W = 15/16 W_n - 5/16 W_{n-1} + 1/16 W_{n-2} + 5/16 W(c = 1);
 //   c = 0:    W_n itself.
@@ -33,6 +33,10 @@ namespace td1c {
 constexpr int LP_H = 4;      // history values a prediction combines
 constexpr int LP_SLOTS = 5;  // ring slots: the history plus the newest value
 constexpr int LP_NF = 32;    // network inputs per unit
+// the network's outputs are weight corrections in units of LP_DW (the cubic's
+// one-step error is ~1e-4 to 1e-6 of a unit's norm, so useful corrections are
+// small); each correction is limited to |dw| <= 1
+constexpr double LP_DW = 1e-3;
 
 __device__ __forceinline__ int lp_slot(int n, int h) { return ((n - h) % LP_SLOTS + LP_SLOTS) % LP_SLOTS; }
 
@@ -141,19 +145,38 @@ __global__ void lp_judge_kernel(LpArgs a) {
   }
 }
 
-// Network inputs of every unit from its Gram matrix (after the shift): the
-// correlations G_ij / sqrt(G_ii G_jj) (i < j, 12 reals), log(G_ii / G_00)
-// (3 reals), the element's position and the pair's kind; zero padding.
+// Network inputs of every unit from the Gram matrix of the four history
+// values the prediction combines (x_0 newest): in FP64, the Gram matrix of
+// the finite differences d_0 = x_0, d_1 = x_0 - x_1, d_2 = x_0 - 2 x_1 + x_2,
+// d_3 = x_0 - 3 x_1 + 3 x_2 - x_3 (the history's value, slope, curvature and
+// third difference), then log10 |d_1| / |d_0|, log10 |d_2| / |d_1|,
+// log10 |d_3| / |d_2| (scaled by 1/4), the correlations of (d_1, d_2),
+// (d_2, d_3), (d_1, d_3) (re, im), the element's position and the pair's
+// kind; zero padding to 32.
 __device__ void lp_feature_row(const cplx* G, int e, int nfe, int kind, float* x) {
-  const double d0 = fmax(G[0].x, 1e-300);
-  int k = 0;
-  for (int i = 0; i < LP_H; ++i)
-    for (int j = i + 1; j < LP_H; ++j) {
-      const double s = rsqrt(fmax(G[i * LP_H + i].x, 1e-300) * fmax(G[j * LP_H + j].x, 1e-300));
-      x[k++] = (float)(G[i * LP_H + j].x * s);
-      x[k++] = (float)(G[i * LP_H + j].y * s);
+  const double D[LP_H][LP_H] = {{1, 0, 0, 0}, {1, -1, 0, 0}, {1, -2, 1, 0}, {1, -3, 3, -1}};
+  cplx Gd[LP_H][LP_H];
+  for (int a = 0; a < LP_H; ++a)
+    for (int b = 0; b < LP_H; ++b) {
+      cplx v = mkc(0.0, 0.0);
+      for (int i = 0; i < LP_H; ++i)
+        for (int j = 0; j < LP_H; ++j) {
+          const double c = D[a][i] * D[b][j];
+          if (c != 0.0) { v.x += c * G[i * LP_H + j].x; v.y += c * G[i * LP_H + j].y; }
+        }
+      Gd[a][b] = v;
     }
-  for (int i = 1; i < LP_H; ++i) x[k++] = (float)log(fmax(G[i * LP_H + i].x, 1e-300) / d0);
+  double nrm[LP_H];
+  for (int a = 0; a < LP_H; ++a) nrm[a] = sqrt(fmax(Gd[a][a].x, 1e-300));
+  int k = 0;
+  for (int a = 1; a < LP_H; ++a) x[k++] = (float)(0.25 * fmax(log10(nrm[a] / nrm[a - 1]), -40.0));
+  const int pr[3][2] = {{1, 2}, {2, 3}, {1, 3}};
+  for (int q = 0; q < 3; ++q) {
+    const int a = pr[q][0], b = pr[q][1];
+    const double sc = 1.0 / (nrm[a] * nrm[b]);
+    x[k++] = (float)fmin(fmax(Gd[a][b].x * sc, -1.0), 1.0);
+    x[k++] = (float)fmin(fmax(Gd[a][b].y * sc, -1.0), 1.0);
+  }
   x[k++] = (float)((e + 0.5) / nfe);
   x[k++] = (float)(kind == 0);
   x[k++] = (float)(kind == 2);
@@ -167,15 +190,15 @@ __global__ void lp_features_kernel(LpArgs a) {
   lp_feature_row(a.gram + (size_t)u * LP_H * LP_H, e, a.nfe, a.pair_kind[p], a.feat + (size_t)u * LP_NF);
 }
 
-// weights of every unit for c = 1 from the network output dw (re, im per
-// history value) added to the cubic's; the correction is limited to |dw| <= 1
+// weights of every unit for c = 1: the cubic's plus LP_DW times the network
+// output (re, im per history value), each correction limited to |dw| <= 1
 __global__ void lp_weights_kernel(LpArgs a) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= a.nu) return;
   const double cub[LP_H] = {4.0, -6.0, 4.0, -1.0};
   for (int h = 0; h < LP_H; ++h) {
-    double dr = a.use_net ? (double)a.net_out[(size_t)u * 2 * LP_H + 2 * h] : 0.0;
-    double di = a.use_net ? (double)a.net_out[(size_t)u * 2 * LP_H + 2 * h + 1] : 0.0;
+    double dr = a.use_net ? LP_DW * a.net_out[(size_t)u * 2 * LP_H + 2 * h] : 0.0;
+    double di = a.use_net ? LP_DW * a.net_out[(size_t)u * 2 * LP_H + 2 * h + 1] : 0.0;
     dr = fmin(fmax(dr, -1.0), 1.0);
     di = fmin(fmax(di, -1.0), 1.0);
     a.weights[(size_t)u * LP_H + h] = mkc(cub[h] + dr, di);
@@ -276,8 +299,8 @@ __global__ void lp_loss_kernel(int n, const double* __restrict__ rec, const int*
   const double cub[LP_H] = {4.0, -6.0, 4.0, -1.0};
   cplx w[LP_H];
   for (int h = 0; h < LP_H; ++h) {
-    double dr = use_net ? (double)out[(size_t)s * 2 * LP_H + 2 * h] : 0.0;
-    double di = use_net ? (double)out[(size_t)s * 2 * LP_H + 2 * h + 1] : 0.0;
+    double dr = use_net ? LP_DW * out[(size_t)s * 2 * LP_H + 2 * h] : 0.0;
+    double di = use_net ? LP_DW * out[(size_t)s * 2 * LP_H + 2 * h + 1] : 0.0;
     w[h] = mkc(cub[h] + fmin(fmax(dr, -1.0), 1.0), fmin(fmax(di, -1.0), 1.0));
   }
   const double t = fmax(r[40], 1e-300);
@@ -288,11 +311,12 @@ __global__ void lp_loss_kernel(int n, const double* __restrict__ rec, const int*
     // err = w^H G w - 2 Re(w^H g) + t = Re(w^H (G w - g)) - Re(w^H g) + t
     err += w[a].x * gw.x + w[a].y * gw.y - (w[a].x * r[32 + 2 * a] + w[a].y * r[33 + 2 * a]);
     if (dy) {
-      // d/d Re w_a = 2 Re (G w - g)_a, d/d Im w_a = 2 Im (G w - g)_a; zero where the limit is active
-      const double dr = use_net ? (double)out[(size_t)s * 2 * LP_H + 2 * a] : 0.0;
-      const double di = use_net ? (double)out[(size_t)s * 2 * LP_H + 2 * a + 1] : 0.0;
-      dy[(size_t)s * 2 * LP_H + 2 * a] = fabs(dr) < 1.0 ? (float)(2.0 * gw.x / t / n) : 0.f;
-      dy[(size_t)s * 2 * LP_H + 2 * a + 1] = fabs(di) < 1.0 ? (float)(2.0 * gw.y / t / n) : 0.f;
+      // d/d Re w_a = 2 Re (G w - g)_a, d/d Im w_a = 2 Im (G w - g)_a, times LP_DW for the
+      // network output; zero where the limit is active
+      const double dr = use_net ? LP_DW * out[(size_t)s * 2 * LP_H + 2 * a] : 0.0;
+      const double di = use_net ? LP_DW * out[(size_t)s * 2 * LP_H + 2 * a + 1] : 0.0;
+      dy[(size_t)s * 2 * LP_H + 2 * a] = fabs(dr) < 1.0 ? (float)(LP_DW * 2.0 * gw.x / t / n) : 0.f;
+      dy[(size_t)s * 2 * LP_H + 2 * a + 1] = fabs(di) < 1.0 ? (float)(LP_DW * 2.0 * gw.y / t / n) : 0.f;
     }
   }
   loss[s] = fmax(err, 0.0) / t;

@@ -104,3 +104,104 @@ def gather(results, dist=None, dst=0):
                 raise ValueError("job %r ran on two ranks" % (k,))
         merged.update(p)
     return dict(sorted(merged.items()))
+
+
+# ---------------------------------------------------------------------------
+# the ensemble on one GPU: a context per job, one captured graph per step
+# ---------------------------------------------------------------------------
+class DeviceEnsemble:
+    """Independent jobs, each in a context of its own (own tables, buffers and streams), stepped
+    together by td1c_gpu_ensemble_split2: one CUDA graph per step holds one split2 step of every job.
+
+    tables(wl) -> (rad, ang) gives the grids and tables of a job (default: the package's builder);
+    state(h, wl) -> (orb, cic) its initial state (default: seeded, orthonormalised and relaxed in
+    imaginary time for relax_cycles ETD-RK2 cycles of relax_dt)."""
+
+    def __init__(self, jobs, tables=None, state=None, relax_cycles=40, relax_dt=0.01):
+        import torch
+        from . import basis
+        from .hprod import HProd
+        from .wfn import seeded_orbitals, seeded_cic
+        self.torch = torch
+        self.jobs = [dict(wl, split_type=1) for wl in jobs]
+        self.h, self.orb, self.cic = [], [], []
+        for wl in self.jobs:
+            rad, ang = tables(wl) if tables else basis.build(wl)
+            h = HProd(wl, rad, ang, new_context=True)
+            if state:
+                orb, cic = state(h, wl)
+                h.set_wfn0(orb, cic)
+            else:
+                d, tb = h.dims, h.ci_tables()
+                orb = seeded_orbitals(wl, rad["xrad"], rad["wrad"], rad["mask"])
+                cic = seeded_cic(wl, d["lcic"], tb["stra"], tb["strb"], tb["detoff"], tb["afirst"], tb["acount"])
+                h.set_wfn0(orb, cic)
+            y = torch.from_numpy(np.ascontiguousarray(orb).reshape(-1).copy()).cuda()
+            yc = torch.from_numpy(np.ascontiguousarray(cic).copy()).cuda()
+            if not state and relax_cycles:
+                h.set_time_kind(0)
+                h.orth_dev(y.data_ptr(), yc.data_ptr())
+                h.set_split(1)
+                h.relax_etdrk2_dev(y.data_ptr(), yc.data_ptr(), relax_dt, relax_cycles)
+                h.set_time_kind(1)
+            h.set_split(1)
+            self.h.append(h)
+            self.orb.append(y)
+            self.cic.append(yc)
+        torch.cuda.synchronize()
+
+    def _arrays(self, t0, orb, cic):
+        import ctypes
+        n = len(self.jobs)
+        ids = (ctypes.c_int * n)(*[h.ctx_id for h in self.h])
+        wf = (ctypes.c_void_p * n)(*[x.data_ptr() for x in orb])
+        ci = (ctypes.c_void_p * n)(*[x.data_ptr() for x in cic])
+        D = ctypes.c_double * n
+        t0s = D(*([t0] * n if np.isscalar(t0) else list(t0)))
+        dts = D(*[wl["dt"] for wl in self.jobs])
+        return ids, wf, ci, t0s, dts, D(*[wl["fint"] for wl in self.jobs]), D(*[wl["wlen"] for wl in self.jobs]), \
+            D(*[wl["numcyc"] for wl in self.jobs]), D(*[wl.get("cep", 0.0) for wl in self.jobs])
+
+    def run(self, nstep, t0=0.0, orb=None, cic=None, maxcyc=20, thresh=1e-10):
+        """nstep steps of every job together (in place on the job states, or on the given copies);
+        returns the device time in ms."""
+        import ctypes
+        orb = self.orb if orb is None else orb
+        cic = self.cic if cic is None else cic
+        ids, wf, ci, t0s, dts, fi, wv, nc, cp = self._arrays(t0, orb, cic)
+        ms = ctypes.c_double(0.0)
+        lib = self.h[0].lib._lib
+        self.torch.cuda.synchronize()
+        rc = lib.td1c_gpu_ensemble_split2(len(self.jobs), ids, wf, ci, t0s, dts, int(nstep), fi, wv, nc, cp, int(maxcyc),
+                                          float(thresh), ctypes.byref(ms))
+        if rc:
+            raise RuntimeError("td1c_gpu_ensemble_split2 failed (status %d)" % rc)
+        return ms.value
+
+    def run_sequential(self, nstep, t0=0.0, orb=None, cic=None, maxcyc=20, thresh=1e-10):
+        """The same steps job after job (each job's graph-captured split2 on its own stream); returns
+        the summed device time in ms."""
+        torch = self.torch
+        orb = self.orb if orb is None else orb
+        cic = self.cic if cic is None else cic
+        total = 0.0
+        for j, h in enumerate(self.h):
+            s = torch.cuda.ExternalStream(h.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(s)
+            h.split2_dev(orb[j].data_ptr(), cic[j].data_ptr(), t0 if np.isscalar(t0) else t0[j], self.jobs[j]["dt"], nstep,
+                         maxcyc=maxcyc, thresh=thresh)
+            e1.record(s)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        return total
+
+    def simulated_fs(self, nstep):
+        """Simulated time of nstep steps of every job, summed over the jobs (fs)."""
+        return sum(nstep * wl["dt"] for wl in self.jobs) * 0.02418884254
+
+    def final(self):
+        for h in self.h:
+            h.final()
+        self.h = []

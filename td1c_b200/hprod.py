@@ -27,12 +27,38 @@ class StatusError(RuntimeError):
     pass
 
 
-class HProd:
-    """One GPU RHS instance (the library holds a single context, like td1c's
-    clhprod singleton, clhprod.cpp:32-34)."""
+class _CtxLib:
+    """The library with a context selected before every call (the library's entry points act on its
+    current context; an ensemble holds one context per job)."""
 
-    def __init__(self, wl, rad, ang):
-        self.lib = _libmod.load()
+    def __init__(self, lib, ctx_id):
+        self._lib, self._id = lib, ctx_id
+
+    def __getattr__(self, name):
+        f = getattr(self._lib, name)
+        if name.startswith(("td1c_gpu_ctx_", "td1c_mlp_", "td1c_lp_", "td1c_gpu_ensemble")):
+            return f
+        lib, cid = self._lib, self._id
+
+        def call(*a):
+            lib.td1c_gpu_ctx_select(cid)
+            return f(*a)
+        return call
+
+
+class HProd:
+    """One GPU RHS instance.  The default one lives in the library's default context (the
+    drop-in entry points' context, like td1c's clhprod singleton, clhprod.cpp:32-34);
+    new_context=True gives it a context of its own (a job of an ensemble)."""
+
+    def __init__(self, wl, rad, ang, new_context=False):
+        raw = _libmod.load()
+        if new_context:
+            self.ctx_id = int(raw.td1c_gpu_ctx_create())
+        else:
+            self.ctx_id = 0
+            raw.td1c_gpu_ctx_select(0)
+        self.lib = _CtxLib(raw, self.ctx_id)
         self.wl = wl
         lib = self.lib
         orbs = wl["orbitals"]
@@ -339,6 +365,11 @@ class HProd:
         self._check(self.lib.td1c_gpu_set_learned(net.depth, net._sizes, net._ptrs(net.W), net._ptrs(net.b),
                                                   ctypes.c_void_p(net._pack.data_ptr()), 1 if use_net else 0, float(bound)))
 
+    def set_learned_policy(self, screen=True):
+        """screen=True: predicted windows only after a history-filling window whose judge values
+        pass the bound; False: after every such window (rolled back when rejected)."""
+        self._check(self.lib.td1c_gpu_set_learned_policy(1 if screen else 0))
+
     def split2_learned_dev(self, d_wfn, d_cic, t0, dt, nstep, maxcyc=20, thresh=1e-10):
         """Learned split2 steps in place; returns the judge statistics."""
         wl = self.wl
@@ -376,5 +407,16 @@ class HProd:
     def launch_count(self):
         return int(self.lib.td1c_gpu_launch_count())
 
+    def set_tuning(self, mt=0, mf_cap=0, i2_split=0):
+        """Launch shapes of this context: the FP64 Legendre GEMM's m-tiles (3 or 6; 0 by size), the
+        persistent mean-field grid cap and the int2e split (0: built-in)."""
+        self._check(self.lib.td1c_gpu_set_tuning(int(mt), int(mf_cap), int(i2_split)))
+
+    def get_tuning(self):
+        out = (ctypes.c_int * 4)()
+        self._check(self.lib.td1c_gpu_get_tuning(out))
+        return dict(mt=out[0], mf_cap=out[1], i2_split=out[2], i2_split_max=out[3])
+
     def final(self):
         self.lib.hprod_final_()
+        self.lib._lib.td1c_gpu_ctx_select(0)
