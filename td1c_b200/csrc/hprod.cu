@@ -3336,6 +3336,7 @@ int td1c_gpu_set_tuning(int mt, int mf_cap, int i2_split_) {
   if ((mt != 0 && mt != 3 && mt != 6) || mf_cap < 0 || i2_split_ < 0) return ST_CONFIG;
   c.tune_mt = mt; c.tune_mf_cap = mf_cap; c.tune_i2_split = i2_split_;
   for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }  // recaptured with the new shapes
+  c.lp_key_y = nullptr;  // and so are the learned form's steps
   return 0;
 }
 

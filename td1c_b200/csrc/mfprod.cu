@@ -182,6 +182,10 @@ __global__ void __launch_bounds__(MF_TQ) mfprod_kernel(MfprodArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int MFD_TQ = 32;              // points per CTA (4 n-tiles)
 constexpr int MFD_WP = MFD_TQ + 2;      // double2 pitch of a W row: rows 8 banks apart
+// double2 pitch of a D2V row: odd, so the 8 rows x 4 column pairs of one
+// fragment store fall on 8 different 16-byte bank groups (4 wavefronts, the
+// minimum for 512 bytes; a pitch of MFD_TQ put all 8 rows on one group)
+constexpr int MFD_DP = MFD_TQ + 1;
 constexpr int MFD_NT = 128;             // threads
 constexpr int MFD_MAXB = 16, MFD_MAXCOL = 256, MFD_MAXROW = 128, MFD_MAXE = 512;
 
@@ -198,7 +202,7 @@ __device__ __forceinline__ void mfd_cp16(void* dst, const void* src, unsigned by
 
 static size_t mfd_smem_bytes(const MfprodArgs& a) {
   return sizeof(cplx) * ((size_t)(a.npair + 1) * MFD_WP + (size_t)a.ncoef_d + 2 * (size_t)a.nfun * MFD_TQ +
-                         (size_t)a.nrow * MFD_TQ + (size_t)a.nact * MFD_TQ);
+                         (size_t)a.nrow * MFD_DP + (size_t)a.nact * MFD_TQ);
 }
 static bool mfd_fits(const MfprodArgs& a) {
   return a.dmma && a.nfun <= MF_MAXF && a.nblk_d <= MFD_MAXB && a.ndcol <= MFD_MAXCOL && a.nrow <= MFD_MAXROW &&
@@ -211,8 +215,8 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
   cplx* sW = mfd_smem;                                   // [npair + 1][WP]
   cplx* sC = sW + (size_t)(npair + 1) * MFD_WP;          // [ncoef_d]
   cplx* sPhi2 = sC + a.ncoef_d;                          // 2 x [nfun][TQ]: this tile's and the next
-  cplx* sD = sPhi2 + 2 * (size_t)nfun * MFD_TQ;          // [nrow][TQ]
-  cplx* sTw = sD + (size_t)a.nrow * MFD_TQ;              // [nact][TQ]
+  cplx* sD = sPhi2 + 2 * (size_t)nfun * MFD_TQ;          // [nrow][DP]
+  cplx* sTw = sD + (size_t)a.nrow * MFD_DP;              // [nact][TQ]
   __shared__ MfdBlock sblk[MFD_MAXB];
   __shared__ int2 scol[MFD_MAXCOL];
   __shared__ int2 sel[MFD_MAXE];
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
     if (r < B.nr) {
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        cplx* drow = sD + (size_t)(B.drow0 + r) * MFD_TQ + t * 8 + 2 * tig;
+        cplx* drow = sD + (size_t)(B.drow0 + r) * MFD_DP + t * 8 + 2 * tig;
         drow[0] = mkc(acc[t][0][0] + acc[t][1][0], acc[t][2][0] + acc[t][3][0]);
         drow[1] = mkc(acc[t][0][1] + acc[t][1][1], acc[t][2][1] + acc[t][3][1]);
       }
@@ -367,7 +371,7 @@ __global__ void __launch_bounds__(MFD_NT) mfprod_dmma_kernel(MfprodArgs a) {
     cplx tw = mkc(0, 0);
     for (int k = seoff[x]; k < seoff[x + 1]; ++k) {
       const int2 en = sel[k];
-      const cplx d = sD[(size_t)en.x * MFD_TQ + t];
+      const cplx d = sD[(size_t)en.x * MFD_DP + t];
       const cplx o = PHI(ncore + (en.y & 0xffff), t);
       tw = cadd(tw, cmul(o, (en.y >> 16) ? cconj(d) : d));
     }
