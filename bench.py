@@ -4,10 +4,11 @@ on one B200, learned+mixed against plain FP64, driven through the td1c_b200 C-AB
 
 Workload: Ne TD-CASSCF (1s frozen core + CAS(8e, 9o), FEDVR 60 x 21 points,
 rmax 120, lmax 47 / 94, velocity gauge, sin^2 800 nm 4-cycle 5e14 W/cm^2
-pulse, dt 0.004 au), complex128.  Start state: the committed relaxed state
-(td1c_b200/data/ne_tdcasscf_relaxed.npz, seeded orbitals and CI relaxed in
-imaginary time; td1c_b200/data/make_relaxed_state.py), read through the
-reference's .orb/.cic text format by both arms.
+pulse, dt 0.004 au), complex128; `--workload he` runs He TDHF instead.  Start
+state: the committed relaxed state of the workload (td1c_b200/data/*.npz,
+seeded orbitals and CI relaxed in imaginary time;
+td1c_b200/data/make_relaxed_state.py), read through the reference's .orb/.cic
+text format by both arms.
 
 A step is td1c's own propagation at this dt: tdse_split2 with clh1itr + clcrk
 and split_type 1 (a Crank-Nicolson one-body half step with the laser by
@@ -73,6 +74,9 @@ def parse():
     ap.add_argument("--full-pulse", action="store_true",
                     help="propagate the whole pulse with every arm; write profiles/full_pulse_<workload>.json")
     ap.add_argument("--nprint", type=int, default=100, help="steps between dipole samples of --full-pulse")
+    ap.add_argument("--sensitivity", default="",
+                    help="--full-pulse: also FP64 trajectories from the start state perturbed by these relative "
+                         "sizes (comma-separated, e.g. 1e-12,1e-9), to show how the dynamics amplify a perturbation")
     ap.add_argument("--ensemble", type=int, default=0, help="also step this many seeded jobs as one ensemble")
     return ap.parse_args()
 
@@ -204,25 +208,23 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
-STATE_FILE = os.path.join(ROOT, "td1c_b200", "data", "ne_tdcasscf_relaxed.npz")
-
-
 def committed_state(wl, nrad, lmax1, mmax1, nfun, lcic):
     """The committed relaxed start state of the workload, through the reference's .orb/.cic text
     format (written and read back, as a td1c restart would read it), or None when there is none."""
-    if not os.path.exists(STATE_FILE):
-        return None
     from td1c_b200 import wfnio
-    from td1c_b200.data.make_relaxed_state import load
-    orb, cic, info = load(STATE_FILE)
+    from td1c_b200.data.make_relaxed_state import load, path_for
+    path = path_for(wl["name"])
+    if path is None or not os.path.exists(path):
+        return None
+    orb, cic, info = load(path)
     if info["workload"] != wl["name"]:
         return None
     with tempfile.TemporaryDirectory() as d:
-        po, pc = os.path.join(d, "ne.orb"), os.path.join(d, "ne.cic")
+        po, pc = os.path.join(d, "state.orb"), os.path.join(d, "state.cic")
         wfnio.write_wfn(po, pc, orb, cic, nrad, lmax1, mmax1)
         orb2, cic2 = wfnio.read_wfn(po, pc, nrad, lmax1, nfun, lcic)
-    return np.asarray(orb2).reshape(nfun, -1), np.asarray(cic2), dict(info, source="committed relaxed state "
-                                                                      "(td1c_b200/data/ne_tdcasscf_relaxed.npz) via .orb/.cic")
+    src = "committed relaxed state (td1c_b200/data/%s) via .orb/.cic" % os.path.basename(path)
+    return np.asarray(orb2).reshape(nfun, -1), np.asarray(cic2), dict(info, source=src)
 
 
 def oracle_setup(wl, prop):
@@ -674,10 +676,20 @@ def full_pulse(args, h, wl, dt, arms, set_arm, steps, placed, deviations, torch,
     out = {"workload": wl["name"], "steps": nstep, "dt_au": dt, "simulated_fs": nstep * dt * AU2FS, "nprint": nprint,
            "bound": args.bound}
     dips, ends = {}, {}
-    for arm in arms:
-        set_arm(arm)
+    # FP64 trajectories from perturbed start states: seeded complex noise of relative size eps (of each
+    # orbital's largest component) on the nonzero components of the orbitals
+    pert = {"fp64_perturbed_%s" % e.strip(): float(e) for e in args.sensitivity.split(",") if e.strip()}
+    rng = np.random.default_rng(11)
+    for arm in list(arms) + list(pert):
+        set_arm("fp64" if arm in pert else arm)
         h.rk4_reset(None, None)
         yo, yc = placed(0.0)
+        if arm in pert:
+            o = yo.cpu().numpy().reshape(len(wl["orbitals"]), -1)
+            big = np.abs(o).max(axis=1, keepdims=True)
+            noise = rng.standard_normal(o.shape) + 1j * rng.standard_normal(o.shape)
+            o = o + pert[arm] * big * noise * (np.abs(o) > 0)
+            yo = torch.from_numpy(o.reshape(-1)).to(yo.device)
         dl, tl, jacc = [h.dipole_dev(yo.data_ptr(), yc.data_ptr())], [], {"accepted": 0, "rejected": 0, "steps_kept": 0}
         s = 0
         tot = 0.0
@@ -705,12 +717,14 @@ def full_pulse(args, h, wl, dt, arms, set_arm, steps, placed, deviations, torch,
         if arm == "learned":
             out[arm]["judge"] = jacc
     set_arm("fp64")
-    for arm in arms:
+    for arm in list(arms) + list(pert):
         if arm == "fp64":
             continue
         dd = np.abs(dips[arm] - dips["fp64"])
         dv = deviations(ends[arm][0], ends[arm][1], ends["fp64"][0], ends["fp64"][1])
         out[arm]["max_dipole_dev_au"] = float(dd.max())
+        over = np.nonzero(dd > 1e-5)[0]
+        out[arm]["first_t_au_dipole_dev_over_1e-5"] = float(min(over[0] * nprint, nstep) * dt) if over.size else None
         out[arm]["vs_fp64_at_end"] = dv
         out[arm]["gates"] = {"dipole_le_1e-5": bool(dd.max() <= 1e-5), "norm_le_1e-8": bool(dv["orbital_norm_dev"] <= 1e-8)}
     out["dipole_fp64_range_au"] = [float(dips["fp64"].min()), float(dips["fp64"].max())]

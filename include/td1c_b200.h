@@ -187,6 +187,13 @@ int td1c_gpu_set_mixed(int on);
  * out[0..2] = max |delta| / max |FP64 value| of the pair-density multipoles,
  * the pair potentials on the grid and hwfn.  lfield: host lfield(3,3). */
 int td1c_gpu_mixed_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
+/* The split-TF32 int2e of the mixed form on one RHS of a device state:
+ * out2[0] = max |delta| / max |value| between the tensor-core int2e and the
+ * FP64 DMMA int2e on the same (mixed) pair densities and potentials; out2[1]
+ * = the same between the mixed RHS's int2e and the FP64 RHS's.  16 (and
+ * out2 = -1) where the tensor-core plan does not apply (no active orbitals,
+ * more than 64 stored active pairs). */
+int td1c_gpu_mixed_int2e_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out2);
 /* Drop-in for hprod_dipole_ (include/wrapper.hpp:114, called by
  * clhprod::dipole, src/hprod/clhprod.cpp:218-222): host lfield(3,3), wfn,
  * cic; writes dip[3], vel[3], acc[3] (td1c_gpu_dipole3 on the library's
@@ -325,7 +332,9 @@ int td1c_gpu_ctx_destroy(int id); /* hprod_final_ of context id (>= 1); the defa
 /* launch shapes of the current context (0 = the built-in choice): mt the
  * FP64 Legendre GEMM's m-tiles per CTA (3 or 6), mf_cap the cap of the
  * persistent mean-field action grid, i2_split the K split of int2e (at most
- * the allocated split, get_tuning's out4[3]) */
+ * the allocated split, get_tuning's out4[3]); a negative i2_split runs int2e
+ * with split -i2_split (-1: the built-in split) on the main stream after the
+ * mean-field action instead of beside it on a side stream */
 int td1c_gpu_set_tuning(int mt, int mf_cap, int i2_split);
 int td1c_gpu_get_tuning(int* out4);
 /* nstep split2 steps (td1c_gpu_split2 with its mask) of njob jobs at once:

@@ -14,7 +14,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtd1c_b200.so")
 SOURCES = ["hprod.cu", "legendre_gemm.cu", "onebody.cu", "poisson.cu", "mfprod.cu", "reductions.cu", "ci.cu",
            "int2e_static.cu", "int2e_dmma.cu", "observables.cu", "h1prop.cu", "poisson_cond.cu",
-           "legendre_tf32.cu", "legendre_tc.cu", "mlp.cu",
+           "legendre_tf32.cu", "legendre_tc.cu", "int2e_tc.cu", "mlp.cu",
            "predictor.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -104,6 +104,8 @@ def load():
     lib.td1c_gpu_set_mixed.argtypes = [c_int]
     lib.td1c_gpu_mixed_selftest.restype = c_int
     lib.td1c_gpu_mixed_selftest.argtypes = [vp, vp, dp, dp]
+    lib.td1c_gpu_mixed_int2e_selftest.restype = c_int
+    lib.td1c_gpu_mixed_int2e_selftest.argtypes = [vp, vp, dp, dp]
     lib.hprod_dipole_.restype = None
     lib.hprod_dipole_.argtypes = [dp, dp, dp, dp, dp, dp]
     lib.td1c_gpu_int2e_static.restype = c_int
@@ -188,7 +190,7 @@ EXPORTED = [
     "td1c_gpu_last_status", "td1c_gpu_dims", "td1c_gpu_ci_tables", "td1c_gpu_energies",
     "td1c_gpu_htot_dev", "td1c_gpu_debug_get", "td1c_gpu_rk4", "td1c_gpu_sync", "td1c_gpu_launch_count",
     "td1c_gpu_stream", "td1c_gpu_profile", "td1c_gpu_rk4_reset", "td1c_gpu_int2e_static", "td1c_gpu_dipole",
-    "td1c_gpu_dipole3", "hprod_dipole_", "td1c_gpu_set_mixed", "td1c_gpu_mixed_selftest",
+    "td1c_gpu_dipole3", "hprod_dipole_", "td1c_gpu_set_mixed", "td1c_gpu_mixed_selftest", "td1c_gpu_mixed_int2e_selftest",
     "td1c_gpu_orth", "td1c_gpu_relax", "td1c_gpu_bind_split", "td1c_gpu_h1itr", "td1c_gpu_dpade",
     "td1c_gpu_split2", "td1c_gpu_etdrk2", "td1c_gpu_etdrk4", "td1c_gpu_relax_etdrk2",
     "h1itr_gen_cninv_", "h1itr_prop_", "dpade_gen_", "dpade_prod_",

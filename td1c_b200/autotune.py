@@ -10,7 +10,8 @@ the jobs compete for them.  The tuner therefore
   2. times whole ensemble steps (on copies of the states, so the jobs do not
      advance) for grid caps proportional to each job's share of the work
      (factor f of the SM count times the job's share; f = 0 is no cap) and
-     for int2e splits, and keeps the fastest.
+     for int2e splits (-1: int2e on the job's main stream after the mean-field
+     action instead of beside it), and keeps the fastest.
 The choice is returned (and written as JSON when a path is given) with the
 times it was based on.
 """
@@ -21,7 +22,7 @@ import numpy as np
 from .ensemble import cost
 
 
-def tune(ens, nstep=2, nsm=148, caps=(0.0, 2.0, 1.0, 0.5), splits=(0, 64, 32), path=None):
+def tune(ens, nstep=2, nsm=148, caps=(0.0, 2.0, 1.0, 0.5), splits=(0, 64, 32, -1), path=None):
     torch = ens.torch
     lf = np.zeros(9)
     choice = {"mt": [], "mf_cap_factor": None, "i2_split": None, "times_ms": {}}

@@ -150,6 +150,8 @@ struct Ctx {
   int i2_nsplit = 128;
   I2dArgs i2d{};          // int2e on the FP64 tensor cores
   bool i2_dmma = false;   // the DMMA plan fits in shared memory
+  I2tArgs i2t{};          // int2e in split TF32 on tcgen05 (mixed-precision form)
+  bool i2_tc = false;     // its plan fits (at most 64 stored active pairs)
   // act2 blocks
   int a2_nblk = 0, a2_nrow = 0, a2_ncol = 0, a2_ncoef = 0;
   Act2Block* a2_blk = nullptr; int2* a2_rows = nullptr; int2* a2_cols = nullptr;
@@ -1104,6 +1106,31 @@ int build_reductions(Ctx& c) {
     }
     c.i2.partial = dalloc<cplx>((size_t)c.i2_nsplit * std::max(1, c.i2.nblkent));
     d2.partial = reinterpret_cast<double*>(c.i2.partial);
+    // the split-TF32 plan: the stored active pairs in compact order and, per entry of the
+    // DMMA plan, its row pair, column pair and conjugation (the DMMA plan's choice)
+    if (c.i2_dmma) {
+      std::vector<int> cpair, compact(c.npair, -1);
+      for (int q = 0; q < c.npair; ++q)
+        if (c.pa[q] >= nc && c.pb[q] >= nc) { compact[q] = (int)cpair.size(); cpair.push_back(q); }
+      std::vector<int4> ent(dst2.size());
+      bool okp = !cpair.empty() && cpair.size() <= 64;
+      for (size_t e = 0; e < dst2.size() && okp; ++e) {
+        const int4 d4 = dst2[e];
+        int pr = -1, pc = -1, cj = 0;
+        for (int q = 0; q < c.npair; ++q) {
+          if (c.pa[q] == nc + d4.x && c.pb[q] == nc + d4.y) pr = q;
+          if (c.pa[q] == nc + d4.z && c.pb[q] == nc + d4.w) { pc = q; cj = 0; }
+          if (c.pa[q] == nc + d4.w && c.pb[q] == nc + d4.z) { pc = q; cj = 1; }
+        }
+        if (pr < 0 || pc < 0 || compact[pr] < 0 || compact[pc] < 0) { okp = false; break; }
+        ent[e] = make_int4(compact[pr], compact[pc], cj, 0);
+      }
+      I2tArgs& t = c.i2t;
+      t.P = (int)cpair.size(); t.NB = (t.P + 15) / 16 * 16; t.K = c.nbas2; t.nent = (int)ent.size();
+      t.rho2 = c.rho2; t.v2sph = c.v2sph; t.partial = c.i2.partial; t.status = c.d_status;
+      c.i2_tc = okp && int2e_tc_fits(t);
+      if (c.i2_tc) { t.pair = dupload(cpair); t.ent = dupload(ent); }
+    }
   }
   // act2 dense blocks: rows ij (i >= j, m_i - m_j = d) in the reference's
   // (i outer, j inner) order, columns kl (m_l - m_k = d) in (k outer, l inner)
@@ -1337,7 +1364,16 @@ int gemm(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
   return launch_legendre_gemm_mt(b, nb, M, K, 2 * c.Nr, pair, c.tune_mt, c.st);
 }
 // the int2e K split: the tuned value where one is set (at most the allocated split)
-int i2_split(const Ctx& c) { return c.tune_i2_split > 0 ? std::min(c.tune_i2_split, c.i2_nsplit) : c.i2_nsplit; }
+int i2_split(const Ctx& c) {
+  const int k = c.tune_i2_split < 0 ? -c.tune_i2_split : c.tune_i2_split;
+  return k > 1 || (k == 1 && c.tune_i2_split > 0) ? std::min(k, c.i2_nsplit) : c.i2_nsplit;
+}
+// int2e: split TF32 on tcgen05 in the mixed-precision form, else FP64 DMMA (or the FFMA blocks)
+int int2e_run(Ctx& c, cudaStream_t s) {
+  if (c.mixed && c.i2_tc) return launch_int2e_tc(c.i2t, c.i2, i2_split(c), s);
+  if (c.i2_dmma) return launch_int2e_dmma(c.i2d, c.i2, i2_split(c), s);
+  return launch_int2e(c.i2, i2_split(c), s);
+}
 int mfprod_run(Ctx& c, cudaStream_t st) {
   MfprodArgs m = c.mf;
   m.max_cta = c.tune_mf_cap;
@@ -1461,11 +1497,12 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     // int2e needs only rho2 and v2sph: third stream, overlapping l->theta,
     // mfprod and the theta->l transforms; then the CI T vectors, which need
     // only int2e and the D vectors of the CI chain; joins before smallmat
-    if (c.nact > 0) {
+    // (a negative tuned split keeps int2e on the main stream, after the mean-field action:
+    // its one-CTA-per-SM grid then does not hold the SMs the transforms and mfprod need)
+    if (c.nact > 0 && c.tune_i2_split >= 0) {
       cudaEventRecord(c.ev_i2_fork, st);
       cudaStreamWaitEvent(c.st3, c.ev_i2_fork, 0);
-      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, i2_split(c), c.st3));
-      else rc |= chk("int2e", launch_int2e(c.i2, i2_split(c), c.st3));
+      rc |= chk("int2e", int2e_run(c, c.st3));
       cudaStreamWaitEvent(c.st3, c.ev_join, 0);
       rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, c.st3));
       cudaEventRecord(c.ev_i2_join, c.st3);
@@ -1494,8 +1531,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
     cudaStreamWaitEvent(st, c.ev_i2_join, 0);
   } else if (c.nact > 0) {
     if (!c.mf_external || c.npair == 0) {
-      if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, i2_split(c), st));
-      else rc |= chk("int2e", launch_int2e(c.i2, i2_split(c), st));
+      rc |= chk("int2e", int2e_run(c, st));
       c.launches += 3;
     }
     rc |= chk("ci tvec", launch_ci_tvec(ca, c.maxsec, st));  // the CI chain joined before mfprod
@@ -2087,6 +2123,7 @@ int etdrk4_step(Ctx& c, cplx* y_orb, cplx* y_cic, double dt, int maxcyc, double 
 // history of exact step-start mean fields (predictor.cu)
 // ---------------------------------------------------------------------------
 int lp_setup(Ctx& c) {
+  if (mlp_infer_prepare()) return ST_CUDA;
   if (c.lp_alloc) return 0;
   if (c.npair < 1 || c.nfe < 1) return ST_CONFIG;
   LpArgs& a = c.lp;
@@ -2139,8 +2176,7 @@ int run_meanfield(Ctx& c, const cplx* wfn, const double* d_lf) {
   c.launches += 3;
   rc |= chk("W gemm", gemm_mf(c, c.b_W, c.npair, c.nlat, c.L2, false));
   if (c.nact > 0) {
-    if (c.i2_dmma) rc |= chk("int2e", launch_int2e_dmma(c.i2d, c.i2, i2_split(c), st));
-    else rc |= chk("int2e", launch_int2e(c.i2, i2_split(c), st));
+    rc |= chk("int2e", int2e_run(c, st));
     c.launches += 3;
   }
   return rc;
@@ -2296,7 +2332,7 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
       if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
       rc |= step();
       if (cudaStreamEndCapture(st, &graph) != cudaSuccess) return ST_CUDA;
-      if (cudaGraphInstantiate(&ge, graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
+      if (cudaGraphInstantiate(&ge, graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
       cudaGraphDestroy(graph);
       const long per_step = c.launches - l0;
       c.launches = l0;
@@ -2337,6 +2373,19 @@ int prop_run(int kind, void* d_wfn, void* d_cic, double t0, double dt, int nstep
 // value of an accepted window; smallest and largest window judge value seen;
 // predicted steps kept; last window judge value; steps run.
 constexpr int LP_WIN = 8;
+// The streams of a context. The main stream (and the one-body correction loop's
+// body stream) carry the critical path of a step: transforms, Poisson solve,
+// mean-field action, integrals, one-body cycles. The side streams carry work that
+// only has to be done by a later join (the CI chain, the one-body stencil, int2e
+// and the CI T vectors, the sigma vector): they get the lowest priority, so their
+// blocks take the SMs the main path leaves free. Captured graphs keep these
+// priorities per node (instantiated with cudaGraphInstantiateFlagUseNodePriority).
+void make_stream(cudaStream_t* q, bool main) {
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) least = greatest = 0;
+  cudaStreamCreateWithPriority(q, cudaStreamNonBlocking, main ? greatest : least);
+}
+
 int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc, double cep,
                 int maxcyc, double thresh, double* record, double* stats) {
   Ctx& c = ctx();
@@ -2400,25 +2449,33 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
     cudaStreamSynchronize(st);  // lf lives on this frame
     return lp_j(c, y, c.lfield);
   };
-  // one step of the given kind: eager the first time (factor set-up), then a
-  // captured graph, kept for later calls with the same inputs
-  bool warm[3] = {false, false, false};
+  // one step of the given kind: the first step after the graphs were dropped runs eagerly (the
+  // first-call set-up: one-body factors, scratch, kernel attributes); the next one captures every
+  // kind the call can use (exact, exact + judge, predicted), so that no capture falls inside a
+  // later window. The graphs are kept for later calls with the same inputs.
+  bool warm = c.lp_exec[0] || c.lp_exec[1] || c.lp_exec[2];
+  auto capture = [&](int kind) -> int {
+    cudaGraphExec_t& ge = c.lp_exec[kind];
+    const long l0 = c.launches;
+    cudaGraph_t graph;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
+    int r = lp_step(c, kind, y, yc, dt, maxcyc, thresh);
+    if (cudaStreamEndCapture(st, &graph) != cudaSuccess || r) return ST_CUDA;
+    if (cudaGraphInstantiate(&ge, graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
+    cudaGraphDestroy(graph);
+    c.lp_exec_launch[kind] = c.launches - l0;
+    c.launches = l0;
+    return 0;
+  };
   auto step = [&](int kind) -> int {
     cudaGraphExec_t& ge = c.lp_exec[kind];
-    if (!ge && !warm[kind]) {
-      warm[kind] = true;
-      return lp_step(c, kind, y, yc, dt, maxcyc, thresh);  // eager: first-call set-up happens here
+    if (!ge && !warm) {
+      warm = true;
+      return lp_step(c, kind, y, yc, dt, maxcyc, thresh);
     }
     if (!ge) {
-      const long l0 = c.launches;
-      cudaGraph_t graph;
-      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return ST_CUDA;
-      int r = lp_step(c, kind, y, yc, dt, maxcyc, thresh);
-      if (cudaStreamEndCapture(st, &graph) != cudaSuccess || r) return ST_CUDA;
-      if (cudaGraphInstantiate(&ge, graph, 0) != cudaSuccess) { cudaGraphDestroy(graph); return ST_CUDA; }
-      cudaGraphDestroy(graph);
-      c.lp_exec_launch[kind] = c.launches - l0;
-      c.launches = l0;
+      for (int k = record ? kind : 0; k <= (record ? kind : 2); ++k)
+        if (!c.lp_exec[k] && capture(k)) return ST_CUDA;
     }
     if (cudaGraphLaunch(ge, st) != cudaSuccess) return ST_CUDA;
     c.launches += c.lp_exec_launch[kind];
@@ -2591,15 +2648,15 @@ void hprod_init_(void) {
   // (td1c_gpu_stream) beyond hprod_final_
   static cudaStream_t lib_stream = nullptr, lib_stream2 = nullptr, lib_stream3 = nullptr, lib_stream4 = nullptr;
   if (g_cur == 0) {
-    if (!lib_stream4) cudaStreamCreateWithFlags(&lib_stream4, cudaStreamNonBlocking);
-    if (!lib_stream) cudaStreamCreateWithFlags(&lib_stream, cudaStreamNonBlocking);
-    if (!lib_stream2) cudaStreamCreateWithFlags(&lib_stream2, cudaStreamNonBlocking);
-    if (!lib_stream3) cudaStreamCreateWithFlags(&lib_stream3, cudaStreamNonBlocking);
+    if (!lib_stream4) make_stream(&lib_stream4, true);
+    if (!lib_stream) make_stream(&lib_stream, true);
+    if (!lib_stream2) make_stream(&lib_stream2, false);
+    if (!lib_stream3) make_stream(&lib_stream3, false);
     c.st = lib_stream; c.st2 = lib_stream2; c.st3 = lib_stream3; c.st4 = lib_stream4;
   } else if (!c.st) {
     // an ensemble job: its own streams, so that a graph captured over several
     // jobs (forked from one stream) has no edges between them
-    for (cudaStream_t* q : {&c.st, &c.st2, &c.st3, &c.st4}) cudaStreamCreateWithFlags(q, cudaStreamNonBlocking);
+    make_stream(&c.st, true); make_stream(&c.st2, false); make_stream(&c.st3, false); make_stream(&c.st4, true);
     c.own_streams = true;
   }
   for (cudaEvent_t* e : {&c.ev_fork, &c.ev_join, &c.ev_ob_fork, &c.ev_ob_join, &c.ev_i2_fork, &c.ev_i2_join,
@@ -3207,6 +3264,47 @@ int td1c_gpu_mixed_selftest(const void* d_wfn, const void* d_cic, const double* 
   return 0;
 }
 
+int td1c_gpu_mixed_int2e_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out2) {
+  Ctx& c = ctx();
+  if (!c.initialized || !out2 || !lfield) return ST_CONFIG;
+  out2[0] = out2[1] = -1.0;
+  if (!c.i2_tc || c.nact == 0) return ST_CONFIG;
+  cudaStream_t st = c.st;
+  if (!c.dip_lfd) c.dip_lfd = dalloc<double>(9);
+  cudaMemcpyAsync(c.dip_lfd, lfield, 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+  const size_t n4 = (size_t)c.nact * c.nact * c.nact * c.nact;
+  std::vector<std::complex<double>> i2[3];
+  const int keep = c.mixed;
+  build_tc_plans(c);
+  int rc = 0;
+  for (int k = 0; k < 3; ++k) {
+    if (k < 2) {
+      c.mixed = k ? std::max(keep, 1) : 0;
+      rc |= run_htot(c, c.dip_lfd, (const cplx*)d_wfn, (const cplx*)d_cic, c.hwfn_io, c.hcic_io, 1.0);
+    } else {
+      // the FP64 DMMA kernel on the mixed RHS's own pair densities and potentials
+      rc |= launch_int2e_dmma(c.i2d, c.i2, i2_split(c), st);
+    }
+    i2[k].resize(n4);
+    cudaMemcpyAsync(i2[k].data(), c.int2e, n4 * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc |= ST_CUDA;
+  }
+  c.mixed = keep;
+  if (rc) return ST_CUDA;
+  int dst = 0;
+  cudaMemcpy(&dst, c.d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  c.status |= dst;
+  if (dst & ST_TIMEOUT) return ST_TIMEOUT;
+  auto rel = [](const std::vector<std::complex<double>>& a, const std::vector<std::complex<double>>& b) {
+    double d = 0.0, m = 0.0;
+    for (size_t k = 0; k < a.size(); ++k) { d = std::max(d, std::abs(b[k] - a[k])); m = std::max(m, std::abs(a[k])); }
+    return m > 0.0 ? d / m : d;
+  };
+  out2[0] = rel(i2[2], i2[1]);  // tensor-core kernel against DMMA on the same inputs
+  out2[1] = rel(i2[0], i2[1]);  // mixed RHS against the FP64 RHS
+  return 0;
+}
+
 int td1c_gpu_profile(int reps, double dtime, const double* lfield, const void* d_wfn, const void* d_cic, void* d_hwfn,
                      void* d_hcic, double* ms, char* names, int names_cap) {
   Ctx& c = ctx();
@@ -3333,7 +3431,7 @@ int td1c_gpu_ctx_destroy(int id) {
 
 int td1c_gpu_set_tuning(int mt, int mf_cap, int i2_split_) {
   Ctx& c = ctx();
-  if ((mt != 0 && mt != 3 && mt != 6) || mf_cap < 0 || i2_split_ < 0) return ST_CONFIG;
+  if ((mt != 0 && mt != 3 && mt != 6) || mf_cap < 0) return ST_CONFIG;
   c.tune_mt = mt; c.tune_mf_cap = mf_cap; c.tune_i2_split = i2_split_;
   for (auto& ge : c.graph_exec) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }  // recaptured with the new shapes
   c.lp_key_y = nullptr;  // and so are the learned form's steps
@@ -3359,7 +3457,7 @@ int td1c_gpu_ensemble_split2(int njob, const int* ids, void* const* d_wfn, void*
   const int keep = g_cur;
   static cudaStream_t master = nullptr;
   static std::vector<cudaEvent_t> evs;
-  if (!master) cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking);
+  if (!master) make_stream(&master, true);
   while ((int)evs.size() < 2 * njob + 2) {
     cudaEvent_t e;
     cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -3415,7 +3513,7 @@ int td1c_gpu_ensemble_split2(int njob, const int* ids, void* const* d_wfn, void*
       cudaStreamWaitEvent(master, evs[2 * j + 1], 0);
     }
     if (cudaStreamEndCapture(master, &graph) != cudaSuccess) rc |= ST_CUDA;
-    if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc |= ST_CUDA;
+    if (!rc && cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) rc |= ST_CUDA;
     if (graph) cudaGraphDestroy(graph);
   }
   if (!rc && exec) {

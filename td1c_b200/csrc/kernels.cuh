@@ -93,6 +93,7 @@ struct MlpInferArgs {
   const unsigned short* wbf16[MLP_MAXDEPTH];  // BF16 weight planes (tensor-core layout)
 };
 int launch_mlp_infer_bf16(const MlpInferArgs& a, cudaStream_t st);
+int mlp_infer_prepare();
 
 // ---- one-body: tprod + zprod/pzprod (hprod_tprod.F90, hprod_zprod.F90, hprod_pzprod.F90)
 struct OneBodyArgs {

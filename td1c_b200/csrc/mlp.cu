@@ -277,12 +277,22 @@ __global__ void __launch_bounds__(MI_THREADS, 1) mlp_infer_bf16_kernel(MlpInferA
 
 int mlp_infer_smem() { return MI_MAXW * MI_MAXW * 2 + MI_BM * MI_MAXW * 2 + (int)sizeof(MiShared) + 16; }
 
+// The kernel's shared-memory opt-in, once per device; callers that capture the
+// launch into a graph call this before the capture.
+int mlp_infer_prepare() {
+  static bool attr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ST_CUDA;
+  if (dev >= 0 && dev < 64 && attr[dev]) return 0;
+  if (cudaFuncSetAttribute(mlp_infer_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp_infer_smem()) !=
+      cudaSuccess)
+    return ST_CUDA;
+  if (dev >= 0 && dev < 64) attr[dev] = true;
+  return 0;
+}
+
 int launch_mlp_infer_bf16(const MlpInferArgs& a, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(mlp_infer_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp_infer_smem());
-    attr = true;
-  }
+  if (mlp_infer_prepare()) return (int)cudaErrorInvalidValue;
   const int ntile = (a.rows + MI_BM - 1) / MI_BM;
   if (ntile > 0) mlp_infer_bf16_kernel<<<ntile, MI_THREADS, mlp_infer_smem(), st>>>(a);
   return (int)cudaGetLastError();

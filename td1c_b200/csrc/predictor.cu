@@ -253,7 +253,7 @@ __global__ void lp_int2e_kernel(LpArgs a, int mode) {
 }
 
 int launch_lp_push_judge(const LpArgs& a, cudaStream_t st) {
-  lp_int2e_kernel<<<(a.ni + 255) / 256, 256, 0, st>>>(a, 0);
+  if (a.ni > 0) lp_int2e_kernel<<<(a.ni + 255) / 256, 256, 0, st>>>(a, 0);  // no active orbitals: no int2e
   lp_push_kernel<<<a.nu, 256, 0, st>>>(a);
   lp_judge_kernel<<<1, 256, 0, st>>>(a);
   return (int)cudaGetLastError();
@@ -268,7 +268,7 @@ int launch_lp_weights(const LpArgs& a, cudaStream_t st) {
 }
 int launch_lp_stage(const LpArgs& a, int half, cudaStream_t st) {
   lp_apply_kernel<<<148 * 8, 256, 0, st>>>(a, half);
-  lp_int2e_kernel<<<(a.ni + 255) / 256, 256, 0, st>>>(a, half ? 2 : 1);
+  if (a.ni > 0) lp_int2e_kernel<<<(a.ni + 255) / 256, 256, 0, st>>>(a, half ? 2 : 1);
   return (int)cudaGetLastError();
 }
 

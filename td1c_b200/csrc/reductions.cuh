@@ -54,4 +54,22 @@ size_t int2e_dmma_smem(const I2dArgs& a);
 bool int2e_dmma_fits(const I2dArgs& a);
 int launch_int2e_dmma(const I2dArgs& d, const Int2eArgs& sum, int nsplit, cudaStream_t st);
 
+// int2e in split TF32 on tcgen05 (the mixed-precision form): every product of
+// the P stored active pairs in one 128 x 2NB GEMM per K slice, entries formed
+// from it per CTA (the same entry list and partial layout as the DMMA plan).
+struct I2tArgs {
+  int P, NB;             // stored active pairs (<= 64); B rows per part (>= P, multiple of 16)
+  size_t K;
+  const int* pair;       // [P] stored pair index of compact pair p
+  const int4* ent;       // [nent] (row pair, column pair, conjugated column, 0) of each entry
+  int nent;
+  const cplx* rho2;
+  const cplx* v2sph;
+  cplx* partial;         // [nsplit][nent]
+  int* status;
+};
+size_t int2e_tc_smem(const I2tArgs& a);
+bool int2e_tc_fits(const I2tArgs& a);
+int launch_int2e_tc(const I2tArgs& t, const Int2eArgs& sum, int nsplit, cudaStream_t st);
+
 }  // namespace td1c

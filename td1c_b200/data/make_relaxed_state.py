@@ -1,6 +1,7 @@
-"""Make the relaxed Ne TD-CASSCF start state of the benchmark (runs on a GPU).
+"""Make the relaxed start states of the benchmark workloads (runs on a GPU).
 
-The seeded orbitals and CI vector of the Ne workload (Philox, td1c_b200.wfn)
+The seeded orbitals and CI vector of a workload (Philox, td1c_b200.wfn; Ne
+TD-CASSCF or He TDHF)
 are orthonormalised and relaxed in imaginary time with ETD-RK2 steps
 (init_prop12 with cletdrk2: 300 cycles of dt = 0.01 au) on the GPU, then
 stored compactly: float32 real and imaginary parts, components below 1e-9 of
@@ -8,7 +9,7 @@ the orbital's largest dropped (sparse index list), CI in float64.  Both arms of
 the benchmark load this file (through the reference's .orb/.cic text format),
 so the CPU reference and the GPU start from the same numbers.
 
-    python td1c_b200/data/make_relaxed_state.py [out.npz]
+    python td1c_b200/data/make_relaxed_state.py [ne|he] [out.npz]
 """
 import os
 import sys
@@ -20,14 +21,25 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 CYCLES, DT, DROP = 300, 0.01, 1e-9
 PATH = os.path.join(HERE, "ne_tdcasscf_relaxed.npz")
+PATHS = {"ne": PATH, "he": os.path.join(HERE, "he_tdhf_relaxed.npz")}
 
 
-def main(out=PATH):
+def path_for(workload_name):
+    """The committed state file of a workload (by its td1c_b200.workloads name), or None."""
+    from td1c_b200 import workloads as W
+    for key, wl in (("ne", W.NE_CAS), ("he", W.HE_TDHF)):
+        if wl["name"] == workload_name:
+            return PATHS[key]
+    return None
+
+
+def main(which="ne", out=None):
     import torch
     from td1c_b200 import basis, workloads as W
     from td1c_b200.hprod import HProd
     from td1c_b200.wfn import seeded_orbitals, seeded_cic
-    wl = dict(W.NE_CAS, split_type=1)
+    out = out or PATHS[which]
+    wl = dict({"ne": W.NE_CAS, "he": W.HE_TDHF}[which], split_type=1)
     rad, ang = basis.build(wl)
     h = HProd(wl, rad, ang)
     d = h.dims
@@ -63,4 +75,4 @@ def load(path=PATH):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:2])
+    main(*sys.argv[1:3])

@@ -30,15 +30,19 @@ ELEMENT_AU = 2.0
 def job(lmax1, nfe, nact, fint, wlen, cep, jid=0):
     """The workload of one ensemble job (same keys as td1c_b200.workloads)."""
     rmax = ELEMENT_AU * nfe
+    mtot = 0
     if nact == 1:
         orbitals, znuc, nel = [(1, 0, 0, 0)], 2.0, 2
     else:
         orbitals = [(1, 0, 0, -1)] + [s + (1,) for s in ACTIVE_SHELLS[:nact]]
         nel = 2 + min(8, 2 * nact)
         znuc = float(nel)
+        if 2 * nact <= 8:
+            # every active orbital doubly occupied: the one determinant has M = 2 sum(m)
+            mtot = 2 * sum(s[2] for s in ACTIVE_SHELLS[:nact])
     return dict(name="ensemble_job%03d_lmax%d_nfe%d_nact%d" % (jid, lmax1, nfe, nact), znuc=znuc, rmin=0.0, rmax=rmax,
                 ndvr=NDVR, nfe=nfe, lmax1=lmax1, lmax2=2 * lmax1, nlat=0, orbitals=orbitals, nela=nel // 2,
-                nelb=nel // 2, mtot=0, smul=1, igauge=1, icomp=1, rmask=0.8 * rmax, mask_cos_order=4.0, fint=fint,
+                nelb=nel // 2, mtot=mtot, smul=1, igauge=1, icomp=1, rmask=0.8 * rmax, mask_cos_order=4.0, fint=fint,
                 wlen=wlen, numcyc=3.0, cep=cep, dt=0.004, seed=1000 + jid)
 
 

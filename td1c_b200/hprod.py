@@ -197,6 +197,18 @@ class HProd:
         self._check(self.lib.td1c_gpu_mixed_selftest(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(lf), _dp(out)))
         return out
 
+    def mixed_int2e_selftest(self, d_wfn, d_cic, lfield):
+        """The mixed form's tensor-core int2e on one RHS: (relative deviation from the FP64 DMMA
+        int2e on the same pair densities and potentials, from the FP64 RHS's int2e), or None where
+        the tensor-core plan does not apply."""
+        out = np.zeros(2)
+        lf = np.ascontiguousarray(lfield, dtype=np.float64)
+        rc = self.lib.td1c_gpu_mixed_int2e_selftest(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic), _dp(lf), _dp(out))
+        if rc == 16:
+            return None
+        self._check(rc)
+        return out
+
     def orth_dev(self, d_wfn, d_cic):
         """wfn_orth_cic + wfn_orth_orb in place on device buffers."""
         self._check(self.lib.td1c_gpu_orth(ctypes.c_void_p(d_wfn), ctypes.c_void_p(d_cic)))

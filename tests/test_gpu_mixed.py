@@ -121,3 +121,37 @@ def test_persistent_and_per_tile_kernels_agree(cuda_ok, base):
         assert h.lib.td1c_gpu_last_status() == 0
     finally:
         h.final()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.NE_SMALL, W.MIXED_SMALL, W.NE_CAS], ids=lambda w: w["name"])
+def test_mixed_int2e_tensor_cores(cuda_ok, base):
+    """The mixed form's int2e in split TF32 on tcgen05: on the same pair densities and potentials
+    it matches the FP64 DMMA kernel to FP32 accumulation (1e-6 of the largest integral), and the
+    mixed RHS's int2e stays within 2e-6 of the FP64 RHS's; the full-size Ne configuration too."""
+    import torch
+    from td1c_b200 import basis
+    from td1c_b200.hprod import HProd
+    from td1c_b200.wfn import seeded_orbitals, seeded_cic
+    if base is W.NE_CAS:
+        wl = dict(base, split_type=1)
+        rad, ang = basis.build(wl)
+        h = HProd(wl, rad, ang)
+        tb = h.ci_tables()
+        orb = seeded_orbitals(wl, rad["xrad"], rad["wrad"], rad["mask"])
+        cic = seeded_cic(wl, h.dims["lcic"], tb["stra"], tb["strb"], tb["detoff"], tb["afirst"], tb["acount"])
+        h.set_wfn0(orb, cic)
+        lf = h.pulse_lfield(100.0)
+    else:
+        o, h, wl, orb, cic = _setup(base)
+        lf = o.field(30.0)
+    try:
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        dev = h.mixed_int2e_selftest(d_orb.data_ptr(), d_cic.data_ptr(), lf)
+        assert dev is not None
+        assert 0.0 < dev[0] < 1e-6, dev
+        assert dev[1] < 2e-6, dev
+        assert h.last_status() == 0
+    finally:
+        h.final()

@@ -218,3 +218,47 @@ def test_full_size_split2(cuda_ok):
         assert abs(np.linalg.norm(cg) - 1.0) < 1e-2
     finally:
         h.final()
+
+
+@pytest.mark.gpu
+def test_full_size_split2_peak_relaxed(cuda_ok):
+    """Ne TD-CASSCF from the committed relaxed state, 12 split2 steps at dt = 0.004 starting at the
+    |A(t)| maximum of the pulse (the most one-body correction cycles): state and the dipole after
+    every step against the oracle, 1e-10 relative."""
+    import torch
+    from td1c_b200.data.make_relaxed_state import load
+    from oracle.oracle import Oracle
+    from td1c_b200.hprod import HProd
+    wl = dict(W.NE_CAS, split_type=1)
+    o = Oracle(wl)
+    o.set_split(1)
+    rad, ang = oracle_tables(o)
+    h = HProd(wl, rad, ang)
+    try:
+        orb, cic, info = load()
+        assert info["workload"] == wl["name"]
+        # set_wfn0 once (the oracle, like hprod_addfc_tmat, adds the frozen-core potential to tmat)
+        o.set_wfn0(orb, cic)
+        h.set_wfn0(orb, cic)
+        freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+        period = wl["numcyc"] * 2 * np.pi / freq
+        ts = np.linspace(0.3 * period, 0.7 * period, 4001)
+        amp = [abs(h.pulse_lfield(t)[2]) for t in ts]
+        t0 = float(ts[int(np.argmax(amp))])
+        dt, nstep = 0.004, 12
+        wo, co, dip = o.split2(orb, cic, t0, dt, nstep)
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        h.rk4_reset(None, None)
+        dip_g = []
+        for s in range(nstep):
+            h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), t0 + s * dt, dt, 1)
+            dip_g.append(h.dipole_dev(d_orb.data_ptr(), d_cic.data_ptr()))
+        h.sync()
+        assert h.last_status() == 0
+        assert rel_err(d_orb.cpu().numpy(), wo.reshape(-1)) < TOL, rel_err(d_orb.cpu().numpy(), wo.reshape(-1))
+        assert rel_err(d_cic.cpu().numpy(), co) < TOL, rel_err(d_cic.cpu().numpy(), co)
+        scale = max(1.0, np.abs(dip).max())
+        assert np.abs(np.array(dip_g) - dip).max() < TOL * scale, (dip_g, dip)
+    finally:
+        h.final()
