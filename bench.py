@@ -78,6 +78,8 @@ def parse():
                     help="--full-pulse: also FP64 trajectories from the start state perturbed by these relative "
                          "sizes (comma-separated, e.g. 1e-12,1e-9), to show how the dynamics amplify a perturbation")
     ap.add_argument("--ensemble", type=int, default=0, help="also step this many seeded jobs as one ensemble")
+    ap.add_argument("--ensemble-small", action="store_true",
+                    help="the ensemble's jobs from the small range (lmax1 5-15, 8-24 elements)")
     return ap.parse_args()
 
 
@@ -620,7 +622,7 @@ def main():
     # ---- the ensemble (optional)
     ens = None
     if args.ensemble:
-        ens = ensemble_leg(args.ensemble)
+        ens = ensemble_leg(args.ensemble, small=args.ensemble_small)
 
     h.final()
     if rank != 0:
@@ -733,12 +735,12 @@ def full_pulse(args, h, wl, dt, arms, set_arm, steps, placed, deviations, torch,
     return out
 
 
-def ensemble_leg(njob, seed=7, nstep=16):
+def ensemble_leg(njob, seed=7, nstep=16, small=False):
     """The seeded ensemble's jobs stepped together by one graph per step, against the same steps run
     job after job (fs/s summed over the jobs)."""
     from td1c_b200 import autotune
     from td1c_b200.ensemble import DeviceEnsemble, job_list
-    jobs = job_list(seed, njob)
+    jobs = job_list(seed, njob, small=small)
     ens = DeviceEnsemble(jobs, relax_cycles=20)
     try:
         choice = autotune.tune(ens, nstep=2)
@@ -751,7 +753,8 @@ def ensemble_leg(njob, seed=7, nstep=16):
         ens.run_sequential(2, orb=orb, cic=cic)
         ms_seq = ens.run_sequential(nstep, orb=orb, cic=cic)
         fs = ens.simulated_fs(nstep)
-        return {"jobs": njob, "seed": seed, "steps": nstep, "fs_per_s": fs / (ms / 1e3), "ms_per_step": ms / nstep,
+        return {"jobs": njob, "seed": seed, "job_range": "small" if small else "full", "steps": nstep,
+                "fs_per_s": fs / (ms / 1e3), "ms_per_step": ms / nstep,
                 "one_by_one_fs_per_s": fs / (ms_seq / 1e3), "one_by_one_ms_per_step": ms_seq / nstep,
                 "speedup": ms_seq / ms, "tuning": choice}
     finally:

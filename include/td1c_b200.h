@@ -181,16 +181,18 @@ int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield,
  * on the tensor cores with FP32 accumulation, FP64 everywhere else; 0 restores
  * the plain FP64 path.  Every later RHS and step uses the mode.  on = 2 is the
  * same arithmetic on the per-tile split-TF32 kernel instead of the persistent
- * one (for comparisons); other values return 16. */
+ * one (for comparisons); on = 3 is mode 1 with the MO two-electron integrals
+ * (hprod_mkint2_sph.F90:2-100) in split TF32 on the tensor cores as well
+ * (FP64 int2e where that plan does not apply); other values return 16. */
 int td1c_gpu_set_mixed(int on);
 /* Deviation of the mixed form from FP64 on one RHS of a device state:
  * out[0..2] = max |delta| / max |FP64 value| of the pair-density multipoles,
  * the pair potentials on the grid and hwfn.  lfield: host lfield(3,3). */
 int td1c_gpu_mixed_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out);
-/* The split-TF32 int2e of the mixed form on one RHS of a device state:
+/* The split-TF32 int2e of mixed mode 3 on one RHS of a device state:
  * out2[0] = max |delta| / max |value| between the tensor-core int2e and the
  * FP64 DMMA int2e on the same (mixed) pair densities and potentials; out2[1]
- * = the same between the mixed RHS's int2e and the FP64 RHS's.  16 (and
+ * = the same between the mode-3 RHS's int2e and the FP64 RHS's.  16 (and
  * out2 = -1) where the tensor-core plan does not apply (no active orbitals,
  * more than 64 stored active pairs). */
 int td1c_gpu_mixed_int2e_selftest(const void* d_wfn, const void* d_cic, const double* lfield, double* out2);

@@ -1368,9 +1368,9 @@ int i2_split(const Ctx& c) {
   const int k = c.tune_i2_split < 0 ? -c.tune_i2_split : c.tune_i2_split;
   return k > 1 || (k == 1 && c.tune_i2_split > 0) ? std::min(k, c.i2_nsplit) : c.i2_nsplit;
 }
-// int2e: split TF32 on tcgen05 in the mixed-precision form, else FP64 DMMA (or the FFMA blocks)
+// int2e: split TF32 on tcgen05 in mixed mode 3, else FP64 DMMA (or the FFMA blocks)
 int int2e_run(Ctx& c, cudaStream_t s) {
-  if (c.mixed && c.i2_tc) return launch_int2e_tc(c.i2t, c.i2, i2_split(c), s);
+  if (c.mixed == 3 && c.i2_tc) return launch_int2e_tc(c.i2t, c.i2, i2_split(c), s);
   if (c.i2_dmma) return launch_int2e_dmma(c.i2d, c.i2, i2_split(c), s);
   return launch_int2e(c.i2, i2_split(c), s);
 }
@@ -1384,8 +1384,8 @@ int mfprod_run(Ctx& c, cudaStream_t st) {
 int gemm_mf(Ctx& c, const LegGemmBatch* b, int nb, int M, int K, bool pair) {
   if (!c.mixed) return gemm(c, b, nb, M, K, pair);
   c.launches++;
-  if (c.mixed == 1 && b == c.b_rho && c.tc_ok_rho) return launch_legendre_tc(c.tc_rho, c.d_status, c.st);
-  if (c.mixed == 1 && b == c.b_W && c.tc_ok_W) return launch_legendre_tc(c.tc_W, c.d_status, c.st);
+  if (c.mixed != 2 && b == c.b_rho && c.tc_ok_rho) return launch_legendre_tc(c.tc_rho, c.d_status, c.st);
+  if (c.mixed != 2 && b == c.b_W && c.tc_ok_W) return launch_legendre_tc(c.tc_W, c.d_status, c.st);
   return launch_legendre_gemm_tf32(b, nb, M, K, 2 * c.Nr, pair, c.d_status, c.st);
 }
 
@@ -3219,7 +3219,7 @@ void* td1c_gpu_stream(void) { return g ? (void*)g->st : nullptr; }
 int td1c_gpu_set_mixed(int on) {
   Ctx& c = ctx();
   if (!c.initialized) return ST_CONFIG;
-  if (on < 0 || on > 2) return ST_CONFIG;
+  if (on < 0 || on > 3) return ST_CONFIG;
   c.mixed = on;
   if (c.mixed) build_tc_plans(c);
   return 0;
@@ -3279,7 +3279,7 @@ int td1c_gpu_mixed_int2e_selftest(const void* d_wfn, const void* d_cic, const do
   int rc = 0;
   for (int k = 0; k < 3; ++k) {
     if (k < 2) {
-      c.mixed = k ? std::max(keep, 1) : 0;
+      c.mixed = k ? 3 : 0;
       rc |= run_htot(c, c.dip_lfd, (const cplx*)d_wfn, (const cplx*)d_cic, c.hwfn_io, c.hcic_io, 1.0);
     } else {
       // the FP64 DMMA kernel on the mixed RHS's own pair densities and potentials

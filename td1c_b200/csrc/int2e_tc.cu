@@ -1,5 +1,5 @@
-// int2e_tc.cu -- the MO two-electron integrals of the mixed-precision RHS in
-// split TF32 on the fifth-generation tensor cores (hprod_mkint2_sph.F90:2-100).
+// int2e_tc.cu -- the MO two-electron integrals of the mixed-precision RHS (mode 3)
+// in split TF32 on the fifth-generation tensor cores (hprod_mkint2_sph.F90:2-100).
 //
 // int2e(i,j,k,l) = sum_x rho2_ij[x] v2sph_kl[x] over x in [0, K), K =
 // Nr (lmax2 + 1), for the active pairs.  With the P stored active pairs
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(I2T_NT, 1) int2e_tc_kernel(I2tArgs a) {
 
 bool int2e_tc_fits(const I2tArgs& a) {
   return a.P >= 1 && a.P <= 64 && a.NB >= a.P && a.NB % 16 == 0 && 2 * a.NB <= 128 &&
-         int2e_tc_smem(a) <= 227 * 1024 && (size_t)128 * (2 * a.NB + 1) * 8 <= int2e_tc_smem(a);
+         int2e_tc_smem(a) <= 224 * 1024 && (size_t)128 * (2 * a.NB + 1) * 8 <= int2e_tc_smem(a);
 }
 
 int launch_int2e_tc(const I2tArgs& t, const Int2eArgs& sum, int nsplit, cudaStream_t st) {
@@ -237,15 +237,17 @@ int launch_int2e_tc(const I2tArgs& t, const Int2eArgs& sum, int nsplit, cudaStre
   if (!int2e_tc_fits(t) || nsplit < 1) return (int)cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(sum.int2e, 0, sizeof(cplx) * n4, st);
   if (e != cudaSuccess) return (int)e;
-  static bool attr[64] = {};
+  // the dynamic shared memory this plan needs (the kernel's static barriers come on top)
+  const size_t smem = int2e_tc_smem(t);
+  static size_t attr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64 || !attr[dev]) {
-    e = cudaFuncSetAttribute(int2e_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (dev < 0 || dev >= 64 || attr[dev] < smem) {
+    e = cudaFuncSetAttribute(int2e_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    if (dev >= 0 && dev < 64) attr[dev] = true;
+    if (dev >= 0 && dev < 64) attr[dev] = smem;
   }
-  int2e_tc_kernel<<<nsplit, I2T_NT, int2e_tc_smem(t), st>>>(t);
+  int2e_tc_kernel<<<nsplit, I2T_NT, smem, st>>>(t);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   return launch_int2e_sum_fill(sum, nsplit, st);

@@ -5,72 +5,51 @@
 //                  velocity gauge A (-i alpha)(d/dr, (l+1)/r) hprod_pzprod.F90:114-213
 //   frozen core in velocity gauge also gets E r alpha_lm    hprod_htot.F90:120-122
 //
-// One CTA per (orbital, 32-point radial tile, chunk of 12 l channels): the
-// tile of the chunk's channels and of one halo channel on each side, with a
-// +-nd radial halo, is staged in shared memory by cp.async (all copies in
-// flight at once), the banded kinetic (tmat) and derivative (pmat) stencils
-// are applied from smem, the derivative is kept in smem, and the l <-> l+-1
-// laser coupling is formed from smem -- orbitals are read from HBM once (plus
-// the halos) and h0/h1 written once.  About 56 KB of smem per CTA for 21-point
-// elements: four CTAs per SM.
+// One CTA per (orbital, 32-point radial tile): the tile of every l channel
+// plus a +-nd halo is staged in shared memory once, the banded kinetic
+// (tmat) and derivative (pmat) stencils are applied to all l channels from
+// smem, the derivative is kept in smem, and the l <-> l+-1 laser coupling is
+// formed from smem -- orbitals are read from HBM once and h0/h1 written once.
 // The band coefficients come from the (2nd+1) x nrad radk/radk0/radp tables
-// (the tile's rows staged in smem with an odd pitch, so that neither the
-// staging stores nor the stencil's loads conflict) plus a per-(l, r) diagonal,
-// instead of the reference's (2nd+1) x Nr x L1 tmat (19 MB for Ne).  Summation
-// runs over r' in ascending order like zdotu.
+// (the tile's rows staged in smem) plus a per-(l, r) diagonal, instead of the
+// reference's (2nd+1) x Nr x L1 tmat (19 MB for Ne).  Summation runs over r'
+// in ascending order like zdotu.
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace td1c {
 
-constexpr int OB_TILE = 32;          // radial points per CTA
-constexpr int OB_TP = OB_TILE + 1;   // smem pitch of a band row (odd)
-constexpr int OB_LC = 12;            // own l channels per CTA
-
-__device__ __forceinline__ void ob_cp16(void* dst, const void* src, bool ok) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src),
-               "r"(ok ? 16u : 0u)
-               : "memory");
-}
-__device__ __forceinline__ void ob_cp8(void* dst, const void* src, bool ok) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src),
-               "r"(ok ? 8u : 0u)
-               : "memory");
-}
+constexpr int OB_TILE = 32;
 
 __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
-  extern __shared__ __align__(16) double smem_d[];
+  extern __shared__ double smem_d[];
   const int Nr = a.Nr, L1 = a.L1, nd = a.nd, bw = 2 * nd + 1;
   const int W = OB_TILE + 2 * nd;
+  cplx* so = reinterpret_cast<cplx*>(smem_d);  // [L1][W]
+  cplx* sdw = so + (size_t)L1 * W;             // [L1][OB_TILE]
+  double* sb = reinterpret_cast<double*>(sdw + (size_t)L1 * OB_TILE);  // [3][bw][OB_TILE] radk, radk0, radp rows
   const int f = blockIdx.y;
   const int r0 = blockIdx.x * OB_TILE;
-  const int l0 = blockIdx.z * OB_LC;                                      // first own channel
-  const int lb = l0 > 0 ? l0 - 1 : 0, le = l0 + OB_LC + 1 < L1 ? l0 + OB_LC + 1 : L1;  // staged [lb, le)
-  const int ns = le - lb;
-  cplx* so = reinterpret_cast<cplx*>(smem_d);                             // [ns][W]
-  cplx* sdw = so + (size_t)(OB_LC + 2) * W;                               // [ns][OB_TILE]
-  double* sb = reinterpret_cast<double*>(sdw + (size_t)(OB_LC + 2) * OB_TILE);  // [3][bw][OB_TP] radk, radk0, radp
   for (int e = threadIdx.x; e < OB_TILE * bw; e += blockDim.x) {
     const int q = e / bw, jb = e % bw;
     const int ir = r0 + q + 1;
-    const bool ok = ir <= Nr;
-    const size_t o = ok ? (size_t)bw * ir + jb : 0;
-    const int d = jb * OB_TP + q;
-    ob_cp8(sb + d, a.radk + o, ok);
-    ob_cp8(sb + OB_TP * bw + d, a.radk0 + o, ok);
-    ob_cp8(sb + 2 * OB_TP * bw + d, a.radp + o, ok);
+    double k0 = 0.0, k1 = 0.0, pp = 0.0;
+    if (ir <= Nr) {
+      const size_t o = (size_t)bw * ir + jb;
+      k0 = a.radk[o]; k1 = a.radk0[o]; pp = a.radp[o];
+    }
+    const int d = jb * OB_TILE + q;  // band index major: lanes (q) hit consecutive banks
+    sb[d] = k0; sb[OB_TILE * bw + d] = k1; sb[2 * OB_TILE * bw + d] = pp;
   }
   const int m = a.mval[f];
   const int am = m < 0 ? -m : m;
   const cplx* __restrict__ orb = a.orb + (size_t)f * L1 * Nr;
-  for (int e = threadIdx.x; e < ns * W; e += blockDim.x) {
-    const int ls = e / W, q = e % W;
-    const int r = r0 - nd + q;
-    const bool ok = r >= 0 && r < Nr;
-    ob_cp16(so + e, orb + (ok ? (size_t)(lb + ls) * Nr + r : 0), ok);
+  // stage
+  for (int e = threadIdx.x; e < L1 * W; e += blockDim.x) {
+    int l = e / W, q = e % W;
+    int r = r0 - nd + q;
+    so[e] = (r >= 0 && r < Nr) ? orb[(size_t)l * Nr + r] : mkc(0.0, 0.0);
   }
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
   const double zf = a.lfield[2];
   const double ef = a.lfield[5];
@@ -78,45 +57,40 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
   const bool fc = f < a.nfcore;
   cplx* __restrict__ h0 = a.h0orb + (size_t)f * L1 * Nr;
   cplx* __restrict__ h1 = a.h1orb + (size_t)f * L1 * Nr;
-  // h0 of the own channels; the radial derivative of every staged channel (velocity gauge)
-  for (int e = threadIdx.x; e < ns * OB_TILE; e += blockDim.x) {
-    const int ls = e / OB_TILE, q = e % OB_TILE, l = lb + ls;
-    const int r = r0 + q;
+  // h0 and radial derivative
+  for (int e = threadIdx.x; e < L1 * OB_TILE; e += blockDim.x) {
+    int l = e / OB_TILE, q = e % OB_TILE;
+    int r = r0 + q;
     if (r >= Nr) continue;
-    const bool own = l >= l0 && l < l0 + OB_LC;
-    if (!own && !vel) continue;
     const int ir = r + 1;  // Fortran irad
     int jll, jul;
     fedvr_row_span(ir, nd, Nr, jll, jul);  // the band is zero outside the row's element(s)
     cplx hs = mkc(0.0, 0.0), ds = mkc(0.0, 0.0);
     if (l >= am) {
-      const double* rk = sb + (l == 0 ? 0 : OB_TP * bw) + q;
-      const double* rp = sb + 2 * OB_TP * bw + q;
-      const double td = own ? a.tdiag[(size_t)l * Nr + r] : 0.0;
-      const cplx* srow = so + (size_t)ls * W + (nd + q);  // srow[k] = orb(r + k)
+      const double* rk = sb + (l == 0 ? 0 : OB_TILE * bw) + q;
+      const double* rp = sb + 2 * OB_TILE * bw + q;
+      const double td = a.tdiag[(size_t)l * Nr + r];
+      const cplx* srow = so + (size_t)l * W + (nd + q);  // srow[k] = orb(r + k)
       for (int jr = jll; jr <= jul; ++jr) {
         int jb = nd + jr - ir;
         cplx w = srow[jr - ir];
-        if (own) {
-          double t = (jr == ir) ? td : rk[jb * OB_TP];
-          hs.x = fma(w.x, t, hs.x); hs.y = fma(w.y, t, hs.y);
-        }
-        if (vel) { double p = rp[jb * OB_TP]; ds.x = fma(w.x, p, ds.x); ds.y = fma(w.y, p, ds.y); }
+        double t = (jr == ir) ? td : rk[jb * OB_TILE];
+        hs.x = fma(w.x, t, hs.x); hs.y = fma(w.y, t, hs.y);
+        if (vel) { double p = rp[jb * OB_TILE]; ds.x = fma(w.x, p, ds.x); ds.y = fma(w.y, p, ds.y); }
       }
     }
-    if (own) h0[(size_t)l * Nr + r] = hs;
-    sdw[(size_t)ls * OB_TILE + q] = ds;
+    h0[(size_t)l * Nr + r] = hs;
+    sdw[(size_t)l * OB_TILE + q] = ds;
   }
   __syncthreads();
-  // laser coupling of the own channels
-  for (int e = threadIdx.x; e < OB_LC * OB_TILE; e += blockDim.x) {
-    const int l = l0 + e / OB_TILE, q = e % OB_TILE;
-    const int r = r0 + q;
-    if (r >= Nr || l >= L1) continue;
-    const int ls = l - lb;
+  // laser coupling
+  for (int e = threadIdx.x; e < L1 * OB_TILE; e += blockDim.x) {
+    int l = e / OB_TILE, q = e % OB_TILE;
+    int r = r0 + q;
+    if (r >= Nr) continue;
     const double x = a.xrad[r + 1];
     const double* __restrict__ al = a.alph + (size_t)(m + a.mmax1) * L1;
-    const cplx* sc = so + nd + q;  // sc[ls * W] = orb(r, lb + ls)
+    const cplx* sc = so + nd + q;  // sc[l * W] = orb(r, l)
     cplx h = mkc(0.0, 0.0);
     if (vel) {
       // iteration l-1 (as upper channel), then iteration l (as lower channel)
@@ -124,7 +98,7 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
         double alp = al[l - 1];
         double t1 = -zf * alp;                         // zfield * (-i alpha): (0, t1)
         double t2 = zf * ((-alp * (double)l) / x);     // zfield * (-i alpha l / r): (0, t2)
-        cplx dwv = sdw[(size_t)(ls - 1) * OB_TILE + q], wv = sc[(size_t)(ls - 1) * W];
+        cplx dwv = sdw[(size_t)(l - 1) * OB_TILE + q], wv = sc[(size_t)(l - 1) * W];
         h.x = h.x - dwv.y * t1; h.y = h.y + dwv.x * t1;
         h.x = h.x + wv.y * t2;  h.y = h.y - wv.x * t2;
       }
@@ -132,7 +106,7 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
         double alp = al[l];
         double t1 = -zf * alp;
         double t2 = zf * ((-alp * (double)(l + 1)) / x);
-        cplx dwv = sdw[(size_t)(ls + 1) * OB_TILE + q], wv = sc[(size_t)(ls + 1) * W];
+        cplx dwv = sdw[(size_t)(l + 1) * OB_TILE + q], wv = sc[(size_t)(l + 1) * W];
         h.x = h.x - dwv.y * t1; h.y = h.y + dwv.x * t1;
         h.x = h.x - wv.y * t2;  h.y = h.y + wv.x * t2;
       }
@@ -143,12 +117,12 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
     if (zz != 0.0 || !vel) {
       if (l - 1 >= am) {
         double t = zz * (x * al[l - 1]);
-        cplx wv = sc[(size_t)(ls - 1) * W];
+        cplx wv = sc[(size_t)(l - 1) * W];
         h.x = fma(wv.x, t, h.x); h.y = fma(wv.y, t, h.y);
       }
       if (l >= am && l <= L1 - 2) {
         double t = zz * (x * al[l]);
-        cplx wv = sc[(size_t)(ls + 1) * W];
+        cplx wv = sc[(size_t)(l + 1) * W];
         h.x = fma(wv.x, t, h.x); h.y = fma(wv.y, t, h.y);
       }
     }
@@ -156,24 +130,15 @@ __global__ void __launch_bounds__(256) onebody_kernel(OneBodyArgs a) {
   }
 }
 
-size_t onebody_smem(int nd) {
-  const int W = OB_TILE + 2 * nd;
-  return sizeof(cplx) * ((size_t)(OB_LC + 2) * W + (size_t)(OB_LC + 2) * OB_TILE) +
-         sizeof(double) * 3 * (size_t)OB_TP * (2 * nd + 1);
-}
-
 int launch_onebody(const OneBodyArgs& a, cudaStream_t st) {
-  const size_t smem = onebody_smem(a.nd);
-  if (smem > 200 * 1024) return (int)cudaErrorInvalidValue;
-  static bool attr[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64 || !attr[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(onebody_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if (e != cudaSuccess) return (int)e;
-    if (dev >= 0 && dev < 64) attr[dev] = true;
+  const int W = OB_TILE + 2 * a.nd;
+  size_t smem = sizeof(cplx) * ((size_t)a.L1 * W + (size_t)a.L1 * OB_TILE) + sizeof(double) * 3 * OB_TILE * (2 * a.nd + 1);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(onebody_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
   }
-  dim3 grid((a.Nr + OB_TILE - 1) / OB_TILE, a.nfun, (a.L1 + OB_LC - 1) / OB_LC);
+  dim3 grid((a.Nr + OB_TILE - 1) / OB_TILE, a.nfun);
   onebody_kernel<<<grid, 256, smem, st>>>(a);
   return (int)cudaGetLastError();
 }

@@ -46,13 +46,15 @@ def job(lmax1, nfe, nact, fint, wlen, cep, jid=0):
                 wlen=wlen, numcyc=3.0, cep=cep, dt=0.004, seed=1000 + jid)
 
 
-def job_list(seed, n=64):
-    """The ensemble's n jobs, drawn from a seeded Philox stream."""
+def job_list(seed, n=64, small=False):
+    """The ensemble's n jobs, drawn from a seeded Philox stream: lmax1 in [15, 63] and 30 to 80
+    elements, or (small) lmax1 in [5, 15] and 8 to 24 elements."""
     rng = np.random.Generator(np.random.Philox(seed))
     jobs = []
+    lrange, frange = ((5, 16), (8, 25)) if small else ((15, 64), (30, 81))
     for j in range(n):
-        lmax1 = int(rng.integers(15, 64))
-        nfe = int(rng.integers(30, 81))
+        lmax1 = int(rng.integers(*lrange))
+        nfe = int(rng.integers(*frange))
         nact = int(rng.integers(1, 10))
         fint = float(10.0 ** rng.uniform(13.0, math.log10(5e14)))
         wlen = float(rng.uniform(400.0, 1600.0))

@@ -4,8 +4,8 @@ TD-CASSCF configuration on the seeded state, through the C-ABI.
     python -m td1c_b200.profile_case [--mode 0|1|2] [--reps N] [--prop]
 
 mode 0 plain FP64, 1 mixed (persistent split TF32), 2 mixed on the per-tile kernel; --prop runs
---reps split2 steps instead of bare RHS evaluations.  Prints the status word; exits non-zero when
-it is not 0.
+--reps split2 steps (from the committed relaxed start state, at the pulse onset) instead of bare
+RHS evaluations.  Prints the status word; exits non-zero when it is not 0.
 """
 import argparse
 import os
@@ -36,10 +36,11 @@ def main():
     d_hw, d_hc = torch.empty_like(d_orb), torch.empty_like(d_cic)
     h.set_mixed(a.mode)
     if a.prop:
-        h.set_time_kind(0)
-        h.orth_dev(d_orb.data_ptr(), d_cic.data_ptr())
-        h.relax_etdrk2_dev(d_orb.data_ptr(), d_cic.data_ptr(), 0.01, 20)
-        h.set_time_kind(1)
+        from td1c_b200.data.make_relaxed_state import load
+        orb, cic, _ = load()
+        h.set_wfn0(orb, cic)
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
         h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), 0.0, wl["dt"], a.reps)
     else:
         for _ in range(a.reps):
