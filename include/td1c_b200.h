@@ -366,7 +366,8 @@ int td1c_gpu_ensemble_split2(int njob, const int* ids, void* const* d_wfn, void*
  * A window of predicted steps stands if its largest judge value is at most
  * the bound, else the state returns to the window's start and the window
  * is recomputed exactly.  After a judge value above the bound, exact steps
- * without history run for a back-off of 1, 3, 7, ... (at most 63) windows.
+ * without history run for a back-off of 1, 3, 7, ... (at most 63) windows
+ * (63 at once when the judge value is more than ten times the bound).
  * Needs a context bound with split_type 1 (the RHS without h0 and laser). */
 /* Register the network (device pointers, FP32 weights as td1c_mlp_forward
  * takes them, widths 32 .. 8; pack: td1c_mlp_pack_size bytes, the BF16

@@ -2386,6 +2386,14 @@ void make_stream(cudaStream_t* q, bool main) {
   cudaStreamCreateWithPriority(q, cudaStreamNonBlocking, main ? greatest : least);
 }
 
+// windows of exact steps after a judge value above the bound: 1, 3, 7, ... 63, and 63 at
+// once when the value is more than ten times the bound (predictions that far off are not
+// worth screening again soon)
+int lp_next_backoff(int backoff, double judge, double bound) {
+  if (!(judge <= 10.0 * bound)) return 63;
+  return std::min(2 * backoff + 1, 63);
+}
+
 int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, double fint, double wlen, double numcyc, double cep,
                 int maxcyc, double thresh, double* record, double* stats) {
   Ctx& c = ctx();
@@ -2509,7 +2517,7 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
         if (w > 4 && can_predict && (!c.lp_screen || (jd[1] <= c.lp_bound && std::isfinite(jd[1])))) {
           mode = 1;
         } else {
-          backoff = std::min(2 * backoff + 1, 63);
+          backoff = lp_next_backoff(backoff, w > 4 ? jd[1] : 0.0, c.lp_bound);
           plain_left = backoff;
           mode = w > 4 ? 2 : 0;
         }
@@ -2538,7 +2546,7 @@ int learned_run(void* d_wfn, void* d_cic, double t0, double dt, int nstep, doubl
           rc |= j0(s);
           for (int k = 0; k < w && !rc; ++k) rc |= step(1);
           s += w;
-          backoff = std::min(2 * backoff + 1, 63);
+          backoff = lp_next_backoff(backoff, wj, c.lp_bound);
           plain_left = backoff;
           mode = 2;
         }
