@@ -43,6 +43,11 @@ import time
 
 import numpy as np
 
+# the ensemble leg forks one graph into four streams per job: give the device enough hardware
+# work queues that the jobs' streams do not share them (read when CUDA starts)
+if any(a.startswith("--ensemble") for a in sys.argv[1:]):
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 

@@ -229,6 +229,13 @@ int launch_h1fac(const H1FacSrc& s, H1Fac& f, cudaStream_t st) {
 constexpr int H1E_NT = 256;
 constexpr int H1E_LC = 4;   // l channels per CTA
 constexpr int H1E_FG = 3;   // orbital groups of the interior solve
+constexpr int H1E_RMAX = 6; // right-hand sides a thread holds while the band products are read
+
+__device__ __forceinline__ void h1_dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
 
 // shared memory of one element pass; ZI (the previous z rows, read once in
 // step 1) aliases R and Z, which are written only afterwards
@@ -432,60 +439,130 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
   const bool do_t = a.b.x != 0.0 || a.b.y != 0.0;
   const bool do_v = cz.x != 0.0 || cz.y != 0.0;
   const bool vel = a.igauge == 1;
-  if (a.make_rhs) {
-    for (int it = tid; it < nfun * H1E_LC * np; it += H1E_NT) {
-      const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC, p = it % np;
-      const int l = l0 + lc, ip = ir0 + p;
-      if (f < a.f_rhs || l >= L1) continue;
-      cplx r = mkc(0, 0);
-      if (valid(ip)) {
-        const int m = a.mv[f], am = m < 0 ? -m : m;
-        const bool owner = p != nd;       // the right bridge belongs to the next element
-        const bool dyn = f >= a.nfcore;   // frozen-core rows take the a-term only
-        const cplx* xl = X + ((size_t)f * lh + lc + 1) * np;  // x(l, .)
-        if (owner) r = cmul(a.a, xl[p]);
-        if (do_t && dyn && l >= am) {
-          const double* tb = (l == 0 ? Tb0 : Tb1) + p * np;
-          cplx t = mkc(0, 0);
-          for (int q = 0; q < np; ++q) { t.x = fma(tb[q], xl[q].x, t.x); t.y = fma(tb[q], xl[q].y, t.y); }
-          if (owner) {
-            const double d = TD[lc * np + p];
-            t.x = fma(d, xl[p].x, t.x); t.y = fma(d, xl[p].y, t.y);
-          }
-          cfma(r, a.b, t);
-        }
-        if (do_v && dyn) {
-          const double* alq = AL + (size_t)f * lh;  // alq[lq] = alpha(l0 - 1 + lq)
-          const double xr = Xr[p];
-          cplx h = mkc(0, 0);
-          for (int side = 0; side < 2; ++side) {
-            // side 0: coupling from l-1 (l-1 >= |m|); side 1: from l+1 (l >= |m|, l+1 < L1)
-            if (side == 0 ? (l - 1 < am) : (l < am || l + 1 >= L1)) continue;
-            const double alp = side == 0 ? alq[lc] : alq[lc + 1];
-            const cplx* xs = X + ((size_t)f * lh + lc + (side == 0 ? 0 : 2)) * np;
-            if (vel) {
-              // -i alpha (d/dr x_s) (this element's share) and -/+ i alpha (l_s/r) x_s (owner)
-              const double* pr = Pb + p * np;
-              cplx dw = mkc(0, 0);
-              for (int q = 0; q < np; ++q) { dw.x = fma(pr[q], xs[q].x, dw.x); dw.y = fma(pr[q], xs[q].y, dw.y); }
-              dw.x = fma(Pd[p], xs[p].x, dw.x); dw.y = fma(Pd[p], xs[p].y, dw.y);
-              const double t1 = -alp;
-              h.x = h.x - dw.y * t1; h.y = h.y + dw.x * t1;
-              if (owner) {
-                const double t2 = side == 0 ? (-alp * (double)l) / xr : (-alp * (double)(l + 1)) / xr;
-                const cplx wv = xs[p];
-                if (side == 0) { h.x = h.x + wv.y * t2; h.y = h.y - wv.x * t2; }
-                else { h.x = h.x - wv.y * t2; h.y = h.y + wv.x * t2; }
-              }
-            } else if (owner) {
-              const double t = xr * alp;
-              h.x = fma(xs[p].x, t, h.x); h.y = fma(xs[p].y, t, h.y);
-            }
-          }
-          cfma(r, cz, h);
-        }
+  // The band products of the element, T x (kinetic, l >= 1, own rows) and P x (radial
+  // derivative, every staged row), run on the FP64 tensor cores: C(p, n) = sum_q A(p, q) B(q, n)
+  // with A = Tb1 or Pb and B's columns the (re, im) parts of the staged rows, as m8n8k4 DMMA
+  // tiles (rows and depth padded to 8 and 4 with zeros). T x goes to TS (free after step 2),
+  // P x over R and Z (written only after the products are read; the right-hand sides wait in
+  // registers). l = 0 keeps the scalar product with its own table.
+  const int n_t = nfun * H1E_LC, n_p = nfun * lh, n_it = nfun * H1E_LC * np;
+  const bool gem = a.make_rhs && np <= 24 && n_it <= H1E_RMAX * H1E_NT && (do_t || (do_v && vel));
+  cplx* TXs = TS;  // [nfun][LC][np]
+  cplx* PXs = R;   // [nfun][lh][np]
+  if (gem) {
+    __syncthreads();  // step 2 has read TS
+    const int warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
+    const int MT = (np + 7) >> 3, KS = (np + 3) >> 2;
+    const int ntT = do_t ? (n_t + 3) >> 2 : 0, ntP = (do_v && vel) ? (n_p + 3) >> 2 : 0;
+    for (int item = warp; item < MT * (ntT + ntP); item += H1E_NT / 32) {
+      const int mt = item % MT, q = item / MT;
+      const bool isT = q < ntT;
+      const int nt = isT ? q : q - ntT, nrows = isT ? n_t : n_p;
+      const double* A = isT ? Tb1 : Pb;
+      const int brow = 4 * nt + (gid >> 1), part = gid & 1;  // this lane's B column: a complex row, re | im
+      int xrow = -1;
+      if (brow < nrows) xrow = isT ? (brow / H1E_LC) * lh + brow % H1E_LC + 1 : brow;
+      const double* xb = reinterpret_cast<const double*>(X) + (xrow >= 0 ? (size_t)xrow * np * 2 + part : 0);
+      const int pa = 8 * mt + gid;
+      double c0 = 0.0, c1 = 0.0;
+      for (int ks = 0; ks < KS; ++ks) {
+        const int qq = 4 * ks + tig;
+        const double av = (pa < np && qq < np) ? A[pa * np + qq] : 0.0;
+        const double bv = (xrow >= 0 && qq < np) ? xb[2 * qq] : 0.0;
+        h1_dmma(c0, c1, av, bv);
       }
-      R[it] = r;
+      const int crow = 4 * nt + tig;  // C(pa, 8 nt + 2 tig + {0, 1}): Re, Im of complex row crow
+      if (pa < np && crow < nrows) (isT ? TXs : PXs)[(size_t)crow * np + pa] = mkc(c0, c1);
+    }
+    __syncthreads();
+  }
+  // the right-hand side at (orbital, own row, point) of item it (f >= f_rhs, l < L1)
+  auto rhs_of = [&](int it) -> cplx {
+    const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC, p = it % np;
+    const int l = l0 + lc, ip = ir0 + p;
+    cplx r = mkc(0, 0);
+    if (valid(ip)) {
+      const int m = a.mv[f], am = m < 0 ? -m : m;
+      const bool owner = p != nd;       // the right bridge belongs to the next element
+      const bool dyn = f >= a.nfcore;   // frozen-core rows take the a-term only
+      const cplx* xl = X + ((size_t)f * lh + lc + 1) * np;  // x(l, .)
+      if (owner) r = cmul(a.a, xl[p]);
+      if (do_t && dyn && l >= am) {
+        cplx t = mkc(0, 0);
+        if (gem && l > 0) {
+          t = TXs[((size_t)f * H1E_LC + lc) * np + p];
+        } else {
+          const double* tb = (l == 0 ? Tb0 : Tb1) + p * np;
+          for (int q = 0; q < np; ++q) { t.x = fma(tb[q], xl[q].x, t.x); t.y = fma(tb[q], xl[q].y, t.y); }
+        }
+        if (owner) {
+          const double d = TD[lc * np + p];
+          t.x = fma(d, xl[p].x, t.x); t.y = fma(d, xl[p].y, t.y);
+        }
+        cfma(r, a.b, t);
+      }
+      if (do_v && dyn) {
+        const double* alq = AL + (size_t)f * lh;  // alq[lq] = alpha(l0 - 1 + lq)
+        const double xr = Xr[p];
+        cplx h = mkc(0, 0);
+        for (int side = 0; side < 2; ++side) {
+          // side 0: coupling from l-1 (l-1 >= |m|); side 1: from l+1 (l >= |m|, l+1 < L1)
+          if (side == 0 ? (l - 1 < am) : (l < am || l + 1 >= L1)) continue;
+          const double alp = side == 0 ? alq[lc] : alq[lc + 1];
+          const int lq = lc + (side == 0 ? 0 : 2);
+          const cplx* xs = X + ((size_t)f * lh + lq) * np;
+          if (vel) {
+            // -i alpha (d/dr x_s) (this element's share) and -/+ i alpha (l_s/r) x_s (owner)
+            cplx dw = mkc(0, 0);
+            if (gem) {
+              dw = PXs[((size_t)f * lh + lq) * np + p];
+            } else {
+              const double* pr = Pb + p * np;
+              for (int q = 0; q < np; ++q) { dw.x = fma(pr[q], xs[q].x, dw.x); dw.y = fma(pr[q], xs[q].y, dw.y); }
+            }
+            dw.x = fma(Pd[p], xs[p].x, dw.x); dw.y = fma(Pd[p], xs[p].y, dw.y);
+            const double t1 = -alp;
+            h.x = h.x - dw.y * t1; h.y = h.y + dw.x * t1;
+            if (owner) {
+              const double t2 = side == 0 ? (-alp * (double)l) / xr : (-alp * (double)(l + 1)) / xr;
+              const cplx wv = xs[p];
+              if (side == 0) { h.x = h.x + wv.y * t2; h.y = h.y - wv.x * t2; }
+              else { h.x = h.x - wv.y * t2; h.y = h.y + wv.x * t2; }
+            }
+          } else if (owner) {
+            const double t = xr * alp;
+            h.x = fma(xs[p].x, t, h.x); h.y = fma(xs[p].y, t, h.y);
+          }
+        }
+        cfma(r, cz, h);
+      }
+    }
+    return r;
+  };
+  if (a.make_rhs) {
+    if (gem) {
+      cplx racc[H1E_RMAX];
+#pragma unroll
+      for (int k = 0; k < H1E_RMAX; ++k) {
+        const int it = tid + k * H1E_NT;
+        racc[k] = mkc(0, 0);
+        if (it >= n_it) continue;
+        const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC;
+        if (f >= a.f_rhs && l0 + lc < L1) racc[k] = rhs_of(it);
+      }
+      __syncthreads();  // every product has been read: R may be written
+#pragma unroll
+      for (int k = 0; k < H1E_RMAX; ++k) {
+        const int it = tid + k * H1E_NT;
+        if (it >= n_it) continue;
+        const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC;
+        if (f >= a.f_rhs && l0 + lc < L1) R[it] = racc[k];
+      }
+    } else {
+      for (int it = tid; it < n_it; it += H1E_NT) {
+        const int f = it / (H1E_LC * np), lc = (it / np) % H1E_LC;
+        if (f >= a.f_rhs && l0 + lc < L1) R[it] = rhs_of(it);
+      }
     }
   }
   __syncthreads();

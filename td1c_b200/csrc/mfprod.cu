@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(MF_TQ) mfprod_kernel(MfprodArgs a) {
 //   4. twfn_x[pt] from the target's D2V rows (in row order, as the
 //      reference's loop), then v2orbg_k = sum_x rden(x, k) twfn_x.
 // ---------------------------------------------------------------------------
-constexpr int MFD_TQ = 32;              // points per CTA (4 n-tiles)
+constexpr int MFD_TQ = 16;              // points per CTA (2 n-tiles): 3 CTAs per SM
 constexpr int MFD_WP = MFD_TQ + 2;      // double2 pitch of a W row: rows 8 banks apart
 // double2 pitch of a D2V row: odd, so the 8 rows x 4 column pairs of one
 // fragment store fall on 8 different 16-byte bank groups (4 wavefronts, the
