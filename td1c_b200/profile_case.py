@@ -4,8 +4,8 @@ TD-CASSCF configuration on the seeded state, through the C-ABI.
     python -m td1c_b200.profile_case [--mode 0|1|2] [--reps N] [--prop]
 
 mode 0 plain FP64, 1 mixed (persistent split TF32), 2 mixed on the per-tile kernel; --prop runs
---reps split2 steps (from the committed relaxed start state, at the pulse onset) instead of bare
-RHS evaluations.  Prints the status word; exits non-zero when it is not 0.
+--reps split2 steps (from the committed relaxed start state, at --t0, default the pulse onset)
+instead of bare RHS evaluations.  Prints the status word; exits non-zero when it is not 0.
 """
 import argparse
 import os
@@ -19,6 +19,7 @@ def main():
     ap.add_argument("--mode", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--prop", action="store_true")
+    ap.add_argument("--t0", type=float, default=0.0, help="start time of the --prop steps (au)")
     a = ap.parse_args()
     import torch
     from td1c_b200 import basis, workloads as W
@@ -41,7 +42,7 @@ def main():
         h.set_wfn0(orb, cic)
         d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
         d_cic = torch.from_numpy(cic.copy()).cuda()
-        h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), 0.0, wl["dt"], a.reps)
+        h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), a.t0, wl["dt"], a.reps)
     else:
         for _ in range(a.reps):
             h.htot_dev(1.0, np.zeros(9), d_orb.data_ptr(), d_cic.data_ptr(), d_hw.data_ptr(), d_hc.data_ptr())
