@@ -567,26 +567,64 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
   }
   __syncthreads();
   if (a.make_rhs) {
-    // 4. z_e = A_e^-1 r(I_e): thread per (l, k, orbital group)
-    for (int it = tid; it < H1E_LC * ni * H1E_FG; it += H1E_NT) {
-      const int g = it / (H1E_LC * ni), lc = (it / ni) % H1E_LC, k = it % ni;
-      const int l = l0 + lc;
-      if (l >= L1) continue;
-      const cplx* av = AI + (size_t)lc * ni * ni + k;  // av[j * ni] = Ainv(k, j)
-      for (int f = a.f_rhs + g; f < nfun; f += H1E_FG) {
-        const int m = a.mv[f];
-        const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np + 1;
-        cplx zv;
-        if (l < (m < 0 ? -m : m)) {
-          zv = rf[k];
-        } else {
-          zv = mkc(0, 0);
-#pragma unroll
-          for (int j = 0; j < (NDT > 0 ? NDT - 1 : 0); ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
-          for (int j = (NDT > 0 ? NDT - 1 : 0); j < ni; ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
+    // 4. z_e = A_e^-1 r(I_e) for every orbital column at once: complex DMMA tiles (rows the
+    //    element's interior points, columns the orbitals, four real products per depth step in
+    //    separate accumulators); channels below |m| pass through
+    const int nfo = nfun - a.f_rhs;
+    if (ni <= 24 && nfo <= 16) {
+      const int warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
+      const int MT = (ni + 7) >> 3, KS = (ni + 3) >> 2, NTo = (nfo + 7) >> 3;
+      for (int item = warp; item < H1E_LC * MT * NTo; item += H1E_NT / 32) {
+        const int lc = item / (MT * NTo), mt = (item / NTo) % MT, nt = item % NTo;
+        const int l = l0 + lc;
+        if (l >= L1) continue;  // the whole warp: one item per warp
+        const int ka = 8 * mt + gid;            // this lane's A row: interior point ka
+        const int fb = a.f_rhs + 8 * nt + gid;  // this lane's B column: orbital fb
+        const cplx* rb = R + ((size_t)(fb < nfun ? fb : 0) * H1E_LC + lc) * np + 1;
+        double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        for (int ks = 0; ks < KS; ++ks) {
+          const int j = 4 * ks + tig;
+          const cplx av = (ka < ni && j < ni) ? AI[((size_t)lc * ni + j) * ni + ka] : mkc(0, 0);  // Ainv(ka, j)
+          const cplx bv = (fb < nfun && j < ni) ? rb[j] : mkc(0, 0);
+          h1_dmma(acc[0][0], acc[0][1], av.x, bv.x);
+          h1_dmma(acc[1][0], acc[1][1], av.y, -bv.y);
+          h1_dmma(acc[2][0], acc[2][1], av.x, bv.y);
+          h1_dmma(acc[3][0], acc[3][1], av.y, bv.x);
         }
-        Z[((size_t)f * H1E_LC + lc) * ni + k] = zv;
-        z_out[((size_t)f * L1 + l) * nfe * ni + eb + k] = zv;
+        if (ka < ni) {
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {  // C(ka, 8 nt + 2 tig + i): orbital f
+            const int f = a.f_rhs + 8 * nt + 2 * tig + i;
+            if (f >= nfun) continue;
+            const int m = a.mv[f];
+            cplx zv = mkc(acc[0][i] + acc[1][i], acc[2][i] + acc[3][i]);
+            if (l < (m < 0 ? -m : m)) zv = R[((size_t)f * H1E_LC + lc) * np + 1 + ka];
+            Z[((size_t)f * H1E_LC + lc) * ni + ka] = zv;
+            z_out[((size_t)f * L1 + l) * nfe * ni + eb + ka] = zv;
+          }
+        }
+      }
+    } else {
+      for (int it = tid; it < H1E_LC * ni * H1E_FG; it += H1E_NT) {
+        const int g = it / (H1E_LC * ni), lc = (it / ni) % H1E_LC, k = it % ni;
+        const int l = l0 + lc;
+        if (l >= L1) continue;
+        const cplx* av = AI + (size_t)lc * ni * ni + k;  // av[j * ni] = Ainv(k, j)
+        for (int f = a.f_rhs + g; f < nfun; f += H1E_FG) {
+          const int m = a.mv[f];
+          const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np + 1;
+          cplx zv;
+          if (l < (m < 0 ? -m : m)) {
+            zv = rf[k];
+          } else {
+            zv = mkc(0, 0);
+#pragma unroll
+            for (int j = 0; j < (NDT > 0 ? NDT - 1 : 0); ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
+            for (int j = (NDT > 0 ? NDT - 1 : 0); j < ni; ++j) cfma(zv, av[(size_t)j * ni], rf[j]);
+          }
+          Z[((size_t)f * H1E_LC + lc) * ni + k] = zv;
+          z_out[((size_t)f * L1 + l) * nfe * ni + eb + k] = zv;
+        }
       }
     }
     __syncthreads();
