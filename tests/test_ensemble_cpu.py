@@ -29,6 +29,24 @@ def test_job_list_is_seeded_and_in_range():
     assert len(sizes) > 50  # uneven sizes
 
 
+def test_every_job_has_determinants():
+    """Every drawn job has a non-empty CI space in its M sector (a fully occupied active space
+    takes M = 2 sum m); checked with the oracle's string tables on a reduced grid."""
+    from oracle.oracle import Oracle
+    seen = set()
+    for small in (False, True):
+        for j in E.job_list(7, small=small):
+            key = (len(j["orbitals"]), j["mtot"])
+            if key in seen:
+                continue
+            seen.add(key)
+            d = Oracle(dict(j, lmax1=5, lmax2=10, nfe=4, rmax=8.0, rmask=6.0)).dims
+            assert d["lcic"] >= 1, (j["name"], j["mtot"], d["lcic"])
+    assert len(seen) >= 8
+    for j in E.job_list(7, small=True):
+        assert 5 <= j["lmax1"] <= 15 and 8 <= j["nfe"] <= 24
+
+
 def test_cost_model_and_partition():
     jobs = E.job_list(7)
     cost = [E.cost(j) for j in jobs]
