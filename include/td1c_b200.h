@@ -181,7 +181,9 @@ int td1c_gpu_dipole3(const void* d_wfn, const void* d_cic, const double* lfield,
  * on the tensor cores with FP32 accumulation, FP64 everywhere else; 0 restores
  * the plain FP64 path.  Every later RHS and step uses the mode.  on = 2 is the
  * same arithmetic on the per-tile split-TF32 kernel instead of the persistent
- * one (for comparisons); on = 3 is mode 1 with the MO two-electron integrals
+ * one (for comparisons); on = 3 is mode 1 with the Poisson solve's interior
+ * products (the pair densities times the element Poisson inverses,
+ * hprod_mkv2mf.F90:143-178) and the MO two-electron integrals
  * (hprod_mkint2_sph.F90:2-100) in split TF32 on the tensor cores as well
  * (FP64 int2e where that plan does not apply); other values return 16. */
 int td1c_gpu_set_mixed(int on);

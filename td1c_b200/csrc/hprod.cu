@@ -1368,6 +1368,13 @@ int i2_split(const Ctx& c) {
   const int k = c.tune_i2_split < 0 ? -c.tune_i2_split : c.tune_i2_split;
   return k > 1 || (k == 1 && c.tune_i2_split > 0) ? std::min(k, c.i2_nsplit) : c.i2_nsplit;
 }
+// the condensed Poisson solve's arguments: in mixed mode 3 the element pass's interior products
+// run in split TF32
+PsCondArgs ps_args(const Ctx& c) {
+  PsCondArgs a = c.ps_cond;
+  a.tf32 = c.mixed == 3 ? 1 : 0;
+  return a;
+}
 // int2e: split TF32 on tcgen05 in mixed mode 3, else FP64 DMMA (or the FFMA blocks)
 int int2e_run(Ctx& c, cudaStream_t s) {
   if (c.mixed == 3 && c.i2_tc) return launch_int2e_tc(c.i2t, c.i2, i2_split(c), s);
@@ -1492,7 +1499,7 @@ int run_htot(Ctx& c, const double* d_lf, const cplx* wfn, const cplx* cic_in, cp
   } else if (c.neltot >= 2 && c.npair > 0) {
     rc |= chk("rho gemm", gemm_mf(c, c.b_rho, c.npair, c.L2, c.nlat, true));
     mark();  // end rho_gemm
-    rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
+    rc |= chk("poisson", launch_ps_cond(ps_args(c), st));
     c.launches += 3;
     // int2e needs only rho2 and v2sph: third stream, overlapping l->theta,
     // mfprod and the theta->l transforms; then the CI T vectors, which need
@@ -2172,7 +2179,7 @@ int run_meanfield(Ctx& c, const cplx* wfn, const double* d_lf) {
     }
   }
   rc |= chk("rho gemm", gemm_mf(c, c.b_rho, c.npair, c.L2, c.nlat, true));
-  rc |= chk("poisson", launch_ps_cond(c.ps_cond, st));
+  rc |= chk("poisson", launch_ps_cond(ps_args(c), st));
   c.launches += 3;
   rc |= chk("W gemm", gemm_mf(c, c.b_W, c.npair, c.nlat, c.L2, false));
   if (c.nact > 0) {

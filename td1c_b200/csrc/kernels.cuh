@@ -165,6 +165,7 @@ struct PsCondArgs {
   cplx* tpart;           // [L2][nfe][npair] element shares of t
   cplx* xb;              // [L2][nb][npair] bridge values
   cplx* t;               // [L2][npair]
+  int tf32;              // element pass: interior products in split TF32 (mixed mode 3)
 };
 int launch_ps_cond_setup(PsCond& f, const double* xrad, const double* radk, const double* invr, const double* rpl0,
                          const double* rpl1, const double* fac2, int* status, cudaStream_t st);

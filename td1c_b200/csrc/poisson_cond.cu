@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tc.cuh"
 
 namespace td1c {
 
@@ -397,7 +398,17 @@ size_t ps_elem_smem(int nd, int er) {
          sizeof(double) * (size_t)PSE_LC * er + sizeof(int) * PSE_PC;
 }
 
-template <int NDT>
+// mixed mode 3: the interior products in split TF32 (x = x_hi + x_lo, three mma.sync m16n8k8
+// per depth step of 8, lo terms first, FP32 accumulation), the bridge and boundary terms in FP64.
+// The 19 x 19 element blocks are far below tcgen05's 64- and 128-row tiles, so the warp-level
+// MMA is the tensor path here.
+__device__ __forceinline__ void ps_mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int NDT, bool TF32>
 __global__ void __launch_bounds__(PSE_NT, 3) ps_elem_kernel(PsCondArgs a) {
   extern __shared__ __align__(16) unsigned char ps_sm[];
   const PsCond& F = a.f;
@@ -447,6 +458,54 @@ __global__ void __launch_bounds__(PSE_NT, 3) ps_elem_kernel(PsCondArgs a) {
     const double* gls = rec + ni * ni;  // fac2 GL, fac2 GR, fac2 rpl1
     const double* grs = gls + ni;
     const double* q1 = grs + ni;
+    const double* rd = reinterpret_cast<const double*>(RHO);
+    if constexpr (TF32) {
+      const int gid = lane >> 2, tig = lane & 3;
+      for (int mt = 0; mt < 2; ++mt) {
+        if (16 * mt >= ni) break;
+        uint32_t ah[3][4], al[3][4];  // A(k, j) = W(k, j) = rec[j ni + k]: rows 16 mt + gid (+8), depths 8 ks + tig (+4)
+#pragma unroll
+        for (int ks = 0; ks < 3; ++ks)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int k = 16 * mt + gid + 8 * (r & 1), j = 8 * ks + tig + 4 * (r >> 1);
+            tc_split((k < ni && j < ni) ? rec[j * ni + k] : 0.0, ah[ks][r], al[ks][r]);
+          }
+        for (int nt = 0; nt < 4; ++nt) {
+          const int pcb = 16 * half + 4 * nt + (gid >> 1), part = gid & 1;  // this lane's B column
+          float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+          for (int ks = 0; ks < 3; ++ks) {
+            const int j0 = 8 * ks + tig, j1 = j0 + 4;
+            uint32_t bh0, bl0, bh1, bl1;
+            tc_split(j0 < ni ? rd[2 * (pcb * S + lc * ni + j0) + part] : 0.0, bh0, bl0);
+            tc_split(j1 < ni ? rd[2 * (pcb * S + lc * ni + j1) + part] : 0.0, bh1, bl1);
+            ps_mma_tf32(acc, al[ks], bh0, bh1);
+            ps_mma_tf32(acc, ah[ks], bl0, bl1);
+            ps_mma_tf32(acc, ah[ks], bh0, bh1);
+          }
+          const int pc = 16 * half + 4 * nt + tig;  // C(16 mt + gid (+8), 2 tig | 2 tig + 1): re, im of x(k, pc)
+          const int p = p0 + pc;
+          if (p >= npair) continue;
+          const int m = PM[pc];
+          const bool zero = l < (m < 0 ? -m : m);
+          const cplx bl = XB[(2 * lc) * PSE_PC + pc], br = XB[(2 * lc + 1) * PSE_PC + pc];
+          const cplx tt = TS[lc * PSE_PC + pc];
+          cplx* out = a.v2sph + ((size_t)p * L2 + l) * Nr + ir0;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = 16 * mt + gid + 8 * h;
+            if (k >= ni) continue;
+            if (zero) { out[k] = mkc(0, 0); continue; }
+            const double gl = gls[k], gr = grs[k], qq = q1[k];
+            double vx = (double)acc[2 * h], vy = (double)acc[2 * h + 1];
+            vx = fma(-gl, bl.x, vx); vy = fma(-gl, bl.y, vy);
+            vx = fma(-gr, br.x, vx); vy = fma(-gr, br.y, vy);
+            out[k] = mkc(fma(qq, tt.x, vx), fma(qq, tt.y, vy));
+          }
+        }
+      }
+    } else {
     double af[PSE_MT][PSE_KS];  // A(k, j) = W(k, j) = rec[j ni + k], k = 8 mt + lane / 4, j = 4 ks + lane % 4
 #pragma unroll
     for (int mt = 0; mt < PSE_MT; ++mt)
@@ -455,7 +514,6 @@ __global__ void __launch_bounds__(PSE_NT, 3) ps_elem_kernel(PsCondArgs a) {
         const int k = 8 * mt + (lane >> 2), j = 4 * ks + (lane & 3);
         af[mt][ks] = (mt < mt_n && ks < ks_n && k < ni && j < ni) ? rec[j * ni + k] : 0.0;
       }
-    const double* rd = reinterpret_cast<const double*>(RHO);
     for (int nt = 0; nt < 4; ++nt) {
       const int pcb = 16 * half + 4 * nt + (lane >> 3), part = (lane >> 2) & 1;  // this lane's B column
       double acc[PSE_MT][2];
@@ -491,6 +549,7 @@ __global__ void __launch_bounds__(PSE_NT, 3) ps_elem_kernel(PsCondArgs a) {
         out[k] = mkc(fma(qq, tt.x, vx), fma(qq, tt.y, vy));
       }
     }
+    }  // FP64 DMMA
   }
   // the left bridge point
   if (e >= 1) {
@@ -522,10 +581,11 @@ int ps_launch(K kernel, size_t smem, dim3 grid, int nt, const PsCondArgs& a, cud
 
 template <int NDT>
 int launch_ps_tiles(const PsCondArgs& a, bool share, cudaStream_t st) {
-  static size_t cur[2] = {0, 0};
+  static size_t cur[3] = {0, 0, 0};
   const dim3 grid(a.f.nfe, (a.L2 + PSE_LC - 1) / PSE_LC, (a.npair + PSE_PC - 1) / PSE_PC);
   if (share) return ps_launch(ps_share_kernel<NDT>, ps_share_smem(a.f.nd, a.f.sr), grid, PSE_NT, a, st, cur[1]);
-  return ps_launch(ps_elem_kernel<NDT>, ps_elem_smem(a.f.nd, a.f.er), grid, PSE_NT, a, st, cur[0]);
+  if (a.tf32) return ps_launch(ps_elem_kernel<NDT, true>, ps_elem_smem(a.f.nd, a.f.er), grid, PSE_NT, a, st, cur[2]);
+  return ps_launch(ps_elem_kernel<NDT, false>, ps_elem_smem(a.f.nd, a.f.er), grid, PSE_NT, a, st, cur[0]);
 }
 
 int launch_ps_pass(const PsCondArgs& a, bool share, cudaStream_t st) {

@@ -186,7 +186,8 @@ class HProd:
     def set_mixed(self, on):
         """Mixed-precision form of every later RHS: the mean field's pair-density multipoles and pair
         potentials in split TF32 on the tensor cores (on=True or 1; 2 = the same arithmetic on the
-        per-tile kernel; 3 = mode 1 with int2e in split TF32 too), or plain FP64 (on=False or 0)."""
+        per-tile kernel; 3 = mode 1 with the Poisson interior products and int2e in split TF32 too),
+        or plain FP64 (on=False or 0)."""
         self._check(self.lib.td1c_gpu_set_mixed(int(on) if not isinstance(on, bool) else (1 if on else 0)))
 
     def mixed_selftest(self, d_wfn, d_cic, lfield):

@@ -156,3 +156,47 @@ def test_mixed_int2e_tensor_cores(cuda_ok, base):
         assert h.last_status() == 0
     finally:
         h.final()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.NE_SMALL, W.NE_CAS], ids=lambda w: w["name"])
+def test_mode3_poisson_interior_in_tf32(cuda_ok, base):
+    """Mixed mode 3 also runs the condensed Poisson solve's interior products (pair density times
+    the element's Poisson inverse) in split TF32: the multipole potentials v2sph of one RHS deviate
+    from FP64 by FP32-class amounts (the transforms' pair densities feed them too), and hwfn stays
+    within 1e-5 of FP64."""
+    import torch
+    from td1c_b200 import basis
+    from td1c_b200.hprod import HProd
+    from td1c_b200.wfn import seeded_orbitals, seeded_cic
+    from .helpers import rel_err
+    if base is W.NE_CAS:
+        wl = dict(base, split_type=1)
+        rad, ang = basis.build(wl)
+        h = HProd(wl, rad, ang)
+        tb = h.ci_tables()
+        orb = seeded_orbitals(wl, rad["xrad"], rad["wrad"], rad["mask"])
+        cic = seeded_cic(wl, h.dims["lcic"], tb["stra"], tb["strb"], tb["detoff"], tb["afirst"], tb["acount"])
+        h.set_wfn0(orb, cic)
+        lf = h.pulse_lfield(100.0)
+    else:
+        o, h, wl, orb, cic = _setup(base)
+        lf = o.field(30.0)
+    try:
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        d_hw, d_hc = torch.empty_like(d_orb), torch.empty_like(d_cic)
+        out = {}
+        for mode in (0, 1, 3):
+            h.set_mixed(mode)
+            h.htot_dev(1.0, lf, d_orb.data_ptr(), d_cic.data_ptr(), d_hw.data_ptr(), d_hc.data_ptr())
+            h.sync()
+            out[mode] = (h.debug("v2sph"), d_hw.cpu().numpy())
+        h.set_mixed(False)
+        d1, d3 = rel_err(out[1][0], out[0][0]), rel_err(out[3][0], out[0][0])
+        assert 0.0 < d1 < 2e-6 and 0.0 < d3 < 5e-6, (d1, d3)
+        assert rel_err(out[3][0], out[1][0]) > 0.0  # the TF32 interior products ran
+        assert rel_err(out[3][1], out[0][1]) < 1e-5
+        assert h.last_status() == 0
+    finally:
+        h.final()
