@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed and learned+mixed arms")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned+mixed arm")
+    ap.add_argument("--mixed-mode", type=int, default=1, choices=[1, 3],
+                    help="mixed-precision mode of the mixed and learned arms (3: Poisson interior products "
+                         "and int2e in split TF32 as well)")
     ap.add_argument("--no-peak", action="store_true", help="skip the window at the |A| peak")
     ap.add_argument("--train-traj", type=int, default=200, help="trajectories of the learned predictor's training set")
     ap.add_argument("--train-iters", type=int, default=400)
@@ -213,6 +216,10 @@ def fp64_peak_tflops(torch):
         best = min(best, e0.elapsed_time(e1) / 1e3)
     del a, b
     return 2.0 * n ** 3 / best / 1e12
+
+
+MIXED_NOTE = {1: "mixed (split TF32 pair-field transforms)",
+              3: "mixed mode 3 (split TF32 pair-field transforms, Poisson interior products and int2e)"}
 
 
 def committed_state(wl, nrad, lmax1, mmax1, nfun, lcic):
@@ -431,7 +438,7 @@ def main():
         return None
 
     def set_arm(arm):
-        h.set_mixed(arm in ("mixed", "learned"))
+        h.set_mixed(args.mixed_mode if arm in ("mixed", "learned") else 0)
 
     def window(arm, t_start, n, warm, o_start=None, c_start=None):
         """warm + n steps of an arm from the given start (default the window start state); returns
@@ -613,7 +620,9 @@ def main():
                 "frac": by / t_dom / 1e9 / hbm, "traffic": traffic, "kernel": dom, "peak_source": hbm_src}
     mixed_dev = None
     if not args.no_mixed:
+        h.set_mixed(args.mixed_mode)  # the self-test compares the current mixed mode with FP64
         rd = h.mixed_selftest(d_relaxed.data_ptr(), c_relaxed.data_ptr(), gauge_field(wl, t0))
+        h.set_mixed(0)
         mixed_dev = {"rho2": float(rd[0]), "W": float(rd[1]), "hwfn": float(rd[2])}
 
     # ---- the whole pulse (optional here; the default line carries the committed measurement)
@@ -641,9 +650,9 @@ def main():
         "data": "synthetic: %s; one trajectory per arm from t0 (velocity-gauge phase of A(t0))" % relax["source"],
         "config": {"workload": wl["name"], "dt_au": dt, "arm": {"learned": "learned+mixed", "mixed": "mixed",
                                                                 "fp64": "fp64"}[head_arm],
-                   "precision": {"learned": "mixed (split TF32 pair-field transforms) + learned stage mean fields "
-                                            "(judge bound %g)" % args.bound,
-                                 "mixed": "mixed (split TF32 pair-field transforms)", "fp64": "fp64"}[head_arm],
+                   "precision": {"learned": "%s + learned stage mean fields (judge bound %g)" % (MIXED_NOTE[args.mixed_mode],
+                                                                                                 args.bound),
+                                 "mixed": MIXED_NOTE[args.mixed_mode], "fp64": "fp64"}[head_arm],
                    "prop": PROP_NOTE[args.prop], "rhs_per_step": RHS_PER_STEP[args.prop],
                    "window": "one trajectory per arm from t0 = %g au: %d warm-up then %d timed steps" % (t0, args.warmup,
                                                                                                        args.steps),
