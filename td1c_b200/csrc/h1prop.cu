@@ -227,7 +227,7 @@ int launch_h1fac(const H1FacSrc& s, H1Fac& f, cudaStream_t st) {
 // consecutive passes alternate between two z buffers.
 // ---------------------------------------------------------------------------
 constexpr int H1E_NT = 256;
-constexpr int H1E_LC = 4;   // l channels per CTA
+constexpr int H1E_LC = 3;   // l channels per CTA (about 64 KB of shared memory: 3 CTAs per SM)
 constexpr int H1E_FG = 3;   // orbital groups of the interior solve
 constexpr int H1E_RMAX = 6; // right-hand sides a thread holds while the band products are read
 
@@ -254,8 +254,7 @@ struct H1ElemSmem {
   __host__ __device__ size_t xb_off() const { return ts_off() + (size_t)nf * H1E_LC * np; }
   __host__ __device__ size_t g_off() const { return xb_off() + (size_t)nf * lh * 2; }
   __host__ __device__ size_t v_off() const { return g_off() + (size_t)2 * lh * ni(); }
-  __host__ __device__ size_t ai_off() const { return v_off() + (size_t)2 * H1E_LC * ni(); }
-  __host__ __device__ size_t cplx_count() const { return ai_off() + (size_t)H1E_LC * ni() * ni(); }
+  __host__ __device__ size_t cplx_count() const { return v_off() + (size_t)2 * H1E_LC * ni(); }
   __host__ __device__ size_t dbl_count() const { return (size_t)3 * np * np + 2 * np + (size_t)H1E_LC * np + (size_t)nf * lh; }
   __host__ __device__ size_t bytes() const { return sizeof(cplx) * cplx_count() + sizeof(double) * dbl_count(); }
 };
@@ -275,7 +274,7 @@ __device__ __forceinline__ void cpa_wait_all() {
 }
 
 template <int NDT>
-__global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
+__global__ void __launch_bounds__(H1E_NT, 3) h1elem_kernel(H1ElemArgs a) {
   if (a.check_skip && *a.done) return;
   extern __shared__ cplx sm[];
   const H1Fac& F = a.fac;
@@ -294,7 +293,6 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
   cplx* GRs = GLs + lh * ni;      // [lh][ni]
   cplx* VLs = sm + lay.v_off();   // [LC][ni]
   cplx* VRs = VLs + H1E_LC * ni;  // [LC][ni]
-  cplx* AI = sm + lay.ai_off();   // [LC][ni][ni], AI[lc][j][k] = (A_e^-1)(k, j)
   double* Pb = reinterpret_cast<double*>(sm + lay.cplx_count());  // [np][np] derivative, off-diagonal
   double* Tb0 = Pb + np * np;     // [np][np] kinetic off-diagonal, l = 0 (radk)
   double* Tb1 = Tb0 + np * np;    // l >= 1 (radk0)
@@ -385,11 +383,6 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
       cpa16(VLs + q2, F.vl + vi, ok);
       cpa16(VRs + q2, F.vr + vi, ok);
     }
-    for (int q2 = tid; q2 < H1E_LC * ni * ni; q2 += H1E_NT) {
-      const int lc = q2 / (ni * ni), jk = q2 % (ni * ni), l = l0 + lc;
-      const bool ok = l < L1;
-      cpa16(AI + q2, F.ainv + (ok ? ((size_t)l * nfe * ni + eb) * ni + jk : 0), ok);
-    }
   }
   cpa_wait_all();
   __syncthreads();
@@ -446,7 +439,8 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
   // P x over R and Z (written only after the products are read; the right-hand sides wait in
   // registers). l = 0 keeps the scalar product with its own table.
   const int n_t = nfun * H1E_LC, n_p = nfun * lh, n_it = nfun * H1E_LC * np;
-  const bool gem = a.make_rhs && np <= 24 && n_it <= H1E_RMAX * H1E_NT && (do_t || (do_v && vel));
+  const bool gem = a.make_rhs && np <= 24 && n_it <= H1E_RMAX * H1E_NT && (do_t || (do_v && vel)) &&
+                   (size_t)n_p * np <= lay.rz_end() - lay.r_off();
   cplx* TXs = TS;  // [nfun][LC][np]
   cplx* PXs = R;   // [nfun][lh][np]
   if (gem) {
@@ -578,13 +572,14 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
         const int lc = item / (MT * NTo), mt = (item / NTo) % MT, nt = item % NTo;
         const int l = l0 + lc;
         if (l >= L1) continue;  // the whole warp: one item per warp
+        const cplx* Ag = F.ainv + ((size_t)l * nfe * ni + eb) * ni;  // (A_e^-1)(k, j) at [j ni + k], L2-resident
         const int ka = 8 * mt + gid;            // this lane's A row: interior point ka
         const int fb = a.f_rhs + 8 * nt + gid;  // this lane's B column: orbital fb
         const cplx* rb = R + ((size_t)(fb < nfun ? fb : 0) * H1E_LC + lc) * np + 1;
         double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
         for (int ks = 0; ks < KS; ++ks) {
           const int j = 4 * ks + tig;
-          const cplx av = (ka < ni && j < ni) ? AI[((size_t)lc * ni + j) * ni + ka] : mkc(0, 0);  // Ainv(ka, j)
+          const cplx av = (ka < ni && j < ni) ? __ldg(Ag + (size_t)j * ni + ka) : mkc(0, 0);  // Ainv(ka, j)
           const cplx bv = (fb < nfun && j < ni) ? rb[j] : mkc(0, 0);
           h1_dmma(acc[0][0], acc[0][1], av.x, bv.x);
           h1_dmma(acc[1][0], acc[1][1], av.y, -bv.y);
@@ -609,7 +604,7 @@ __global__ void __launch_bounds__(H1E_NT, 2) h1elem_kernel(H1ElemArgs a) {
         const int g = it / (H1E_LC * ni), lc = (it / ni) % H1E_LC, k = it % ni;
         const int l = l0 + lc;
         if (l >= L1) continue;
-        const cplx* av = AI + (size_t)lc * ni * ni + k;  // av[j * ni] = Ainv(k, j)
+        const cplx* av = F.ainv + ((size_t)l * nfe * ni + eb) * ni + k;  // av[j * ni] = Ainv(k, j)
         for (int f = a.f_rhs + g; f < nfun; f += H1E_FG) {
           const int m = a.mv[f];
           const cplx* rf = R + ((size_t)f * H1E_LC + lc) * np + 1;
