@@ -200,3 +200,40 @@ def test_mode3_poisson_interior_in_tf32(cuda_ok, base):
         assert h.last_status() == 0
     finally:
         h.final()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("base", [W.NE_SMALL, W.MIXED_SMALL], ids=lambda w: w["name"])
+def test_mixed_against_the_oracle(cuda_ok, base):
+    """The mixed form against the oracle directly (not only against the device's FP64 path): one
+    RHS (hwfn and hcic within 1e-5 relative) and 8 split2 steps at dt = 0.004 (state within 1e-5,
+    the dipole after every step within 1e-5 a.u.)."""
+    import torch
+    from .helpers import rel_err
+    o, h, wl, orb, cic = _setup(base)
+    try:
+        lf = o.field(30.0)
+        hw_o, hc_o = o.htot(1.0, lf, orb, cic)
+        d_orb = torch.from_numpy(orb.reshape(-1).copy()).cuda()
+        d_cic = torch.from_numpy(cic.copy()).cuda()
+        d_hw, d_hc = torch.empty_like(d_orb), torch.empty_like(d_cic)
+        h.set_mixed(1)
+        h.htot_dev(1.0, lf, d_orb.data_ptr(), d_cic.data_ptr(), d_hw.data_ptr(), d_hc.data_ptr())
+        h.sync()
+        assert rel_err(d_hw.cpu().numpy(), np.asarray(hw_o).reshape(-1)) < 1e-5
+        assert rel_err(d_hc.cpu().numpy(), np.asarray(hc_o).reshape(-1)) < 1e-5
+        freq = 1239.84190 / (wl["wlen"] * 27.2113845)
+        t0, dt, nstep = 0.4 * wl["numcyc"] * 2 * np.pi / freq, 0.004, 8
+        wo, co, dip = o.split2(orb, cic, t0, dt, nstep)
+        h.rk4_reset(None, None)
+        dip_g = []
+        for s in range(nstep):
+            h.split2_dev(d_orb.data_ptr(), d_cic.data_ptr(), t0 + s * dt, dt, 1)
+            dip_g.append(h.dipole_dev(d_orb.data_ptr(), d_cic.data_ptr()))
+        h.sync()
+        h.set_mixed(0)
+        assert rel_err(d_orb.cpu().numpy(), np.asarray(wo).reshape(-1)) < 1e-5
+        assert np.abs(np.array(dip_g) - np.asarray(dip)).max() < 1e-5, (dip_g, dip)
+        assert h.last_status() == 0
+    finally:
+        h.final()
